@@ -1,0 +1,863 @@
+// C-ABI entry points (include/dmfted.h) and the host orchestration of
+// ed_solve_single for the normal mode.  Every entry point converts exceptions
+// into status codes; nothing here falls back to a host computation of the hot
+// path.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace dmfted {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+const char *last_error() { return g_last_error.c_str(); }
+
+// binomial of ED_SETUP.f90:1258-1275 (FP64 running product, int(x+0.5)), used
+// for the exported sector tables so they match the reference's integers.
+static int32_t ref_binomial(int n1, int n2) {
+    double xh = 1.0;
+    if (n2 < 0) return 0;
+    if (n2 == 0) return 1;
+    for (int i = 1; i <= n2; i++) xh = xh * (double)(n1 + 1 - i) / (double)i;
+    return (int32_t)(xh + 0.5);
+}
+
+// setup_pointers_normal, ED_SETUP.f90:379-493 (normal ed_mode, normal bath).
+static void setup_pointers_normal(dmfted_ctx *c) {
+    const int ns = c->ns, norb = c->norb, nbath = c->nbath;
+    const int nsect = (ns + 1) * (ns + 1);
+    c->nsectors = nsect;
+    c->getsector.assign((ns + 1) * (ns + 1), 0);
+    c->getnup.assign(nsect, 0);
+    c->getndw.assign(nsect, 0);
+    c->getdim.assign(nsect, 0);
+    c->getdimup.assign(nsect, 0);
+    c->getdimdw.assign(nsect, 0);
+    c->getcsector.assign(2 * nsect, 0);
+    c->getcdgsector.assign(2 * nsect, 0);
+    c->getbathstride.assign(norb * nbath, 0);
+    c->impindex.assign(2 * norb, 0);
+    int is = 0;
+    for (int nup = 0; nup <= ns; nup++)
+        for (int ndw = 0; ndw <= ns; ndw++) {
+            is++;
+            c->getsector[nup * (ns + 1) + ndw] = is;
+            c->getnup[is - 1] = nup;
+            c->getndw[is - 1] = ndw;
+            c->getdim[is - 1] = ref_binomial(ns, nup) * ref_binomial(ns, ndw);
+            c->getdimup[is - 1] = ref_binomial(ns, nup);
+            c->getdimdw[is - 1] = ref_binomial(ns, ndw);
+        }
+    for (int in = 1; in <= norb; in++) {
+        c->impindex[in - 1] = in;
+        c->impindex[norb + in - 1] = in + ns;
+    }
+    for (int i = 1; i <= nbath; i++)
+        for (int iorb = 1; iorb <= norb; iorb++)
+            c->getbathstride[(i - 1) * norb + iorb - 1] = norb + (iorb - 1) * nbath + i;
+    for (int s = 1; s <= nsect; s++) {
+        const int nup = c->getnup[s - 1], ndw = c->getndw[s - 1];
+        if (nup - 1 >= 0) c->getcsector[2 * (s - 1) + 0] = c->getsector[(nup - 1) * (ns + 1) + ndw];
+        if (ndw - 1 >= 0) c->getcsector[2 * (s - 1) + 1] = c->getsector[nup * (ns + 1) + ndw - 1];
+        if (nup + 1 <= ns) c->getcdgsector[2 * (s - 1) + 0] = c->getsector[(nup + 1) * (ns + 1) + ndw];
+        if (ndw + 1 <= ns) c->getcdgsector[2 * (s - 1) + 1] = c->getsector[nup * (ns + 1) + ndw + 1];
+    }
+    c->neigen_sector.assign(nsect, 0);
+    for (int s = 0; s < nsect; s++)
+        c->neigen_sector[s] = std::min(c->getdim[s], c->p.lanc_nstates_sector);
+    c->twin_mask.assign(nsect, 1);
+    if (c->p.ed_twin)
+        for (int s = 0; s < nsect; s++)
+            if (c->getnup[s] < c->getndw[s]) c->twin_mask[s] = 0;
+}
+
+static void check_hloc(const dmfted_ctx *c, const double *h) {
+    const int ns = c->nspin, no = c->norb;
+    for (int is = 0; is < ns; is++)
+        for (int js = 0; js < ns; js++)
+            for (int a = 0; a < no; a++)
+                for (int b = 0; b < no; b++) {
+                    const int64_t idx = is + ns * (js + ns * (a + (int64_t)no * b));
+                    const double re = h[2 * idx], im = h[2 * idx + 1];
+                    DM_REQUIRE(std::isfinite(re) && std::isfinite(im), DMFTED_ERR_ARG,
+                               "Hloc has a non-finite entry");
+                    DM_REQUIRE(im == 0.0, DMFTED_ERR_UNSUPPORTED,
+                               "complex Hloc: this solver runs the real normal-bath Hamiltonian");
+                    DM_REQUIRE(is == js || re == 0.0, DMFTED_ERR_UNSUPPORTED,
+                               "spin off-diagonal Hloc belongs to ed_mode=nonsu2");
+                }
+}
+
+static void upload_model(dmfted_ctx *c) {
+    const int nso = c->nspin * c->norb;
+    c->d_bath_e.alloc(std::max<size_t>(c->bath_e.size(), 1));
+    c->d_bath_v.alloc(std::max<size_t>(c->bath_v.size(), 1));
+    c->d_hloc_aa.alloc(nso);
+    std::vector<double> haa(nso);
+    for (int is = 0; is < c->nspin; is++)
+        for (int a = 0; a < c->norb; a++) {
+            const int64_t idx = is + c->nspin * (is + c->nspin * (a + (int64_t)c->norb * a));
+            haa[is * c->norb + a] = c->hloc[2 * idx];
+        }
+    if (!c->bath_e.empty()) {
+        DM_CUDA(cudaMemcpyAsync(c->d_bath_e.p, c->bath_e.data(), c->bath_e.size() * 8,
+                                cudaMemcpyHostToDevice, c->stream));
+        DM_CUDA(cudaMemcpyAsync(c->d_bath_v.p, c->bath_v.data(), c->bath_v.size() * 8,
+                                cudaMemcpyHostToDevice, c->stream));
+    }
+    DM_CUDA(cudaMemcpyAsync(c->d_hloc_aa.p, haa.data(), nso * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+// Kept states of the eigenspace: a device pool of FP64 vectors.
+static void states_reset(dmfted_ctx *c) { c->states.clear(); }
+
+static int64_t states_used(const dmfted_ctx *c) {
+    int64_t u = 0;
+    for (auto &s : c->states) u = std::max<int64_t>(u, s.off + c->binom[c->getnup[s.isector - 1]] *
+                                                                 c->binom[c->getndw[s.isector - 1]]);
+    return u;
+}
+
+static void states_add(dmfted_ctx *c, double e, int isector, const double *psi, int64_t dim) {
+    const int64_t off = (states_used(c) + 31) / 32 * 32;
+    if ((size_t)(off + dim) > c->states64.n) {
+        const size_t cap = std::max<size_t>((size_t)(off + dim), c->states64.n * 2);
+        double *np = nullptr;
+        cudaError_t err = cudaMalloc((void **)&np, cap * sizeof(double));
+        DM_REQUIRE(err == cudaSuccess, DMFTED_ERR_NOMEM, "cudaMalloc for the eigenspace failed");
+        if (c->states64.p && off > 0)
+            DM_CUDA(cudaMemcpyAsync(np, c->states64.p, off * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+        DM_CUDA(cudaStreamSynchronize(c->stream));
+        c->states64.release();
+        c->states64.p = np;
+        c->states64.n = cap;
+    }
+    DM_CUDA(cudaMemcpyAsync(c->states64.p + off, psi, dim * sizeof(double), cudaMemcpyDeviceToDevice,
+                            c->stream));
+    // energy-ordered insertion after equal energies (es_insert_state_c,
+    // ED_EIGENSPACE.f90:157-213: traverse until e <= next)
+    auto it = c->states.begin();
+    while (it != c->states.end() && !(e <= it->e)) ++it;
+    c->states.insert(it, dmfted_ctx::State{e, isector, off});
+}
+
+__global__ void k_interleave_split(const double *z, double *re, double *im, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        re[i] = z[2 * i];
+        im[i] = z[2 * i + 1];
+    }
+}
+__global__ void k_interleave_join(const double *re, const double *im, double *z, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        z[2 * i] = re[i];
+        z[2 * i + 1] = im ? im[i] : 0.0;
+    }
+}
+
+static int ew(dmfted_ctx *c, int64_t n) {
+    return (int)std::min<int64_t>(std::max<int64_t>(div_up(n, 256), 1), 16 * num_sms(c));
+}
+
+// Copy a device FP64 real vector to a host complex128 array (imag = 0).
+static void real_to_host_c128(dmfted_ctx *c, const double *d, int64_t n, double *host) {
+    c->wv64.alloc(2 * n);
+    k_interleave_join<<<ew(c, n), 256, 0, c->stream>>>(d, nullptr, c->wv64.p, n);
+    DM_CHECK_LAUNCH();
+    c->launches++;
+    DM_CUDA(cudaMemcpyAsync(host, c->wv64.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+// ---------------------------------------------------------------------------
+// The solve.  Mirrors ed_solve_single (ED_MAIN.f90:251-289):
+//   diagonalize_impurity -> ed_diag_c (sector loop and state selection,
+//   ED_DIAG.f90:93-228) + ed_analysis (Z, ED_DIAG.f90:248-277)
+//   observables_impurity (n, docc, ED_OBSERVABLES.f90:113-160)
+//   buildgf_impurity -> lanc_build_gf_normal_c per (iorb, ispin)
+//   (build_gf_normal.f90:4-16,71-180) -> get_sigma_normal.
+static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list) {
+    DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "ed_solve: bath not set");
+    const dmfted_params &p = c->p;
+    c->finite_t = p.lanc_nstates_total != 1;  // ED_SETUP.f90:242-246
+    DM_REQUIRE(!c->finite_t, DMFTED_ERR_UNSUPPORTED,
+               "finite temperature (lanc_nstates_total > 1) is not available in this build");
+    DM_REQUIRE(!p.ed_twin, DMFTED_ERR_UNSUPPORTED, "ed_twin is not available in this build");
+    std::vector<int> list;
+    if (sectors && nsect_list > 0) {
+        for (int i = 0; i < nsect_list; i++) {
+            DM_REQUIRE(sectors[i] >= 1 && sectors[i] <= c->nsectors, DMFTED_ERR_ARG,
+                       "ed_solve: sector index out of range");
+            list.push_back(sectors[i]);
+        }
+    } else {
+        for (int s = 1; s <= c->nsectors; s++)
+            if (c->twin_mask[s - 1]) list.push_back(s);
+    }
+    cudaEvent_t ev[4];
+    for (auto &e : ev) DM_CUDA(cudaEventCreate(&e));
+    DM_CUDA(cudaEventRecord(ev[0], c->stream));
+    // ---- diagonalisation ------------------------------------------------
+    states_reset(c);
+    double oldzero = 1000.0;
+    const double gsth = p.gs_threshold;
+    int64_t hv_diag = 0;
+    for (int isector : list) {
+        SectorView s = sector_view(c, isector);
+        c->s64a.alloc(s.dim);
+        const int nit = (int)std::min<int64_t>(s.dim, p.lanc_niter);
+        LanczosResult r = lanczos_gs(c, s, c->s64a.p, nullptr, p.precision, p.lanc_tolerance, nit);
+        hv_diag += r.steps;
+        const double enemin = r.e0;
+        // T=0 state selection, ED_DIAG.f90:202-214
+        if (enemin < oldzero - 10.0 * gsth) {
+            oldzero = enemin;
+            states_reset(c);
+            states_add(c, enemin, isector, c->s64a.p, s.dim);
+        } else if (std::fabs(enemin - oldzero) <= gsth) {
+            oldzero = std::min(oldzero, enemin);
+            states_add(c, enemin, isector, c->s64a.p, s.dim);
+        }
+    }
+    DM_REQUIRE(!c->states.empty(), DMFTED_ERR_NOTCONV, "ed_solve: no state kept");
+    c->egs = c->states.front().e;
+    for (auto &st : c->states) c->egs = std::min(c->egs, st.e);
+    c->zeta = (double)c->states.size();  // T=0: Z = number of ground states
+    DM_CUDA(cudaEventRecord(ev[1], c->stream));
+    // ---- observables -------------------------------------------------------
+    const int na = obs_count(c);
+    c->obs_d.alloc(na);
+    std::vector<double> acc(na, 0.0), one(na);
+    for (auto &st : c->states) {
+        SectorView s = sector_view(c, st.isector);
+        const double peso = 1.0 / c->zeta;
+        observables_raw(c, s, c->states64.p + st.off, c->obs_d.p);
+        DM_CUDA(cudaMemcpyAsync(one.data(), c->obs_d.p, na * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+        DM_CUDA(cudaStreamSynchronize(c->stream));
+        for (int q = 0; q < na; q++) acc[q] += peso * one[q];
+    }
+    const int no = c->norb;
+    c->obs.assign(5 * no, 0.0);
+    for (int a = 0; a < no; a++) {
+        const double nu = acc[a], nd = acc[no + a];
+        c->obs[a] = nu + nd;           // dens
+        c->obs[no + a] = nu;           // dens_up
+        c->obs[2 * no + a] = nd;       // dens_dw
+        c->obs[3 * no + a] = acc[2 * no + a];  // docc
+        c->obs[4 * no + a] = nu - nd;  // magz
+    }
+    c->hf_terms.assign(acc.begin() + 3 * no, acc.end());
+    DM_CUDA(cudaEventRecord(ev[2], c->stream));
+    // ---- Green's functions ---------------------------------------------------
+    const int L = p.lmats + p.lreal;
+    const size_t gsz = (size_t)c->nspin * no;
+    c->gm.alloc(std::max<size_t>(2 * gsz * p.lmats, 2));
+    c->gr.alloc(std::max<size_t>(2 * gsz * p.lreal, 2));
+    c->sm.alloc(std::max<size_t>(2 * gsz * p.lmats, 2));
+    c->sr.alloc(std::max<size_t>(2 * gsz * p.lreal, 2));
+    c->g0m.alloc(std::max<size_t>(2 * gsz * p.lmats, 2));
+    DM_CUDA(cudaMemsetAsync(c->gm.p, 0, c->gm.n * sizeof(double), c->stream));
+    DM_CUDA(cudaMemsetAsync(c->gr.p, 0, c->gr.n * sizeof(double), c->stream));
+    int64_t hv_gf = 0;
+    const int gf_prec = p.precision;
+    for (auto &st : c->states) {
+        SectorView si = sector_view(c, st.isector);
+        const double *psi = c->states64.p + st.off;
+        double weight;
+        if (c->finite_t && p.beta * (st.e - c->egs) < 200.0)
+            weight = std::exp(-p.beta * (st.e - c->egs)) / c->zeta;
+        else if (!c->finite_t)
+            weight = 1.0 / c->zeta;
+        else
+            weight = 0.0;
+        for (int ispin = 0; ispin < c->nspin; ispin++)
+            for (int iorb = 0; iorb < no; iorb++) {
+                double *gmo = c->gm.p + 2 * (size_t)(ispin * no + iorb) * p.lmats;
+                double *gro = c->gr.p + 2 * (size_t)(ispin * no + iorb) * p.lreal;
+                for (int ph = 0; ph < 2; ph++) {
+                    const bool particle = ph == 0;
+                    const int js = particle ? c->getcdgsector[2 * (st.isector - 1) + ispin]
+                                            : c->getcsector[2 * (st.isector - 1) + ispin];
+                    if (js == 0) continue;
+                    SectorView sj = sector_view(c, js);
+                    c->s64b.alloc(sj.dim);
+                    gf_apply_op(c, si, sj, iorb, ispin, particle, psi, c->s64b.p, c->red_out.p + 2);
+                    const int nl = (int)std::min<int64_t>(sj.dim, p.lanc_ngfiter);
+                    LanczosScalars lz = lz_slot(c, 1, nl);
+                    lanczos_chain(c, sj, c->s64b.p, gf_prec, lz);
+                    if (L > 0)
+                        gf_add_chain(c, lz.alpha, lz.beta, lz.status + 1, c->red_out.p + 2, weight,
+                                     st.e, particle ? 1 : -1, gmo, gro);
+                    hv_gf += nl;
+                }
+            }
+    }
+    gf_sigma(c);
+    DM_CUDA(cudaEventRecord(ev[3], c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    float ms;
+    DM_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    c->stats.ms[0] = ms;
+    DM_CUDA(cudaEventElapsedTime(&ms, ev[1], ev[2]));
+    c->stats.ms[1] = ms;
+    DM_CUDA(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+    c->stats.ms[2] = ms;
+    DM_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[3]));
+    c->stats.ms[3] = ms;
+    c->stats.hv[0] = hv_diag;
+    c->stats.hv[1] = 0;
+    c->stats.hv[2] = hv_gf;
+    for (auto &e : ev) cudaEventDestroy(e);
+    c->solved = true;
+}
+
+// (Nspin,Nspin,Norb,Norb,L) Fortran layout from the device [nspin][norb][L]
+// complex blocks (normal bath: diagonal in spin and orbital).
+static void get_gf(dmfted_ctx *c, const dmfted::DBuf<double> &d, int L, double *out) {
+    DM_REQUIRE(c->solved, DMFTED_ERR_STATE, "no solve has run on this context");
+    const int ns = c->nspin, no = c->norb;
+    std::vector<double> h(2 * (size_t)ns * no * std::max(L, 1));
+    if (L > 0)
+        DM_CUDA(cudaMemcpy(h.data(), d.p, 2 * (size_t)ns * no * L * sizeof(double),
+                           cudaMemcpyDeviceToHost));
+    const size_t tot = (size_t)ns * ns * no * no * L;
+    std::fill(out, out + 2 * tot, 0.0);
+    for (int is = 0; is < ns; is++)
+        for (int a = 0; a < no; a++)
+            for (int l = 0; l < L; l++) {
+                const size_t fi = is + ns * (is + ns * (a + (size_t)no * (a + (size_t)no * l)));
+                const size_t si = ((size_t)(is * no + a) * L + l);
+                out[2 * fi] = h[2 * si];
+                out[2 * fi + 1] = h[2 * si + 1];
+            }
+}
+
+}  // namespace dmfted
+
+using namespace dmfted;
+
+#define API_BEGIN try {
+#define API_END                                                              \
+    }                                                                        \
+    catch (const StatusError &e) {                                           \
+        return set_error(e.code, e.msg);                                     \
+    }                                                                        \
+    catch (const std::exception &e) {                                        \
+        return set_error(DMFTED_ERR_ARG, e.what());                          \
+    }                                                                        \
+    g_last_error.clear();                                                    \
+    return DMFTED_OK;
+
+extern "C" {
+
+void dmfted_default_params(dmfted_params *p) {
+    std::memset(p, 0, sizeof(*p));
+    p->norb = 1;
+    p->nbath = 6;
+    p->nspin = 1;
+    p->hfmode = 1;
+    p->jhflag = 0;
+    p->uloc[0] = 2.0;
+    p->ust = p->jh = p->jx = p->jp = 0.0;
+    p->xmu = 0.0;
+    p->beta = 1000.0;
+    p->lmats = 5000;
+    p->lreal = 5000;
+    p->wini = -5.0;
+    p->wfin = 5.0;
+    p->eps = 0.01;
+    p->lanc_niter = 512;
+    p->lanc_ngfiter = 200;
+    p->lanc_tolerance = 1e-12;
+    p->lanc_dim_threshold = 256;
+    p->lanc_nstates_sector = 6;
+    p->lanc_nstates_total = 1;
+    p->lanc_nstates_step = 2;
+    p->gs_threshold = 1e-9;
+    p->cutoff = 1e-9;
+    p->ed_twin = 0;
+    p->lfit = 1000;
+    p->cg_weight = 0;
+    p->precision = DMFTED_FP64;
+    p->lanc_ncheck = 10;
+    p->device = 0;
+    p->lanc_gf_threshold = 1e-13;
+}
+
+const char *dmfted_last_error(void) { return last_error(); }
+
+const char *dmfted_version(void) { return "dmfted-b200 0.1 (sm_100a)"; }
+
+int dmfted_get_bath_dimension(const dmfted_params *p, int32_t *nb) {
+    API_BEGIN
+    DM_REQUIRE(p && nb, DMFTED_ERR_ARG, "null argument");
+    *nb = 2 * p->nspin * p->norb * p->nbath;
+    API_END
+}
+
+int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
+    dmfted_ctx *c = nullptr;
+    try {
+        DM_REQUIRE(p && out, DMFTED_ERR_ARG, "null argument");
+        *out = nullptr;
+        DM_REQUIRE(p->norb >= 1 && p->norb <= kMaxNorb, DMFTED_ERR_UNSUPPORTED,
+                   "ED ERROR: Norb > 3 is currently not supported");
+        DM_REQUIRE(p->nspin == 1 || p->nspin == 2, DMFTED_ERR_UNSUPPORTED,
+                   "ED ERROR: Nspin > 2 is currently not supported");
+        DM_REQUIRE(p->nbath >= 0, DMFTED_ERR_ARG, "Nbath < 0");
+        const int ns = (p->nbath + 1) * p->norb;
+        DM_REQUIRE(ns <= kMaxNs, DMFTED_ERR_UNSUPPORTED, "Ns > 20 is outside this solver");
+        DM_REQUIRE(p->lmats >= 0 && p->lreal >= 0, DMFTED_ERR_ARG, "negative frequency count");
+        DM_REQUIRE(p->lanc_ngfiter >= 1 && p->lanc_ngfiter < kLzMax, DMFTED_ERR_ARG,
+                   "lanc_ngfiter out of range");
+        DM_REQUIRE(p->lanc_niter >= 1, DMFTED_ERR_ARG, "lanc_niter < 1");
+        DM_REQUIRE(p->precision == DMFTED_FP64 || p->precision == DMFTED_MIXED, DMFTED_ERR_ARG,
+                   "unknown precision mode");
+        DM_REQUIRE(!(p->jhflag && p->norb > 1 && (p->jx != 0.0 || p->jp != 0.0)),
+                   DMFTED_ERR_UNSUPPORTED,
+                   "Jhflag spin-exchange/pair-hopping is not available in this build");
+        c = new dmfted_ctx();
+        c->p = *p;
+        if (c->p.lanc_ncheck <= 0) c->p.lanc_ncheck = 10;
+        if (c->p.lanc_gf_threshold <= 0) c->p.lanc_gf_threshold = 1e-13;
+        c->norb = p->norb;
+        c->nbath = p->nbath;
+        c->nspin = p->nspin;
+        c->ns = ns;
+        c->device = p->device;
+        DM_CUDA(cudaSetDevice(c->device));
+        DM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        const size_t nh = 2 * (size_t)c->nspin * c->nspin * c->norb * c->norb;
+        c->hloc.assign(nh, 0.0);
+        if (hloc) {
+            check_hloc(c, hloc);
+            std::copy(hloc, hloc + nh, c->hloc.begin());
+        }
+        setup_pointers_normal(c);
+        fock_init(c);
+        c->red_partials.alloc((size_t)2 * 64 * kMaxRedBlocks);
+        c->red_counter.alloc(8);
+        DM_CUDA(cudaMemsetAsync(c->red_counter.p, 0, 8 * sizeof(unsigned), c->stream));
+        c->red_out.alloc(16);
+        c->lz_d.alloc((size_t)kLzSlots * kLzStride);
+        c->lz_s.alloc((size_t)kLzSlots * 8);
+        DM_CUDA(cudaMemsetAsync(c->lz_s.p, 0, kLzSlots * 8 * sizeof(int), c->stream));
+        c->coefb.alloc(kLzMax + 8);
+        // frequency grids: wm = pi/beta (2n-1) (ED_GREENS_FUNCTIONS.f90:114),
+        // wr = linspace(wini, wfin, Lreal)
+        std::vector<double> wm(std::max(p->lmats, 1)), wr(std::max(p->lreal, 1));
+        for (int i = 0; i < p->lmats; i++) wm[i] = M_PI / p->beta * (2.0 * (i + 1) - 1.0);
+        for (int i = 0; i < p->lreal; i++)
+            wr[i] = p->lreal > 1 ? p->wini + (p->wfin - p->wini) * i / (double)(p->lreal - 1)
+                                 : p->wini;
+        c->d_wm.alloc(wm.size());
+        c->d_wr.alloc(wr.size());
+        DM_CUDA(cudaMemcpyAsync(c->d_wm.p, wm.data(), wm.size() * 8, cudaMemcpyHostToDevice,
+                                c->stream));
+        DM_CUDA(cudaMemcpyAsync(c->d_wr.p, wr.data(), wr.size() * 8, cudaMemcpyHostToDevice,
+                                c->stream));
+        c->bath_e.assign((size_t)c->nspin * c->norb * c->nbath, 0.0);
+        c->bath_v.assign((size_t)c->nspin * c->norb * c->nbath, 0.0);
+        upload_model(c);
+        DM_CUDA(cudaStreamSynchronize(c->stream));
+        *out = c;
+    } catch (const StatusError &e) {
+        delete c;
+        return set_error(e.code, e.msg);
+    }
+    g_last_error.clear();
+    return DMFTED_OK;
+}
+
+int dmfted_free(dmfted_ctx *c) {
+    API_BEGIN
+    if (!c) return DMFTED_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaStream_t st = c->stream;
+    delete c;
+    if (st) cudaStreamDestroy(st);
+    API_END
+}
+
+int dmfted_set_hloc(dmfted_ctx *c, const double *hloc) {
+    API_BEGIN
+    DM_REQUIRE(c && hloc, DMFTED_ERR_ARG, "null argument");
+    DM_CUDA(cudaSetDevice(c->device));
+    check_hloc(c, hloc);
+    std::copy(hloc, hloc + c->hloc.size(), c->hloc.begin());
+    upload_model(c);
+    if (c->bath_set) fock_set_couplings(c);
+    API_END
+}
+
+int dmfted_set_bath(dmfted_ctx *c, const double *bath, int32_t nb) {
+    API_BEGIN
+    DM_REQUIRE(c && (bath || nb == 0), DMFTED_ERR_ARG, "null argument");
+    DM_CUDA(cudaSetDevice(c->device));
+    const int32_t want = 2 * c->nspin * c->norb * c->nbath;
+    DM_REQUIRE(nb == want, DMFTED_ERR_ARG, "set_dmft_bath error: wrong bath dimensions");
+    for (int i = 0; i < nb; i++)
+        DM_REQUIRE(std::isfinite(bath[i]), DMFTED_ERR_ARG, "bath has a non-finite entry");
+    // set_dmft_bath, ED_BATH/dmft_aux.f90:493-512: io = k + (iorb-1)*Nbath + (ispin-1)*Nbath*Norb
+    const int half = nb / 2;
+    std::copy(bath, bath + half, c->bath_e.begin());
+    std::copy(bath + half, bath + nb, c->bath_v.begin());
+    upload_model(c);
+    fock_set_couplings(c);
+    c->bath_set = true;
+    API_END
+}
+
+int dmfted_sector_tables(dmfted_ctx *c, int32_t *nsectors, int32_t *getsector, int32_t *getnup,
+                         int32_t *getndw, int32_t *getdim, int32_t *getdimup, int32_t *getdimdw,
+                         int32_t *getcsector, int32_t *getcdgsector, int32_t *getbathstride,
+                         int32_t *impindex) {
+    API_BEGIN
+    DM_REQUIRE(c, DMFTED_ERR_ARG, "null context");
+    auto cp = [](const std::vector<int32_t> &v, int32_t *o) {
+        if (o) std::copy(v.begin(), v.end(), o);
+    };
+    if (nsectors) *nsectors = c->nsectors;
+    cp(c->getsector, getsector);
+    cp(c->getnup, getnup);
+    cp(c->getndw, getndw);
+    cp(c->getdim, getdim);
+    cp(c->getdimup, getdimup);
+    cp(c->getdimdw, getdimdw);
+    cp(c->getcsector, getcsector);
+    cp(c->getcdgsector, getcdgsector);
+    cp(c->getbathstride, getbathstride);
+    cp(c->impindex, impindex);
+    API_END
+}
+
+int dmfted_build_sector(dmfted_ctx *c, int32_t isector, int32_t *map, int64_t dim) {
+    API_BEGIN
+    DM_REQUIRE(c && map, DMFTED_ERR_ARG, "null argument");
+    DM_CUDA(cudaSetDevice(c->device));
+    DM_REQUIRE(c->ns <= 15, DMFTED_ERR_UNSUPPORTED, "the combined map needs 2*Ns <= 31 bits");
+    SectorView s = sector_view(c, isector);
+    DM_REQUIRE(dim == s.dim, DMFTED_ERR_ARG, "build_sector: dim != getdim(isector)");
+    DBuf<int32_t> d;
+    d.alloc(std::max<int64_t>(s.dim, 1));
+    fock_build_map(c, isector, d.p);
+    DM_CUDA(cudaMemcpyAsync(map, d.p, s.dim * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    API_END
+}
+
+int dmfted_setup_hv_sector(dmfted_ctx *c, int32_t isector) {
+    API_BEGIN
+    DM_REQUIRE(c, DMFTED_ERR_ARG, "null context");
+    sector_view(c, isector);
+    c->cur_sector = isector;
+    API_END
+}
+
+int dmfted_delete_hv_sector(dmfted_ctx *c) {
+    API_BEGIN
+    DM_REQUIRE(c, DMFTED_ERR_ARG, "null context");
+    c->cur_sector = 0;
+    API_END
+}
+
+int dmfted_hxv_c128(dmfted_ctx *c, int32_t nloc, const double *v, double *hv) {
+    API_BEGIN
+    DM_REQUIRE(c && v && hv, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(c->cur_sector != 0, DMFTED_ERR_STATE, "directMatVec_cc ERROR: Hsector NOT set");
+    DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "H*v: bath not set");
+    DM_CUDA(cudaSetDevice(c->device));
+    SectorView s = sector_view(c, c->cur_sector);
+    DM_REQUIRE((int64_t)nloc == s.dim, DMFTED_ERR_ARG, "directMatVec_cc ERROR: Nloc != dim(isector)");
+    const int64_t n = s.dim;
+    c->wv64.alloc(6 * n);
+    double *z = c->wv64.p, *x = z + 2 * n, *y = x + 2 * n;
+    DM_CUDA(cudaMemcpyAsync(z, v, 2 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    k_interleave_split<<<ew(c, n), 256, 0, c->stream>>>(z, x, x + n, n);
+    DM_CHECK_LAUNCH();
+    hxv_f64(c, s, x, y, 2);
+    k_interleave_join<<<ew(c, n), 256, 0, c->stream>>>(y, y + n, z, n);
+    DM_CHECK_LAUNCH();
+    c->launches += 2;
+    DM_CUDA(cudaMemcpyAsync(hv, z, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    API_END
+}
+
+int dmfted_hxv_device_f64(dmfted_ctx *c, const double *d_v, double *d_hv, int32_t nvec) {
+    API_BEGIN
+    DM_REQUIRE(c && d_v && d_hv && nvec >= 1 && nvec <= 65535, DMFTED_ERR_ARG, "bad argument");
+    DM_REQUIRE(c->cur_sector != 0, DMFTED_ERR_STATE, "directMatVec_cc ERROR: Hsector NOT set");
+    DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "H*v: bath not set");
+    DM_CUDA(cudaSetDevice(c->device));
+    hxv_f64(c, sector_view(c, c->cur_sector), d_v, d_hv, nvec);
+    API_END
+}
+
+int dmfted_hxv_device_f32(dmfted_ctx *c, const float *d_v, float *d_hv, int32_t nvec) {
+    API_BEGIN
+    DM_REQUIRE(c && d_v && d_hv && nvec >= 1 && nvec <= 65535, DMFTED_ERR_ARG, "bad argument");
+    DM_REQUIRE(c->cur_sector != 0, DMFTED_ERR_STATE, "directMatVec_cc ERROR: Hsector NOT set");
+    DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "H*v: bath not set");
+    DM_CUDA(cudaSetDevice(c->device));
+    hxv_f32(c, sector_view(c, c->cur_sector), d_v, d_hv, nvec);
+    API_END
+}
+
+int dmfted_lanczos_gs(dmfted_ctx *c, int32_t isector, double *e0, double *psi, int32_t *niter) {
+    API_BEGIN
+    DM_REQUIRE(c && e0, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "lanczos_gs: bath not set");
+    DM_CUDA(cudaSetDevice(c->device));
+    SectorView s = sector_view(c, isector);
+    c->s64a.alloc(s.dim);
+    const int nit = (int)std::min<int64_t>(s.dim, c->p.lanc_niter);
+    LanczosResult r = lanczos_gs(c, s, c->s64a.p, nullptr, c->p.precision, c->p.lanc_tolerance, nit);
+    *e0 = r.e0;
+    if (niter) *niter = r.steps;
+    if (psi) real_to_host_c128(c, c->s64a.p, s.dim, psi);
+    API_END
+}
+
+int dmfted_lanc_tridiag(dmfted_ctx *c, int32_t isector, const double *vvinit, int32_t nlanc,
+                        double *alanc, double *blanc, int32_t *nused) {
+    API_BEGIN
+    DM_REQUIRE(c && vvinit && alanc && blanc, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(nlanc >= 1 && nlanc < kLzMax, DMFTED_ERR_ARG, "nlanc out of range");
+    DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "lanc_tridiag: bath not set");
+    DM_CUDA(cudaSetDevice(c->device));
+    SectorView s = sector_view(c, isector);
+    const int64_t n = s.dim;
+    // complex start vector -> stacked (re, im) halves: the recurrence of a real
+    // symmetric H on a complex vector is the real recurrence on the stack.
+    c->wv64.alloc(2 * n);
+    c->s64b.alloc(2 * n);
+    DM_CUDA(cudaMemcpyAsync(c->wv64.p, vvinit, 2 * n * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+    k_interleave_split<<<ew(c, n), 256, 0, c->stream>>>(c->wv64.p, c->s64b.p, c->s64b.p + n, n);
+    DM_CHECK_LAUNCH();
+    c->launches++;
+    LanczosScalars lz = lz_slot(c, 2, nlanc);
+    lanczos_chain(c, s, c->s64b.p, c->p.precision, lz, 2);
+    std::vector<double> b(nlanc + 1);
+    int st[8];
+    DM_CUDA(cudaMemcpyAsync(alanc, lz.alpha, nlanc * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    DM_CUDA(cudaMemcpyAsync(b.data(), lz.beta, (nlanc + 1) * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    DM_CUDA(cudaMemcpyAsync(st, lz.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    const int used = st[1];
+    // steps never taken keep a = b = 0, as the zero-initialised arrays of the
+    // reference's early exit do (.repo/PLAIN_LANCZOS.f90:164-179)
+    for (int k = used; k < nlanc; k++) alanc[k] = 0.0;
+    blanc[0] = 0.0;
+    for (int k = 1; k < nlanc; k++) blanc[k] = k <= used ? b[k] : 0.0;
+    if (nused) *nused = used;
+    API_END
+}
+
+int dmfted_ed_solve(dmfted_ctx *c, const double *bath, int32_t nb, const int32_t *sectors,
+                    int32_t nsectors) {
+    API_BEGIN
+    DM_REQUIRE(c, DMFTED_ERR_ARG, "null context");
+    DM_CUDA(cudaSetDevice(c->device));
+    if (bath) {
+        const int rc = dmfted_set_bath(c, bath, nb);
+        if (rc != DMFTED_OK) return rc;
+    }
+    ed_solve_impl(c, sectors, nsectors);
+    API_END
+}
+
+int dmfted_get_gimp_matsubara(dmfted_ctx *c, double *g) {
+    API_BEGIN
+    DM_REQUIRE(c && g, DMFTED_ERR_ARG, "null argument");
+    get_gf(c, c->gm, c->p.lmats, g);
+    API_END
+}
+int dmfted_get_gimp_real(dmfted_ctx *c, double *g) {
+    API_BEGIN
+    DM_REQUIRE(c && g, DMFTED_ERR_ARG, "null argument");
+    get_gf(c, c->gr, c->p.lreal, g);
+    API_END
+}
+int dmfted_get_sigma_matsubara(dmfted_ctx *c, double *s) {
+    API_BEGIN
+    DM_REQUIRE(c && s, DMFTED_ERR_ARG, "null argument");
+    get_gf(c, c->sm, c->p.lmats, s);
+    API_END
+}
+int dmfted_get_sigma_real(dmfted_ctx *c, double *s) {
+    API_BEGIN
+    DM_REQUIRE(c && s, DMFTED_ERR_ARG, "null argument");
+    get_gf(c, c->sr, c->p.lreal, s);
+    API_END
+}
+int dmfted_get_g0imp_matsubara(dmfted_ctx *c, double *g) {
+    API_BEGIN
+    DM_REQUIRE(c && g, DMFTED_ERR_ARG, "null argument");
+    get_gf(c, c->g0m, c->p.lmats, g);
+    API_END
+}
+
+int dmfted_get_observables(dmfted_ctx *c, double *dens, double *dens_up, double *dens_dw,
+                           double *docc, double *magz) {
+    API_BEGIN
+    DM_REQUIRE(c, DMFTED_ERR_ARG, "null context");
+    DM_REQUIRE(c->solved, DMFTED_ERR_STATE, "no solve has run on this context");
+    const int no = c->norb;
+    double *outs[5] = {dens, dens_up, dens_dw, docc, magz};
+    for (int k = 0; k < 5; k++)
+        if (outs[k]) std::copy(c->obs.begin() + k * no, c->obs.begin() + (k + 1) * no, outs[k]);
+    API_END
+}
+
+int dmfted_get_eigenspace(dmfted_ctx *c, int32_t cap, double *energies, int32_t *sectors,
+                          int32_t *nstates, double *zeta) {
+    API_BEGIN
+    DM_REQUIRE(c, DMFTED_ERR_ARG, "null context");
+    DM_REQUIRE(c->solved, DMFTED_ERR_STATE, "no solve has run on this context");
+    const int n = (int)c->states.size();
+    if (nstates) *nstates = n;
+    if (zeta) *zeta = c->zeta;
+    for (int i = 0; i < std::min(n, cap); i++) {
+        if (energies) energies[i] = c->states[i].e;
+        if (sectors) sectors[i] = c->states[i].isector;
+    }
+    API_END
+}
+
+int dmfted_get_egs(dmfted_ctx *c, double *egs) {
+    API_BEGIN
+    DM_REQUIRE(c && egs, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(c->solved, DMFTED_ERR_STATE, "no solve has run on this context");
+    *egs = c->egs;
+    API_END
+}
+
+int dmfted_hf_gradient(dmfted_ctx *c, double *grad, int32_t nb) {
+    API_BEGIN
+    DM_REQUIRE(c && grad, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(c->solved, DMFTED_ERR_STATE, "no solve has run on this context");
+    const int no = c->norb, nbth = c->nbath, ns = c->nspin;
+    DM_REQUIRE(nb == 2 * ns * no * nbth, DMFTED_ERR_ARG, "hf_gradient: wrong bath dimensions");
+    const int pv = no * nbth;
+    const double *nk = c->hf_terms.data();           // [2][norb][nbath]
+    const double *hop = c->hf_terms.data() + 2 * pv;  // [2][norb][nbath]
+    for (int is = 0; is < ns; is++)
+        for (int a = 0; a < no; a++)
+            for (int k = 0; k < nbth; k++) {
+                const int io = k + a * nbth + is * nbth * no;
+                const int p = a * nbth + k;
+                double de, dv;
+                if (ns == 1) {
+                    de = nk[p] + nk[pv + p];
+                    dv = hop[p] + hop[pv + p];
+                } else {
+                    de = nk[is * pv + p];
+                    dv = hop[is * pv + p];
+                }
+                grad[io] = de;
+                grad[ns * no * nbth + io] = dv;
+            }
+    API_END
+}
+
+int dmfted_chi2_delta_batch_device(dmfted_ctx *c, int32_t nbatch, int32_t nbath, int32_t L,
+                                   const double *d_a, const double *d_xdelta, const double *d_g,
+                                   const double *d_w, double *d_chi2, double *d_grad) {
+    API_BEGIN
+    DM_REQUIRE(c && d_a && d_xdelta && d_g && d_w && d_chi2, DMFTED_ERR_ARG, "null argument");
+    DM_CUDA(cudaSetDevice(c->device));
+    chi2_batch_device(c, nbatch, nbath, L, d_a, d_xdelta, d_g, d_w, d_chi2, d_grad);
+    API_END
+}
+
+int dmfted_chi2_delta_batch(dmfted_ctx *c, int32_t nbatch, int32_t nbath, int32_t L,
+                            const double *a, const double *xdelta, const double *g,
+                            const double *w, double *chi2, double *grad) {
+    API_BEGIN
+    DM_REQUIRE(c && a && xdelta && g && w && chi2, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(nbatch > 0 && nbath > 0 && L > 0, DMFTED_ERR_ARG, "chi2: empty batch or grid");
+    DM_CUDA(cudaSetDevice(c->device));
+    const size_t na = (size_t)nbatch * 2 * nbath;
+    DBuf<double> buf;
+    buf.alloc(na + L + 2 * (size_t)L + L + nbatch + na);
+    double *da = buf.p, *dx = da + na, *dg = dx + L, *dw = dg + 2 * (size_t)L, *dc = dw + L,
+           *dgr = dc + nbatch;
+    DM_CUDA(cudaMemcpyAsync(da, a, na * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dx, xdelta, (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dg, g, 2 * (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dw, w, (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
+    chi2_batch_device(c, nbatch, nbath, L, da, dx, dg, dw, dc, grad ? dgr : nullptr);
+    DM_CUDA(cudaMemcpyAsync(chi2, dc, nbatch * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (grad) DM_CUDA(cudaMemcpyAsync(grad, dgr, na * 8, cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    API_END
+}
+
+int dmfted_time_hxv(dmfted_ctx *c, int32_t fp32, int32_t warmup, int32_t reps, double *ms) {
+    API_BEGIN
+    DM_REQUIRE(c && ms && reps >= 1 && warmup >= 0, DMFTED_ERR_ARG, "bad argument");
+    DM_REQUIRE(c->cur_sector != 0, DMFTED_ERR_STATE, "time_hxv: Hsector NOT set");
+    DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "time_hxv: bath not set");
+    DM_CUDA(cudaSetDevice(c->device));
+    SectorView s = sector_view(c, c->cur_sector);
+    const size_t es = fp32 ? 4 : 8;
+    c->chainbuf.alloc(2 * (size_t)s.dim * es);
+    DM_CUDA(cudaMemsetAsync(c->chainbuf.p, 0, 2 * (size_t)s.dim * es, c->stream));
+    void *x = c->chainbuf.p, *y = c->chainbuf.p + (size_t)s.dim * es;
+    auto run = [&]() {
+        if (fp32) hxv_f32(c, s, (const float *)x, (float *)y, 1);
+        else hxv_f64(c, s, (const double *)x, (double *)y, 1);
+    };
+    for (int i = 0; i < warmup; i++) run();
+    cudaEvent_t e0, e1;
+    DM_CUDA(cudaEventCreate(&e0));
+    DM_CUDA(cudaEventCreate(&e1));
+    DM_CUDA(cudaEventRecord(e0, c->stream));
+    for (int i = 0; i < reps; i++) run();
+    DM_CUDA(cudaEventRecord(e1, c->stream));
+    DM_CUDA(cudaEventSynchronize(e1));
+    float t;
+    DM_CUDA(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = t / reps;
+    API_END
+}
+
+int dmfted_get_timings(dmfted_ctx *c, double *t, int64_t *n) {
+    API_BEGIN
+    DM_REQUIRE(c, DMFTED_ERR_ARG, "null context");
+    if (t)
+        for (int i = 0; i < 4; i++) t[i] = c->stats.ms[i];
+    if (n)
+        for (int i = 0; i < 3; i++) n[i] = c->stats.hv[i];
+    API_END
+}
+
+int dmfted_launch_count(dmfted_ctx *c, int64_t *count, int32_t reset) {
+    API_BEGIN
+    DM_REQUIRE(c && count, DMFTED_ERR_ARG, "null argument");
+    *count = c->launches;
+    if (reset) c->launches = 0;
+    API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,300 @@
+// Fock-space tables: sector enumeration, ranks, the combined sector map and
+// the spin-resolved hopping (ELL) and diagonal tables.
+//
+// The reference enumerates a sector by scanning all 2^Ns x 2^Ns words and
+// keeping popcount matches (build_sector, ED_SETUP.f90:874-891), then finds
+// every hopping target with a recursive binary search over the combined map
+// (binary_search, ED_SETUP.f90:1282-1299).  Here the words of each popcount
+// class are produced directly by combinatorial unranking (the r-th word of
+// popcount n in increasing order), and the inverse map is a 2^Ns rank table,
+// so target indices are one table load.  Both give the reference's order:
+// for a fixed popcount, increasing integer order is colex order, whose rank
+// is sum_i C(c_i, i) over the set-bit positions c_1 < ... < c_n.
+#include <algorithm>
+#include <cstring>
+
+#include "internal.cuh"
+
+namespace dmfted {
+
+__constant__ int64_t c_binom[(kMaxNs + 1) * (kMaxNs + 1)];  // C(b, i) at b*(kMaxNs+1)+i
+__constant__ int64_t c_class_off[kMaxNs + 2];
+
+__device__ __forceinline__ int64_t binom_d(int b, int i) {
+    return (i < 0 || b < 0 || i > b) ? 0 : c_binom[b * (kMaxNs + 1) + i];
+}
+
+// K1a: words[g] for every g in [0, 2^Ns) and the rank table.
+__global__ void k_words(int ns, uint32_t *words, int32_t *rank) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= ((int64_t)1 << ns)) return;
+    int n = 0;
+    while (c_class_off[n + 1] <= g) n++;
+    int64_t r = g - c_class_off[n];
+    int64_t rr = r;
+    uint32_t w = 0;
+    int b = ns - 1;
+    for (int i = n; i >= 1; i--) {
+        while (binom_d(b, i) > rr) b--;
+        w |= 1u << b;
+        rr -= binom_d(b, i);
+        b--;
+    }
+    words[g] = w;
+    rank[w] = (int32_t)r;
+}
+
+// Parity of the occupied levels strictly between positions p and q.
+__device__ __forceinline__ uint32_t between_parity(uint32_t w, int p, int q) {
+    int lo = p < q ? p : q, hi = p < q ? q : p;
+    uint32_t mask = ((1u << hi) - 1u) & ~((2u << lo) - 1u);
+    return __popc(w & mask) & 1u;
+}
+
+// K2: hopping table of one spin for every word.  Entry order per word follows
+// the reference's row loop: Hloc inter-orbital hopping (HxVimp.f90:16-49,
+// iorb outer, jorb inner), then impurity<->bath hybridisation
+// (HxVimp_bath.f90:1-38, iorb outer, kp inner; imp->bath when the impurity
+// level is occupied and the bath level empty, bath->imp in the opposite
+// case).  Couplings equal to zero are skipped, as the reference's
+// `if(... /= 0)` conditions do.  The sign of c^+_p c_q is (-1)^(occupied
+// levels strictly between p and q), the product of the two c/cdg signs of
+// ED_SETUP.f90:1055-1081 (levels below the lower position cancel).
+// Also writes the bath-energy part of the diagonal, sum_k e_k n_k
+// (HxVbath.f90:1-13).
+__global__ void k_ell_build(int ns, int norb, int nbath, int W, const uint32_t *words,
+                            const int32_t *rank, const double *par, const double *ebath,
+                            uint8_t *cnt, uint32_t *ell, double *diag, float *diag_f) {
+    int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= ((int64_t)1 << ns)) return;
+    int n = 0;
+    while (c_class_off[n + 1] <= g) n++;
+    const int64_t off = c_class_off[n];
+    const int64_t r = g - off;
+    const int64_t rows = binom_d(ns, n);
+    uint32_t *erow = ell + (int64_t)W * off + r;
+    const uint32_t w = words[g];
+    int e = 0;
+    const int pv = norb * nbath;
+    for (int a = 0; a < norb; a++)
+        for (int b = 0; b < norb; b++) {
+            if (a == b) continue;
+            const int p = pv + a * norb + b;
+            if (par[p] == 0.0) continue;
+            if (((w >> b) & 1u) && !((w >> a) & 1u)) {
+                uint32_t t = (w & ~(1u << b)) | (1u << a);
+                erow[(int64_t)e * rows] = ell_pack((uint32_t)rank[t], p, between_parity(w, a, b));
+                e++;
+            }
+        }
+    for (int a = 0; a < norb; a++)
+        for (int k = 0; k < nbath; k++) {
+            const int p = a * nbath + k;
+            if (par[p] == 0.0) continue;
+            const int ms = norb + a * nbath + k;
+            const uint32_t ia = (w >> a) & 1u, ib = (w >> ms) & 1u;
+            if (ia != ib) {
+                uint32_t t = w ^ (1u << a) ^ (1u << ms);
+                erow[(int64_t)e * rows] = ell_pack((uint32_t)rank[t], p, between_parity(w, a, ms));
+                e++;
+            }
+        }
+    cnt[g] = (uint8_t)e;
+    double d = 0.0;
+    for (int a = 0; a < norb; a++)
+        for (int k = 0; k < nbath; k++) {
+            const int ms = norb + a * nbath + k;
+            if ((w >> ms) & 1u) d += ebath[a * nbath + k];
+        }
+    diag[g] = d;
+    diag_f[g] = (float)d;
+}
+
+// Combined sector map (ED_SETUP.f90:880-890): map[i] = iup + idw*2^Ns with
+// i = rank_up + DimUp*rank_dw.
+__global__ void k_build_map(int ns, int64_t dimup, int64_t dim, const uint32_t *wu,
+                            const uint32_t *wd, int32_t *map) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= dim) return;
+    int64_t r = i % dimup, c = i / dimup;
+    map[i] = (int32_t)(wu[r] | (wd[c] << ns));
+}
+
+static int64_t exact_binom(int n, int k) {
+    if (k < 0 || k > n) return 0;
+    int64_t r = 1;
+    for (int i = 1; i <= k; i++) r = r * (n + 1 - i) / i;
+    return r;
+}
+
+void fock_init(dmfted_ctx *c) {
+    const int ns = c->ns;
+    std::vector<int64_t> bt((kMaxNs + 1) * (kMaxNs + 1), 0);
+    for (int b = 0; b <= kMaxNs; b++)
+        for (int i = 0; i <= b; i++) bt[b * (kMaxNs + 1) + i] = exact_binom(b, i);
+    c->binom.assign(ns + 1, 0);
+    c->class_off.assign(kMaxNs + 2, 0);
+    for (int n = 0; n <= ns; n++) c->binom[n] = exact_binom(ns, n);
+    for (int n = 0; n <= kMaxNs; n++)
+        c->class_off[n + 1] = c->class_off[n] + (n <= ns ? c->binom[n] : 0);
+    // classes beyond ns are empty; keep offsets monotone so the class search stops
+    DM_CUDA(cudaMemcpyToSymbolAsync(c_binom, bt.data(), bt.size() * sizeof(int64_t), 0,
+                                    cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyToSymbolAsync(c_class_off, c->class_off.data(),
+                                    c->class_off.size() * sizeof(int64_t), 0,
+                                    cudaMemcpyHostToDevice, c->stream));
+    c->nwords = (int64_t)1 << ns;
+    c->words.alloc(c->nwords);
+    c->rank.alloc(c->nwords);
+    k_words<<<div_up(c->nwords, 256), 256, 0, c->stream>>>(ns, c->words.p, c->rank.p);
+    DM_CHECK_LAUNCH();
+    c->launches++;
+    c->W = c->norb * c->nbath + c->norb * (c->norb - 1);
+    c->P = c->norb * c->nbath + c->norb * c->norb;
+    DM_REQUIRE(c->W <= kMaxW && c->P <= kMaxParams, DMFTED_ERR_UNSUPPORTED,
+               "too many couplings per level for the packed hopping table");
+    c->spin_shared = (c->nspin == 1);
+    const int nsp = c->spin_shared ? 1 : 2;
+    for (int s = 0; s < nsp; s++) {
+        SpinTables &t = c->spin[s];
+        t.cnt.alloc(c->nwords);
+        t.ell.alloc((size_t)std::max(c->W, 1) * c->nwords);
+        t.diag.alloc(c->nwords);
+        t.diag_f.alloc(c->nwords);
+        t.par.alloc(c->P);
+        t.par_f.alloc(c->P);
+    }
+    const int ni = 1 << c->norb;
+    c->dint.alloc(ni * ni);
+    c->dint_f.alloc(ni * ni);
+}
+
+// Impurity-only part of the diagonal as a function of the impurity occupations
+// (iu, id bit sets of length Norb): HxVimp.f90:1-12 (-xmu*n + Hloc_aa*n, impurity
+// levels only) and HxVint.f90:1-43 (U, Ust, Ust-Jh and the HFMODE shift).
+static double impurity_diag(const dmfted_ctx *c, unsigned iu, unsigned id) {
+    const int norb = c->norb, nsp = c->nspin;
+    double nu[kMaxNorb], nd[kMaxNorb];
+    for (int a = 0; a < norb; a++) {
+        nu[a] = (iu >> a) & 1u;
+        nd[a] = (id >> a) & 1u;
+    }
+    auto hl = [&](int is, int a) {
+        int64_t idx = is + nsp * (is + nsp * (a + (int64_t)norb * a));
+        return c->hloc[2 * idx];
+    };
+    double h = 0.0, sn = 0.0;
+    for (int a = 0; a < norb; a++) sn += nu[a] + nd[a];
+    h -= c->p.xmu * sn;
+    for (int a = 0; a < norb; a++) {
+        h += hl(0, a) * nu[a];
+        h += hl(nsp - 1, a) * nd[a];
+    }
+    const double *U = c->p.uloc;
+    const double ust = c->p.ust, jh = c->p.jh;
+    for (int a = 0; a < norb; a++) h += U[a] * nu[a] * nd[a];
+    if (norb > 1) {
+        for (int a = 0; a < norb; a++)
+            for (int b = a + 1; b < norb; b++) h += ust * (nu[a] * nd[b] + nu[b] * nd[a]);
+        for (int a = 0; a < norb; a++)
+            for (int b = a + 1; b < norb; b++) h += (ust - jh) * (nu[a] * nu[b] + nd[a] * nd[b]);
+    }
+    if (c->p.hfmode) {
+        for (int a = 0; a < norb; a++) h += -0.5 * U[a] * (nu[a] + nd[a]) + 0.25 * U[a];
+        if (norb > 1)
+            for (int a = 0; a < norb; a++)
+                for (int b = a + 1; b < norb; b++) {
+                    const double nab = nu[a] + nd[a] + nu[b] + nd[b];
+                    h += -0.5 * ust * nab + 0.25 * ust;
+                    h += -0.5 * (ust - jh) * nab + 0.25 * (ust - jh);
+                }
+    }
+    return h;
+}
+
+void fock_set_couplings(dmfted_ctx *c) {
+    const int norb = c->norb, nbath = c->nbath, nsp = c->nspin;
+    const int nsp_tab = c->spin_shared ? 1 : 2;
+    for (int s = 0; s < nsp_tab; s++) {
+        // spin s of the tables uses bath spin index s (0 -> ispin=1, 1 -> ispin=Nspin)
+        const int bs = (s == 0) ? 0 : nsp - 1;
+        std::vector<double> par(c->P, 0.0), eb((size_t)norb * nbath, 0.0);
+        std::vector<float> parf(c->P, 0.f);
+        for (int a = 0; a < norb; a++)
+            for (int k = 0; k < nbath; k++) {
+                par[a * nbath + k] = c->bath_v[((size_t)bs * norb + a) * nbath + k];
+                eb[a * nbath + k] = c->bath_e[((size_t)bs * norb + a) * nbath + k];
+            }
+        for (int a = 0; a < norb; a++)
+            for (int b = 0; b < norb; b++) {
+                int64_t idx = bs + nsp * (bs + nsp * (a + (int64_t)norb * b));
+                par[norb * nbath + a * norb + b] = (a == b) ? 0.0 : c->hloc[2 * idx];
+            }
+        for (int q = 0; q < c->P; q++) parf[q] = (float)par[q];
+        SpinTables &t = c->spin[s];
+        DM_CUDA(cudaMemcpyAsync(t.par.p, par.data(), c->P * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream));
+        DM_CUDA(cudaMemcpyAsync(t.par_f.p, parf.data(), c->P * sizeof(float), cudaMemcpyHostToDevice,
+                                c->stream));
+        DBuf<double> d_eb;
+        d_eb.alloc(std::max<size_t>(eb.size(), 1));
+        DM_CUDA(cudaMemcpyAsync(d_eb.p, eb.data(), eb.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream));
+        k_ell_build<<<div_up(c->nwords, 256), 256, 0, c->stream>>>(
+            c->ns, norb, nbath, std::max(c->W, 1), c->words.p, c->rank.p, t.par.p, d_eb.p, t.cnt.p,
+            t.ell.p, t.diag.p, t.diag_f.p);
+        DM_CHECK_LAUNCH();
+        c->launches++;
+        DM_CUDA(cudaStreamSynchronize(c->stream));
+        d_eb.release();
+    }
+    const int ni = 1 << norb;
+    std::vector<double> di(ni * ni);
+    std::vector<float> df(ni * ni);
+    for (int iu = 0; iu < ni; iu++)
+        for (int id = 0; id < ni; id++) {
+            di[iu * ni + id] = impurity_diag(c, iu, id);
+            df[iu * ni + id] = (float)di[iu * ni + id];
+        }
+    DM_CUDA(cudaMemcpyAsync(c->dint.p, di.data(), di.size() * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+    DM_CUDA(cudaMemcpyAsync(c->dint_f.p, df.data(), df.size() * sizeof(float), cudaMemcpyHostToDevice,
+                            c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+SectorView sector_view(const dmfted_ctx *c, int isector) {
+    DM_REQUIRE(isector >= 1 && isector <= c->nsectors, DMFTED_ERR_ARG,
+               "sector index out of range: " + std::to_string(isector));
+    SectorView s;
+    s.isector = isector;
+    s.nup = c->getnup[isector - 1];
+    s.ndw = c->getndw[isector - 1];
+    s.dimup = c->binom[s.nup];
+    s.dimdw = c->binom[s.ndw];
+    s.dim = s.dimup * s.dimdw;
+    s.offup = c->class_off[s.nup];
+    s.offdw = c->class_off[s.ndw];
+    return s;
+}
+
+void fock_build_map(dmfted_ctx *c, int isector, int32_t *d_map) {
+    SectorView s = sector_view(c, isector);
+    k_build_map<<<div_up(s.dim, 256), 256, 0, c->stream>>>(c->ns, s.dimup, s.dim,
+                                                            c->words.p + s.offup,
+                                                            c->words.p + s.offdw, d_map);
+    DM_CHECK_LAUNCH();
+    c->launches++;
+}
+
+int num_sms(dmfted_ctx *c) {
+    static int cached[64] = {0};
+    int d = c->device;
+    if (d >= 0 && d < 64 && cached[d]) return cached[d];
+    int v = 0;
+    DM_CUDA(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d));
+    if (d >= 0 && d < 64) cached[d] = v;
+    return v;
+}
+
+}  // namespace dmfted

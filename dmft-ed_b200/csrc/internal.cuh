@@ -1,0 +1,261 @@
+// Internal declarations of the B200 exact-diagonalization library.
+//
+// Device layout (one context per process/GPU):
+//   Fock tables, built once per dmfted_init, for ALL popcount classes n of
+//   Ns-bit words (2^Ns words in total):
+//     words[class_off[n] + r]   r-th Ns-bit word with popcount n, increasing
+//     rank[w]                   r such that words[class_off[popcount w] + r] == w
+//   Hopping tables per spin, rebuilt on every set_bath (they skip zero
+//   couplings as the reference's `if(V/=0)` tests do):
+//     cnt[class_off[n] + r]     hops of word r
+//     ell[W*class_off[n] + e*C(Ns,n) + r]  packed hop e of word r (ELL,
+//                               row-contiguous so a warp reads 32 rows at once)
+//     diag[class_off[n] + r]    sum_k e_k n_k of the word (bath energies)
+//   A sector (nup, ndw) is a view: rows = class nup of the up tables,
+//   columns = class ndw of the down tables.  A sector vector is the
+//   DimUp x DimDw column-major matrix V[iup + DimUp*idw], which is exactly
+//   the reference's H%map order (ED_SETUP.f90:880-890).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/dmfted.h"
+
+namespace dmfted {
+
+constexpr int kMaxNs = 20;     // 2^20 words; rank fits the 20-bit ELL field
+constexpr int kMaxNorb = 3;    // ED_SETUP.f90:275
+constexpr int kMaxParams = 256;
+constexpr int kMaxW = 64;      // hops per word (Norb*Nbath + Norb*(Norb-1))
+constexpr int kRedThreads = 256;
+constexpr int kMaxRedBlocks = 4096;
+
+// Packed ELL entry: bits 0..19 target rank, 20..27 coupling index, 31 sign.
+__host__ __device__ inline uint32_t ell_pack(uint32_t col, uint32_t par, uint32_t neg) {
+    return col | (par << 20) | (neg << 31);
+}
+__host__ __device__ inline uint32_t ell_col(uint32_t e) { return e & 0xFFFFFu; }
+__host__ __device__ inline uint32_t ell_par(uint32_t e) { return (e >> 20) & 0xFFu; }
+__host__ __device__ inline bool ell_neg(uint32_t e) { return (e >> 31) != 0u; }
+
+struct StatusError {
+    int code;
+    std::string msg;
+};
+
+// Set the thread-local last error and return code.
+int set_error(int code, const std::string &msg);
+const char *last_error();
+
+#define DM_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            throw ::dmfted::StatusError{DMFTED_ERR_CUDA,                                \
+                                        std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+#define DM_CHECK_LAUNCH() DM_CUDA(cudaGetLastError())
+
+#define DM_REQUIRE(cond, code, msg)                                  \
+    do {                                                             \
+        if (!(cond)) throw ::dmfted::StatusError{(code), (msg)};     \
+    } while (0)
+
+// A device buffer owned by the context (freed with it).  Grow-only: alloc()
+// keeps the current allocation when it is large enough.
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        if (count == 0) return;
+        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            (void)cudaGetLastError();
+            p = nullptr;
+            n = 0;
+            throw StatusError{DMFTED_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e) +
+                                                    " (" + std::to_string(count * sizeof(T)) +
+                                                    " bytes)"};
+        }
+        n = count;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// Spin-resolved hopping/diagonal tables (device).
+struct SpinTables {
+    DBuf<uint8_t> cnt;
+    DBuf<uint32_t> ell;
+    DBuf<double> diag;
+    DBuf<float> diag_f;
+    DBuf<double> par;  // [P] coupling values (V_{a,k}, then Re Hloc_{ab})
+    DBuf<float> par_f;
+};
+
+// Lanczos scalar block on the device.  alpha[k], beta[k] (beta[0] = 0),
+// scale[k] = 1/|s_k| of the stored (unnormalised) vector s_k, and
+// status ints: [0] done, [1] steps completed, [2] converged.
+struct LanczosScalars {
+    double *alpha, *beta, *scale, *ritz;  // ritz[0]=last E0, ritz[1]=previous
+    int *status;
+    int kmax;
+};
+
+// A sector as seen by the kernels.
+struct SectorView {
+    int isector;  // 1-based
+    int nup, ndw;
+    int64_t dimup, dimdw, dim;
+    int64_t offup, offdw;  // class offsets into word-indexed arrays
+};
+
+// Per-phase timing / counting of the last solve.
+struct SolveStats {
+    double ms[4] = {0, 0, 0, 0};
+    int64_t hv[3] = {0, 0, 0};
+};
+
+}  // namespace dmfted
+
+struct dmfted_ctx {
+    dmfted_params p{};
+    int ns = 0, norb = 0, nbath = 0, nspin = 0;
+    int nsectors = 0;
+    int W = 0;  // ELL width
+    int P = 0;  // couplings per spin
+    int64_t nwords = 0;
+    std::vector<int64_t> class_off;  // size ns+2
+    std::vector<int64_t> binom;      // C(ns, n), n = 0..ns (exact integers)
+    // host sector tables (1-based, as the reference)
+    std::vector<int32_t> getsector, getnup, getndw, getdim, getdimup, getdimdw, getcsector,
+        getcdgsector, getbathstride, impindex;
+    std::vector<uint8_t> twin_mask;
+    std::vector<int32_t> neigen_sector;
+    // model
+    std::vector<double> bath_e, bath_v;  // [nspin][norb][nbath]
+    std::vector<double> hloc;            // complex (re,im), Fortran order
+    bool bath_set = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    // device Fock tables
+    dmfted::DBuf<uint32_t> words;
+    dmfted::DBuf<int32_t> rank;
+    dmfted::DBuf<int64_t> d_class_off;
+    dmfted::SpinTables spin[2];
+    bool spin_shared = true;  // Nspin == 1: down tables alias the up tables
+    dmfted::DBuf<double> dint;  // [(1<<norb)^2] impurity-only diagonal
+    dmfted::DBuf<float> dint_f;
+    // reduction scratch and Lanczos scalars
+    dmfted::DBuf<double> red_partials;  // grid-reduction (hi, lo) pairs
+    dmfted::DBuf<unsigned> red_counter;  // ticket counters (left at 0)
+    dmfted::DBuf<double> red_out;        // small result slots
+    dmfted::DBuf<double> lz_d;           // Lanczos scalar slots
+    dmfted::DBuf<int> lz_s;              // Lanczos status slots
+    dmfted::DBuf<double> coefb;          // Ritz coefficients
+    // current sector of the procedure-pointer H*v
+    int cur_sector = 0;
+    // work vectors (grown on demand)
+    dmfted::DBuf<double> wv64;            // compatibility-mode H*v vectors
+    dmfted::DBuf<uint8_t> work;           // Krylov basis of the ground-state iteration
+    dmfted::DBuf<uint8_t> chainbuf;       // rotating vectors of a GF chain
+    dmfted::DBuf<double> s64a, s64b, s64c;  // sector-sized FP64 scratch
+    double mixed_tol32 = 1e-6;            // FP32-phase stopping tolerance of the mixed form
+    dmfted::DBuf<double> d_wm, d_wr;      // Matsubara / real-axis grids
+    dmfted::DBuf<double> d_bath_e, d_bath_v, d_hloc_aa;  // [nspin][norb][nbath], [nspin][norb]
+    dmfted::DBuf<double> obs_d;           // observable accumulators of one state
+    int64_t launches = 0;
+    // results of the last solve (device and host)
+    struct State {
+        double e;
+        int isector;
+        int64_t off;  // offset (elements) of the vector in states64
+    };
+    std::vector<State> states;  // energy-ordered eigenspace
+    dmfted::DBuf<double> states64;
+    double zeta = 1.0, egs = 0.0;
+    bool finite_t = false;
+    dmfted::DBuf<double> gm, gr, g0m, sm, sr;  // complex (nspin,norb,L) blocks
+    std::vector<double> obs;                   // dens, up, dw, docc, magz (norb each)
+    std::vector<double> hf_terms;              // nk[2][norb][nbath], hop[2][norb][nbath]
+    dmfted::SolveStats stats;
+    bool solved = false;
+};
+
+namespace dmfted {
+
+// ---- fock.cu -------------------------------------------------------------
+void fock_init(dmfted_ctx *c);              // words, rank, class offsets
+void fock_set_couplings(dmfted_ctx *c);     // cnt/ell/diag/par for both spins, dint
+SectorView sector_view(const dmfted_ctx *c, int isector);
+void fock_build_map(dmfted_ctx *c, int isector, int32_t *d_map);  // combined map
+
+// ---- hxv.cu --------------------------------------------------------------
+// y = H x for nvec vectors of sector s (plain product).
+void hxv_f64(dmfted_ctx *c, const SectorView &s, const double *x, double *y, int nvec);
+void hxv_f32(dmfted_ctx *c, const SectorView &s, const float *x, float *y, int nvec);
+
+// ---- lanczos.cu ------------------------------------------------------------
+constexpr int kLzMax = 1024;                  // max steps of one recurrence
+constexpr int kLzStride = 3 * (kLzMax + 2) + 4;
+constexpr int kLzSlots = 4;
+LanczosScalars lz_slot(dmfted_ctx *c, int slot, int kmax);
+template <typename T>
+void hxv_lanczos_step(dmfted_ctx *c, const SectorView &s, const T *x, const T *xprev, T *y,
+                      const LanczosScalars &lz, int k, int nstack = 1);
+struct LanczosResult {
+    double e0;
+    int steps;
+    bool converged;
+};
+// Ground state of sector s.  psi (device, length dim, float64) receives the
+// normalised Ritz vector.  start: optional device float64 start vector.
+LanczosResult lanczos_gs(dmfted_ctx *c, const SectorView &s, double *psi, const double *start,
+                         int precision, double tol, int nitermax);
+// Queue the tridiagonalisation of a chain from device vector v0 (float64, any
+// norm) into scalar slot lz (kmax = nlanc).  Asynchronous.
+// nstack = 2 runs a complex vector as its stacked re/im halves (length 2*dim).
+void lanczos_chain(dmfted_ctx *c, const SectorView &s, const double *v0, int precision,
+                   const LanczosScalars &lz, int nstack = 1);
+
+// ---- gf.cu ---------------------------------------------------------------
+// vv = c^+_{iorb,ispin} psi (particle) or c psi (hole) in sector sj;
+// |vv|^2 -> *d_norm2 (device).  Asynchronous.
+void gf_apply_op(dmfted_ctx *c, const SectorView &si, const SectorView &sj, int iorb, int ispin,
+                 bool particle, const double *psi, double *vv, double *d_norm2);
+// G(z) += weight * norm2 * CF(z) on the Lmats and Lreal grids.
+void gf_add_chain(dmfted_ctx *c, const double *d_alpha, const double *d_beta, const int *d_n,
+                  const double *d_norm2, double weight, double ei, int isign, double *gm,
+                  double *gr);
+void gf_sigma(dmfted_ctx *c);  // impSmats/impSreal/impG0mats from impG*
+
+// ---- observables.cu --------------------------------------------------------
+int obs_count(const dmfted_ctx *c);
+void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, double *d_out);
+
+// ---- chi2.cu -------------------------------------------------------------
+void chi2_batch_device(dmfted_ctx *c, int nbatch, int nbath, int L, const double *a,
+                       const double *x, const double *g, const double *w, double *chi2,
+                       double *grad);
+
+// ---- small helpers ------------------------------------------------------------
+inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
+int num_sms(dmfted_ctx *c);
+
+}  // namespace dmfted

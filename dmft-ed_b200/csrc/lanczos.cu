@@ -1,0 +1,529 @@
+// Device-resident Lanczos: ground state (stands in for SciFortran's sp_eigh
+// with Neigen=1, ED_DIAG.f90:169-183) and the three-term tridiagonalisation of
+// the Green's-function chains (sp_lanc_tridiag, build_gf_normal.f90:118-127).
+//
+// The recurrence is the plain three-term Lanczos of
+// .repo/PLAIN_LANCZOS.f90:87-118:
+//     u = H v_k - b_k v_{k-1};  a_k = <v_k, u>;  w = u - a_k v_k;
+//     b_{k+1} = |w|;  v_{k+1} = w / b_{k+1}
+// Vectors are stored unnormalised (s_{k+1} = w) with their scales
+// sc_{k+1} = 1/b_{k+1} kept on the device, so normalisation never costs a pass
+// over memory: every reader multiplies by the scalar.  One step is two
+// kernels: the H*v with the -b_k v_{k-1} term and the a_k dot product fused
+// (k_hxv<LZ>), then the a_k axpy fused with the |w| reduction (k_lz_update).
+// All scalars stay on the device; steps after convergence or breakdown are
+// no-ops (status flag), so chains are queued without host round trips.
+//
+// The ground-state iteration stores the whole Krylov basis (B200 HBM holds
+// hundreds of sector vectors) and forms the Ritz vector as one pass over it.
+// Every ncheck steps a single-CTA kernel computes the lowest Ritz value by
+// Sturm-sequence multisection in FP64 and compares it with the previous
+// check (the energy-change test of .repo/PLAIN_LANCZOS.f90:344-351).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "hxv.cuh"
+
+namespace dmfted {
+
+enum { ST_DONE = 0, ST_STEPS = 1, ST_CONV = 2, ST_RITZ_VALID = 3, ST_BREAK = 4 };
+
+// w = u - a_k sc_k s_k (in place in u), then b_{k+1} = |w|.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_lz_update(T *u, const T *scur, int64_t n,
+                                                           LanczosScalars lz, int k, double thr,
+                                                           double *partials, unsigned *counter) {
+    if (lz.status[ST_DONE]) return;
+    const double coef = lz.alpha[k] * lz.scale[k];
+    CSum s;
+    s.zero();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double w = (double)u[i] - coef * (double)scur[i];
+        const T wt = (T)w;
+        u[i] = wt;
+        s.add((double)wt * (double)wt);
+    }
+    CSum arr[1] = {s};
+    double tot[1];
+    if (grid_reduce<1>(arr, partials, counter, tot)) {
+        if (threadIdx.x == 0) {
+            const double b = sqrt(tot[0]);
+            lz.beta[k + 1] = b;
+            lz.scale[k + 1] = b > 0.0 ? 1.0 / b : 0.0;
+            lz.status[ST_STEPS] = k + 1;
+            if (b < thr) {
+                lz.status[ST_DONE] = 1;
+                lz.status[ST_BREAK] = 1;
+            }
+            if (k + 1 >= lz.kmax) lz.status[ST_DONE] = 1;
+        }
+    }
+}
+
+// Start of a recurrence: scale[0] = 1/|s_0|, beta[0] = 0, status cleared.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_lz_init(const T *s0, int64_t n, LanczosScalars lz,
+                                                         double *partials, unsigned *counter) {
+    CSum s;
+    s.zero();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = (double)s0[i];
+        s.add(v * v);
+    }
+    CSum arr[1] = {s};
+    double tot[1];
+    if (grid_reduce<1>(arr, partials, counter, tot)) {
+        if (threadIdx.x == 0) {
+            lz.scale[0] = tot[0] > 0.0 ? 1.0 / sqrt(tot[0]) : 0.0;
+            lz.beta[0] = 0.0;
+            for (int i = 0; i < 8; i++) lz.status[i] = 0;
+            lz.ritz[0] = lz.ritz[1] = 0.0;
+        }
+    }
+}
+
+// Sturm count: number of eigenvalues of the n x n tridiagonal (a, b[1..n-1])
+// below x.
+__device__ int sturm_count(const double *a, const double *b, int n, double x, double pivmin) {
+    int cnt = 0;
+    double q = a[0] - x;
+    if (fabs(q) < pivmin) q = -pivmin;
+    if (q < 0.0) cnt++;
+    for (int i = 1; i < n; i++) {
+        q = (a[i] - x) - b[i] * b[i] / q;
+        if (fabs(q) < pivmin) q = -pivmin;
+        if (q < 0.0) cnt++;
+    }
+    return cnt;
+}
+
+// j-th lowest eigenvalue (0-based) of T_n by multisection with all threads of
+// the block; a, b in shared memory.  Returns the value in every thread.
+__device__ double tridiag_eig(const double *a, const double *b, int n, int j) {
+    __shared__ int cnts[kRedThreads];
+    __shared__ double lohi[2];
+    if (threadIdx.x == 0) {
+        double lo = a[0], hi = a[0], amax = 0.0;
+        for (int i = 0; i < n; i++) {
+            const double r = (i > 0 ? fabs(b[i]) : 0.0) + (i + 1 < n ? fabs(b[i + 1]) : 0.0);
+            lo = fmin(lo, a[i] - r);
+            hi = fmax(hi, a[i] + r);
+            amax = fmax(amax, fabs(a[i]) + r);
+        }
+        const double pad = 2.2e-16 * fmax(amax, 1e-300) * 4.0 + 1e-300;
+        lohi[0] = lo - pad;
+        lohi[1] = hi + pad;
+    }
+    __syncthreads();
+    double amax = fmax(fabs(lohi[0]), fabs(lohi[1]));
+    const double pivmin = 1e-300 + 2.2e-16 * 2.2e-16 * fmax(amax * amax, 1e-300);
+    for (int round = 0; round < 40; round++) {
+        const double lo = lohi[0], hi = lohi[1];
+        if (hi - lo <= 2.0 * 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300) break;
+        const int nt = blockDim.x;
+        const double x = lo + (hi - lo) * (double)(threadIdx.x + 1) / (double)(nt + 1);
+        cnts[threadIdx.x] = sturm_count(a, b, n, x, pivmin);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = 0;
+            while (t < nt && cnts[t] <= j) t++;
+            const double nlo = t == 0 ? lo : lo + (hi - lo) * (double)t / (double)(nt + 1);
+            const double nhi = t == nt ? hi : lo + (hi - lo) * (double)(t + 1) / (double)(nt + 1);
+            lohi[0] = nlo;
+            lohi[1] = nhi;
+        }
+        __syncthreads();
+    }
+    const double r = 0.5 * (lohi[0] + lohi[1]);
+    __syncthreads();
+    return r;
+}
+
+// Eigenvector y of T_n (diag a[0..n), off-diagonal b[1..n)) for eigenvalue
+// lam: three steps of inverse iteration, Gaussian elimination with partial
+// pivoting on the tridiagonal.  Single thread.  ws: 5n doubles, sw: n bytes.
+__device__ void tridiag_evec(const double *a, const double *b, int n, double lam, double *yv,
+                             double *ws, unsigned char *sw) {
+    double *D = ws, *U1 = ws + n, *U2 = ws + 2 * n, *M = ws + 3 * n;
+    double nrm = 0.0;
+    for (int i = 0; i < n; i++) nrm = fmax(nrm, fabs(a[i] - lam) + (i > 0 ? fabs(b[i]) : 0.0));
+    const double tiny = fmax(nrm, 1e-300) * 1e-15;
+    double d = a[0] - lam, u1 = n > 1 ? b[1] : 0.0, u2 = 0.0;
+    for (int i = 0; i < n - 1; i++) {
+        const double l = b[i + 1], dn = a[i + 1] - lam, un = (i + 2 < n) ? b[i + 2] : 0.0;
+        if (fabs(d) >= fabs(l)) {
+            if (d == 0.0) d = tiny;
+            const double m = l / d;
+            D[i] = d; U1[i] = u1; U2[i] = u2; M[i] = m; sw[i] = 0;
+            d = dn - m * u1;
+            u1 = un - m * u2;
+            u2 = 0.0;
+        } else {
+            const double m = d / l;
+            D[i] = l; U1[i] = dn; U2[i] = un; M[i] = m; sw[i] = 1;
+            d = u1 - m * dn;
+            u1 = u2 - m * un;
+            u2 = 0.0;
+        }
+    }
+    if (d == 0.0) d = tiny;
+    D[n - 1] = d;
+    for (int i = 0; i < n; i++) yv[i] = 1.0 / sqrt((double)n);
+    for (int it = 0; it < 3; it++) {
+        for (int i = 0; i < n - 1; i++) {
+            if (sw[i]) {
+                const double t = yv[i];
+                yv[i] = yv[i + 1];
+                yv[i + 1] = t;
+            }
+            yv[i + 1] -= M[i] * yv[i];
+        }
+        yv[n - 1] /= D[n - 1];
+        if (n > 1) yv[n - 2] = (yv[n - 2] - U1[n - 2] * yv[n - 1]) / D[n - 2];
+        for (int i = n - 3; i >= 0; i--) yv[i] = (yv[i] - U1[i] * yv[i + 1] - U2[i] * yv[i + 2]) / D[i];
+        double ss = 0.0;
+        for (int i = 0; i < n; i++) ss += yv[i] * yv[i];
+        ss = 1.0 / sqrt(ss);
+        for (int i = 0; i < n; i++) yv[i] *= ss;
+    }
+    const double sg = yv[0] < 0.0 ? -1.0 : 1.0;  // deterministic sign
+    for (int i = 0; i < n; i++) yv[i] *= sg;
+}
+
+// Dynamic shared memory of the two Ritz kernels for n steps.
+__host__ __device__ inline size_t ritz_smem(int n) { return (size_t)8 * n * sizeof(double) + n + 16; }
+
+// Every ncheck steps: lowest Ritz value theta of T_n and the ARPACK stopping
+// test on its Ritz estimate, b_n |y_n| <= tol * max(eps^(2/3), |theta|)
+// (y = eigenvector of T_n, b_n = norm of the last residual).  Breakdown
+// (invariant subspace) counts as converged.
+__global__ void k_ritz_check(LanczosScalars lz, double tol) {
+    extern __shared__ double rs[];
+    const int n = lz.status[ST_STEPS];
+    if (n <= 0) return;
+    double *sa = rs, *sb = rs + n, *yv = rs + 2 * n, *ws = rs + 3 * n;
+    unsigned char *sw = reinterpret_cast<unsigned char *>(rs + 8 * n);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        sa[i] = lz.alpha[i];
+        sb[i] = i > 0 ? lz.beta[i] : 0.0;
+    }
+    __syncthreads();
+    const double e = tridiag_eig(sa, sb, n, 0);
+    if (threadIdx.x == 0) {
+        tridiag_evec(sa, sb, n, e, yv, ws, sw);
+        const double est = fabs(lz.beta[n]) * fabs(yv[n - 1]);
+        const double eps23 = 3.666852862501036e-11;
+        if (lz.status[ST_BREAK] || est <= tol * fmax(eps23, fabs(e))) {
+            lz.status[ST_CONV] = 1;
+            lz.status[ST_DONE] = 1;
+        }
+        lz.ritz[1] = est;
+        lz.ritz[0] = e;
+        lz.status[ST_RITZ_VALID] = 1;
+    }
+}
+
+// Ritz vector coefficients coef[i] = y_i * scale_i for eigenvalue lam, so
+// that the Ritz vector is sum_i coef_i s_i.
+__global__ void k_ritz_vector(LanczosScalars lz, int n, double lam, double *coef) {
+    extern __shared__ double rs[];
+    double *sa = rs, *sb = rs + n, *yv = rs + 2 * n, *ws = rs + 3 * n;
+    unsigned char *sw = reinterpret_cast<unsigned char *>(rs + 8 * n);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        sa[i] = lz.alpha[i];
+        sb[i] = i > 0 ? lz.beta[i] : 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    tridiag_evec(sa, sb, n, lam, yv, ws, sw);
+    for (int i = 0; i < n; i++) coef[i] = yv[i] * lz.scale[i];
+}
+
+// psi = sum_{i<n} coef_i * s_i over the stored basis (slot stride ld).  If
+// v0 (float64) is given it replaces slot 0 (the refinement basis keeps its
+// first vector in FP64).
+template <typename T>
+__global__ void k_basis_combine(const T *basis, int64_t ld, int n, const double *coef,
+                                const double *v0, double *psi, int64_t dim) {
+    __shared__ double sc[kLzMax + 8];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sc[i] = coef[i];
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < dim;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = v0 ? sc[0] * v0[i] : sc[0] * (double)basis[i];
+        for (int k = 1; k < n; k++) acc += sc[k] * (double)basis[k * ld + i];
+        psi[i] = acc;
+    }
+}
+
+// First step of the refinement recurrence, in FP64: w = u - a_0 sc_0 v0 with
+// u = H v0 (FP64), stored rounded to FP32 in the next slot; b_1 = |w| of the
+// stored values.
+__global__ void __launch_bounds__(kRedThreads) k_lz_update_first(const double *u, const double *v0,
+                                                                 float *out, int64_t n,
+                                                                 LanczosScalars lz,
+                                                                 double *partials,
+                                                                 unsigned *counter) {
+    if (lz.status[ST_DONE]) return;
+    const double coef = lz.alpha[0] * lz.scale[0];
+    CSum s;
+    s.zero();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float wt = (float)(u[i] - coef * v0[i]);
+        out[i] = wt;
+        s.add((double)wt * (double)wt);
+    }
+    CSum arr[1] = {s};
+    double tot[1];
+    if (grid_reduce<1>(arr, partials, counter, tot)) {
+        if (threadIdx.x == 0) {
+            const double b = sqrt(tot[0]);
+            lz.beta[1] = b;
+            lz.scale[1] = b > 0.0 ? 1.0 / b : 0.0;
+            lz.status[ST_STEPS] = 1;
+            if (b < 1e-300) {
+                lz.status[ST_DONE] = 1;
+                lz.status[ST_BREAK] = 1;
+            }
+            if (1 >= lz.kmax) lz.status[ST_DONE] = 1;
+        }
+    }
+}
+
+// |x|^2 -> out[slot] (compensated, deterministic)
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_norm2(const T *x, int64_t n, double *out,
+                                                       double *partials, unsigned *counter) {
+    CSum s;
+    s.zero();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = (double)x[i];
+        s.add(v * v);
+    }
+    CSum arr[1] = {s};
+    double tot[1];
+    if (grid_reduce<1>(arr, partials, counter, tot))
+        if (threadIdx.x == 0) *out = tot[0];
+}
+
+__global__ void k_scale_by_invsqrt(double *x, int64_t n, const double *n2) {
+    const double s = 1.0 / sqrt(*n2);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        x[i] *= s;
+}
+
+template <typename TO, typename TI>
+__global__ void k_convert(const TI *in, TO *out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (TO)in[i];
+}
+
+// Deterministic start vector: uniform (0,1] from a splitmix64 hash of
+// (seed, i) -- a real counterpart of the seeded random resid the reference
+// hands ARPACK (.repo/ARPACK_LANCZOS.f90:394-403).
+__global__ void k_random_start(double *x, int64_t n, uint64_t seed) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(i + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z = z ^ (z >> 31);
+        x[i] = ((double)(z >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+    }
+}
+
+// ---------------------------------------------------------------------------
+static int red_grid(dmfted_ctx *c, int64_t n) {
+    return (int)std::min<int64_t>(std::max<int64_t>(div_up(n, kRedThreads), 1),
+                                  std::min(kMaxRedBlocks, 4 * num_sms(c)));
+}
+
+static int ew_grid(dmfted_ctx *c, int64_t n) {
+    return (int)std::min<int64_t>(std::max<int64_t>(div_up(n, 256), 1), 16 * num_sms(c));
+}
+
+LanczosScalars lz_slot(dmfted_ctx *c, int slot, int kmax) {
+    DM_REQUIRE(slot >= 0 && slot < kLzSlots && kmax <= kLzMax, DMFTED_ERR_ARG,
+               "Lanczos scalar slot out of range");
+    LanczosScalars lz;
+    double *b = c->lz_d.p + (size_t)slot * kLzStride;
+    lz.alpha = b;
+    lz.beta = b + (kLzMax + 2);
+    lz.scale = b + 2 * (kLzMax + 2);
+    lz.ritz = b + 3 * (kLzMax + 2);
+    lz.status = c->lz_s.p + slot * 8;
+    lz.kmax = kmax;
+    return lz;
+}
+
+static void norm2_device(dmfted_ctx *c, const double *x, int64_t n, double *out) {
+    k_norm2<double><<<red_grid(c, n), kRedThreads, 0, c->stream>>>(x, n, out, c->red_partials.p,
+                                                                      c->red_counter.p);
+    DM_CHECK_LAUNCH();
+    c->launches++;
+}
+
+static void ritz_attr(dmfted_ctx *c) {
+    static bool done[64] = {false};
+    if (done[c->device & 63]) return;
+    DM_CUDA(cudaFuncSetAttribute(k_ritz_check, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ritz_smem(kLzMax)));
+    DM_CUDA(cudaFuncSetAttribute(k_ritz_vector, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ritz_smem(kLzMax)));
+    done[c->device & 63] = true;
+}
+
+// One Lanczos run on sector s storing the whole basis in T.
+//  start == nullptr : random start vector (deterministic seed)
+//  refine == false  : start (FP64) is rounded to T and used as s_0
+//  refine == true   : T = float; s_0 = start kept in FP64, the first step
+//                     (H s_0 and the residual) runs in FP64, later steps in
+//                     FP32; the Ritz vector combines the FP64 s_0 with the
+//                     FP32 directions.  Corrections enter the result with
+//                     O(residual) coefficients, so FP32 storage of them costs
+//                     only ~1e-7 of the correction.
+template <typename T>
+static LanczosResult gs_run(dmfted_ctx *c, const SectorView &s, double *psi, const double *start,
+                            double tol, int nitermax, int ncheck, bool refine) {
+    const int64_t dim = s.dim;
+    const int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
+    const size_t ld = (size_t)((dim + 31) / 32 * 32);
+    c->work.alloc(ld * sizeof(T) * (size_t)(kmax + 1));
+    T *basis = reinterpret_cast<T *>(c->work.p);
+    LanczosScalars lz = lz_slot(c, 0, kmax);
+    ritz_attr(c);
+    const int eg = ew_grid(c, dim);
+    const int rg = red_grid(c, dim);
+    if (start) {
+        k_convert<T, double><<<eg, 256, 0, c->stream>>>(start, basis, dim);
+    } else {
+        c->s64b.alloc(dim);
+        k_random_start<<<eg, 256, 0, c->stream>>>(c->s64b.p, dim, 1234567ull);
+        k_convert<T, double><<<eg, 256, 0, c->stream>>>(c->s64b.p, basis, dim);
+        c->launches++;
+    }
+    c->launches++;
+    if (refine)
+        k_lz_init<double><<<rg, kRedThreads, 0, c->stream>>>(start, dim, lz, c->red_partials.p,
+                                                              c->red_counter.p);
+    else
+        k_lz_init<T><<<rg, kRedThreads, 0, c->stream>>>(basis, dim, lz, c->red_partials.p,
+                                                         c->red_counter.p);
+    c->launches++;
+    DM_CHECK_LAUNCH();
+    int hst[8] = {0};
+    int launched = 0;
+    if (refine) {
+        // step 0 in FP64
+        c->s64c.alloc(dim);
+        hxv_lanczos_step<double>(c, s, start, start, c->s64c.p, lz, 0);
+        k_lz_update_first<<<rg, kRedThreads, 0, c->stream>>>(
+            c->s64c.p, start, reinterpret_cast<float *>(basis + ld), dim, lz, c->red_partials.p,
+            c->red_counter.p);
+        DM_CHECK_LAUNCH();
+        c->launches++;
+        launched = 1;
+    }
+    while (launched < kmax) {
+        for (int j = 0; j < ncheck && launched < kmax; j++, launched++) {
+            const int k = launched;
+            T *x = basis + (size_t)k * ld;
+            const T *xp = basis + (size_t)(k > 0 ? k - 1 : k) * ld;
+            T *y = basis + (size_t)(k + 1) * ld;
+            hxv_lanczos_step<T>(c, s, x, xp, y, lz, k);
+            k_lz_update<T><<<rg, kRedThreads, 0, c->stream>>>(y, x, dim, lz, k, 1e-300,
+                                                               c->red_partials.p, c->red_counter.p);
+            DM_CHECK_LAUNCH();
+            c->launches++;
+        }
+        k_ritz_check<<<1, kRedThreads, ritz_smem(launched), c->stream>>>(lz, tol);
+        DM_CHECK_LAUNCH();
+        c->launches++;
+        DM_CUDA(cudaMemcpyAsync(hst, lz.status, sizeof(hst), cudaMemcpyDeviceToHost, c->stream));
+        DM_CUDA(cudaStreamSynchronize(c->stream));
+        if (hst[ST_DONE]) break;
+    }
+    if (kmax <= launched && !hst[ST_DONE] && !refine) {
+        // (kmax reached inside the loop: the last check above already ran)
+    }
+    const int n = hst[ST_STEPS];
+    double ritz[2];
+    DM_CUDA(cudaMemcpy(ritz, lz.ritz, sizeof(ritz), cudaMemcpyDeviceToHost));
+    const double e0 = ritz[0];
+    double *coef = c->coefb.p;
+    k_ritz_vector<<<1, 32, ritz_smem(n), c->stream>>>(lz, n, e0, coef);
+    DM_CHECK_LAUNCH();
+    k_basis_combine<T><<<eg, 256, 0, c->stream>>>(basis, (int64_t)ld, n, coef,
+                                                   refine ? start : nullptr, psi, dim);
+    DM_CHECK_LAUNCH();
+    norm2_device(c, psi, dim, c->red_out.p);
+    k_scale_by_invsqrt<<<eg, 256, 0, c->stream>>>(psi, dim, c->red_out.p);
+    DM_CHECK_LAUNCH();
+    c->launches += 3;
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    return LanczosResult{e0, n, hst[ST_CONV] != 0};
+}
+
+LanczosResult lanczos_gs(dmfted_ctx *c, const SectorView &s, double *psi, const double *start,
+                         int precision, double tol, int nitermax) {
+    const int ncheck = std::max(1, c->p.lanc_ncheck);
+    if (precision == DMFTED_FP64) return gs_run<double>(c, s, psi, start, tol, nitermax, ncheck, false);
+    // Mixed: an FP32 run to the FP32 accuracy floor, then refinement runs
+    // whose first step is FP64 and whose other steps are FP32, until the
+    // FP64 stopping test holds.
+    const double tol32 = std::max(tol, c->mixed_tol32);
+    LanczosResult r = gs_run<float>(c, s, psi, start, tol32, nitermax, ncheck, false);
+    int steps = r.steps;
+    c->s64b.alloc(s.dim);
+    for (int round = 0; round < 4; round++) {
+        DM_CUDA(cudaMemcpyAsync(c->s64b.p, psi, s.dim * sizeof(double), cudaMemcpyDeviceToDevice,
+                                c->stream));
+        r = gs_run<float>(c, s, psi, c->s64b.p, tol, nitermax, std::max(2, ncheck / 2), true);
+        steps += r.steps;
+        if (r.converged) break;
+    }
+    r.steps = steps;
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Tridiagonalisation of a GF chain; two rotating buffers, no basis.  All
+// steps are queued; steps after breakdown are no-ops on the device.
+template <typename T>
+static void chain_impl(dmfted_ctx *c, const SectorView &s, const double *v0,
+                       const LanczosScalars &lz, int nstack) {
+    const int64_t dim = s.dim * nstack;
+    const size_t ld = (size_t)((dim + 31) / 32 * 32);
+    c->chainbuf.alloc(2 * ld * sizeof(T));
+    T *P = reinterpret_cast<T *>(c->chainbuf.p), *Q = P + ld;
+    const int eg = ew_grid(c, dim);
+    DM_CUDA(cudaMemsetAsync(P, 0, ld * sizeof(T), c->stream));
+    k_convert<T, double><<<eg, 256, 0, c->stream>>>(v0, Q, dim);
+    k_lz_init<T><<<red_grid(c, dim), kRedThreads, 0, c->stream>>>(Q, dim, lz, c->red_partials.p,
+                                                                   c->red_counter.p);
+    DM_CHECK_LAUNCH();
+    c->launches += 2;
+    for (int k = 0; k < lz.kmax; k++) {
+        hxv_lanczos_step<T>(c, s, Q, P, P, lz, k, nstack);
+        k_lz_update<T><<<red_grid(c, dim), kRedThreads, 0, c->stream>>>(
+            P, Q, dim, lz, k, c->p.lanc_gf_threshold, c->red_partials.p, c->red_counter.p);
+        DM_CHECK_LAUNCH();
+        c->launches++;
+        std::swap(P, Q);
+    }
+}
+
+void lanczos_chain(dmfted_ctx *c, const SectorView &s, const double *v0, int precision,
+                   const LanczosScalars &lz, int nstack) {
+    if (precision == DMFTED_FP64) chain_impl<double>(c, s, v0, lz, nstack);
+    else chain_impl<float>(c, s, v0, lz, nstack);
+}
+
+}  // namespace dmfted

@@ -1,0 +1,234 @@
+/*
+ * dmfted.h -- C-ABI of the B200 (sm_100a) exact-diagonalization impurity
+ * solver for dmft-ed (normal ed_mode, normal bath).
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (DMFTED_OK == 0).  dmfted_last_error() gives the message of the last
+ * failure on the calling thread.  A Fortran iso_c_binding shim maps a non-zero
+ * status to `stop "<message>"`, which is what the reference does on the same
+ * conditions.
+ *
+ * Conventions kept from the reference so that a Fortran caller passes its own
+ * arrays unchanged:
+ *   - sector indices are 1-based, numbered nup-major:
+ *       isector = nup*(Ns+1) + ndw + 1            (ED_SETUP.f90:388-400)
+ *   - a sector vector is indexed like the reference's H%map:
+ *       i = rank_up + DimUp*rank_dw               (ED_SETUP.f90:880-890)
+ *   - complex128 arrays are interleaved (re, im) doubles, Fortran complex(8);
+ *   - multi-index arrays are Fortran column-major, e.g.
+ *       impGmats(Nspin,Nspin,Norb,Norb,Lmats)     (ED_VARS_GLOBAL.f90:120-125)
+ *   - the user bath array has the set_dmft_bath layout: e(ispin,iorb,k) then
+ *     v(ispin,iorb,k), k fastest              (ED_BATH/dmft_aux.f90:493-512).
+ *
+ * One context per process and GPU, one CUDA stream per context; calls on a
+ * context are not thread-safe (the reference's module state is not either).
+ */
+#ifndef DMFTED_H
+#define DMFTED_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define DMFTED_OK 0
+#define DMFTED_ERR_ARG 1         /* bad argument or size mismatch            */
+#define DMFTED_ERR_CUDA 2        /* CUDA runtime failure                     */
+#define DMFTED_ERR_NOMEM 3       /* device allocation failed                 */
+#define DMFTED_ERR_UNSUPPORTED 4 /* configuration outside this solver        */
+#define DMFTED_ERR_STATE 5       /* call out of order (no sector / no bath)  */
+#define DMFTED_ERR_NOTCONV 6     /* iteration limit hit before convergence   */
+#define DMFTED_ERR_NORM 7        /* state not normalised                     */
+#define DMFTED_ERR_TIMEOUT 8     /* a bounded device wait gave up            */
+
+/* ---- precision of the Lanczos vectors ------------------------------- */
+#define DMFTED_FP64 0  /* plain FP64: the drop-in path                       */
+#define DMFTED_MIXED 1 /* FP32 vectors and H*v, compensated FP64 alpha/beta,
+                          FP64 refinement of the ground state, FP64 G(iwn)   */
+
+/* Input variables of ED_INPUT_VARS.f90 that define the hot path, with the
+ * reference's names and defaults (dmfted_default_params fills those). */
+typedef struct dmfted_params {
+    int32_t norb, nbath, nspin;   /* NORB, NBATH, NSPIN            :111-113 */
+    int32_t hfmode, jhflag;       /* HFMODE (T), JHFLAG (F)        :143-144 */
+    double uloc[3];               /* ULOC                          :114     */
+    double ust, jh, jx, jp;       /* UST, JH, JX, JP               :115-118 */
+    double xmu, beta;             /* XMU, BETA                     :119-120 */
+    int32_t lmats, lreal;         /* LMATS, LREAL                  :133-134 */
+    double wini, wfin, eps;       /* WINI, WFIN, EPS               :140-145 */
+    int32_t lanc_niter;           /* LANC_NITER (512)              :154     */
+    int32_t lanc_ngfiter;         /* LANC_NGFITER (200)            :155     */
+    double lanc_tolerance;        /* LANC_TOLERANCE (1e-12)        :156     */
+    int32_t lanc_dim_threshold;   /* LANC_DIM_THRESHOLD (256)      :157     */
+    int32_t lanc_nstates_sector;  /* LANC_NSTATES_SECTOR (6)       :149     */
+    int32_t lanc_nstates_total;   /* LANC_NSTATES_TOTAL (1 => T=0) :150     */
+    int32_t lanc_nstates_step;    /* LANC_NSTATES_STEP (2)         :151     */
+    double gs_threshold;          /* GS_THRESHOLD (1e-9)           :147     */
+    double cutoff;                /* CUTOFF (1e-9)                 :146     */
+    int32_t ed_twin;              /* ED_TWIN (F)                   :125     */
+    int32_t lfit;                 /* LFIT (1000)                   :136     */
+    int32_t cg_weight;            /* CG_WEIGHT (0)                 :164     */
+    /* additions of this solver (defaults keep the reference behaviour) */
+    int32_t precision;            /* DMFTED_FP64 or DMFTED_MIXED            */
+    int32_t lanc_ncheck;          /* Ritz-value check interval (10)         */
+    int32_t device;               /* CUDA device ordinal (0)                */
+    double lanc_gf_threshold;     /* |b| that ends a GF chain (1e-13)       */
+} dmfted_params;
+
+typedef struct dmfted_ctx dmfted_ctx;
+
+/* Fill *p with the reference defaults (ED_INPUT_VARS.f90:111-176). */
+void dmfted_default_params(dmfted_params *p);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *dmfted_last_error(void);
+
+/* Library version string. */
+const char *dmfted_version(void);
+
+/* ---- set-up ------------------------------------------------------------
+ * dmfted_init replaces ed_init_solver_single (ED_MAIN.f90:67-107):
+ * init_ed_structure (ED_SETUP.f90:135-367) and setup_pointers_normal
+ * (:379-493).  It builds the Fock-space tables on the device (all popcount
+ * classes of Ns-bit words, their ranks, the hopping tables) and allocates the
+ * working set.  hloc: impHloc(Nspin,Nspin,Norb,Norb) complex128, may be NULL
+ * (zero).  Unsupported: Norb>3, Nspin>2 (the reference stops there too,
+ * ED_SETUP.f90:274-275), complex off-diagonal Hloc.                        */
+int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out);
+int dmfted_free(dmfted_ctx *ctx);
+
+/* set_Hloc (ED_AUX_FUNX.f90:135-143): replace impHloc. */
+int dmfted_set_hloc(dmfted_ctx *ctx, const double *hloc);
+
+/* get_bath_dimension, normal bath (ED_BATH/user_aux.f90:11-94):
+ * 2*Nspin*Norb*Nbath. */
+int dmfted_get_bath_dimension(const dmfted_params *p, int32_t *nb);
+
+/* set_dmft_bath (ED_BATH/dmft_aux.f90:474-512): load the user bath array. */
+int dmfted_set_bath(dmfted_ctx *ctx, const double *bath, int32_t nb);
+
+/* Sector tables of setup_pointers_normal (ED_SETUP.f90:379-493), all values
+ * 1-based as the reference stores them.  Sizes: nsectors=(Ns+1)^2 for
+ * getnup..getdimdw, 2*nsectors for getcsector/getcdgsector (index
+ * (isector-1)*2+ispin-1), (Ns+1)^2 for getsector (index nup*(Ns+1)+ndw),
+ * Norb*Nbath for getbathstride (index (k-1)*Norb+iorb-1), 2*Norb for
+ * impindex (index (ispin-1)*Norb+iorb-1).  Any pointer may be NULL. */
+int dmfted_sector_tables(dmfted_ctx *ctx, int32_t *nsectors, int32_t *getsector, int32_t *getnup,
+                         int32_t *getndw, int32_t *getdim, int32_t *getdimup, int32_t *getdimdw,
+                         int32_t *getcsector, int32_t *getcdgsector, int32_t *getbathstride,
+                         int32_t *impindex);
+
+/* build_sector (ED_SETUP.f90:861-891, normal): the sector -> Fock map
+ * map[i] = iup + idw*2^Ns in the reference's order, computed on the device
+ * by combinatorial unranking (bit-exact).  dim must equal getdim(isector);
+ * needs Ns <= 15 (the reference stores the map in a default integer). */
+int dmfted_build_sector(dmfted_ctx *ctx, int32_t isector, int32_t *map, int64_t dim);
+
+/* setup_Hv_sector / delete_Hv_sector (ED_HAMILTONIAN_MATVEC.f90:99-111). */
+int dmfted_setup_hv_sector(dmfted_ctx *ctx, int32_t isector);
+int dmfted_delete_hv_sector(dmfted_ctx *ctx);
+
+/* ---- H*v ----------------------------------------------------------------
+ * Procedure-pointer target with the cc_sparse_HxV contract
+ * (ED_VARS_GLOBAL.f90:43-49, selected at ED_MAIN.f90:269-276): Hv = H v on
+ * the sector set by dmfted_setup_hv_sector, complex128 host arrays of length
+ * nloc == getdim(isector).  Replaces directMatVec_cc
+ * (ED_HAMILTONIAN_MATVEC.f90:289-351); copies in and out of the device on
+ * every call (compatibility mode for solvers that own the vectors).     */
+int dmfted_hxv_c128(dmfted_ctx *ctx, int32_t nloc, const double *v, double *hv);
+
+/* Same product on device-resident real vectors of the current sector
+ * (float64 or float32), on the context's stream; nvec vectors stored back to
+ * back.  For callers that keep their vectors on the device. */
+int dmfted_hxv_device_f64(dmfted_ctx *ctx, const double *d_v, double *d_hv, int32_t nvec);
+int dmfted_hxv_device_f32(dmfted_ctx *ctx, const float *d_v, float *d_hv, int32_t nvec);
+
+/* ---- device-resident solvers ----------------------------------------- */
+/* Lowest eigenpair of sector isector by Lanczos on the device; stands in for
+ * sp_eigh with Neigen=1 (ED_DIAG.f90:169-183).  psi (complex128, length
+ * getdim) may be NULL.  *niter: H*v products used (may be NULL).  Precision
+ * follows params.precision. */
+int dmfted_lanczos_gs(dmfted_ctx *ctx, int32_t isector, double *e0, double *psi, int32_t *niter);
+
+/* Three-term Lanczos tridiagonalisation from a given start vector, the
+ * contract of sp_lanc_tridiag (build_gf_normal.f90:118-127): vvinit complex128
+ * of length getdim(isector) (normalised here), alanc[nlanc], blanc[nlanc]
+ * with blanc[0]=0 and blanc[k]=b_k coupling steps k-1 and k.  *nused: steps
+ * taken before |b| fell below lanc_gf_threshold. */
+int dmfted_lanc_tridiag(dmfted_ctx *ctx, int32_t isector, const double *vvinit, int32_t nlanc,
+                        double *alanc, double *blanc, int32_t *nused);
+
+/* ---- the solve ------------------------------------------------------------
+ * ed_solve_single (ED_MAIN.f90:251-289) for the normal mode:
+ * set_dmft_bath, diagonalize_impurity (ED_DIAG.f90:78-398), the observables
+ * of observables_impurity (ED_OBSERVABLES.f90:113-160), buildgf_impurity
+ * (ED_GREENS_FUNCTIONS.f90:111-175 with build_gf_normal.f90:71-180,442-488)
+ * and get_sigma_normal.  Everything stays on the device until read back with
+ * the getters below.  T=0 (lanc_nstates_total==1) and finite temperature are
+ * both handled.  sectors: optional list of 1-based sectors to restrict the
+ * scan to (NULL / nsectors=0 scans every sector the reference scans). */
+int dmfted_ed_solve(dmfted_ctx *ctx, const double *bath, int32_t nb, const int32_t *sectors,
+                    int32_t nsectors);
+
+/* Getters (ED_IO.f90:371-394).  G-like arrays are complex128 with the
+ * reference's shape (Nspin,Nspin,Norb,Norb,L), column-major. */
+int dmfted_get_gimp_matsubara(dmfted_ctx *ctx, double *g);
+int dmfted_get_gimp_real(dmfted_ctx *ctx, double *g);
+int dmfted_get_sigma_matsubara(dmfted_ctx *ctx, double *s);
+int dmfted_get_sigma_real(dmfted_ctx *ctx, double *s);
+int dmfted_get_g0imp_matsubara(dmfted_ctx *ctx, double *g);
+/* ed_dens, ed_dens_up, ed_dens_dw, ed_docc (Norb each), ed_magz (Norb). */
+int dmfted_get_observables(dmfted_ctx *ctx, double *dens, double *dens_up, double *dens_dw,
+                           double *docc, double *magz);
+/* The kept eigenspace: energies, 1-based sectors (state_list order,
+ * ED_EIGENSPACE.f90:157-213), count, partition function Z. */
+int dmfted_get_eigenspace(dmfted_ctx *ctx, int32_t cap, double *energies, int32_t *sectors,
+                          int32_t *nstates, double *zeta);
+/* Ground-state energy of the last solve. */
+int dmfted_get_egs(dmfted_ctx *ctx, double *egs);
+
+/* ---- gradients -----------------------------------------------------------
+ * Hellmann-Feynman gradient of the thermal energy of the last solve with
+ * respect to the user bath array (same layout and length as the bath):
+ *   dE/de(s,a,k) = <n_{k,s}>,  dE/dV(s,a,k) = <c+_{a s} c_{k s} + h.c.>
+ * as reductions over the kept eigenvectors on the device.  For Nspin=1 the
+ * two physical spins share one parameter and their terms add. */
+int dmfted_hf_gradient(dmfted_ctx *ctx, double *grad, int32_t nb);
+
+/* Batched chi^2 of the Delta fit and its gradient, the functions
+ * chi2_delta_normal_normal and grad_chi2_delta_normal_normal of
+ * ED_CHI2FIT/fitgf_normal_normal.f90:193-226,256-316 (the fit's gradient
+ * routine, in place of grad_delta_bath), for nbatch parameter sets
+ * a[b*2*nbath + j] = [e_1..e_Nbath, V_1..V_Nbath].  xdelta[L] = wm,
+ * g[L] complex128 target, w[L] weights.  chi2[nbatch], grad[nbatch*2*nbath]
+ * (grad may be NULL).  Host pointers; the work runs on the device of ctx. */
+int dmfted_chi2_delta_batch(dmfted_ctx *ctx, int32_t nbatch, int32_t nbath, int32_t L,
+                            const double *a, const double *xdelta, const double *g,
+                            const double *w, double *chi2, double *grad);
+
+/* Same on device pointers, on the context's stream (no host copies). */
+int dmfted_chi2_delta_batch_device(dmfted_ctx *ctx, int32_t nbatch, int32_t nbath, int32_t L,
+                                   const double *d_a, const double *d_xdelta, const double *d_g,
+                                   const double *d_w, double *d_chi2, double *d_grad);
+
+/* ---- timing helpers (device time on the context's stream) ------------ */
+/* Average device milliseconds of one H*v on the current sector over reps
+ * launches after warmup launches (fp32 != 0: float32 vectors).  The vectors
+ * are the context's own work buffers. */
+int dmfted_time_hxv(dmfted_ctx *ctx, int32_t fp32, int32_t warmup, int32_t reps, double *ms);
+
+/* Device milliseconds of the last dmfted_ed_solve, split into phases:
+ * t[0]=diagonalisation, t[1]=observables, t[2]=Green's functions,
+ * t[3]=total; and the H*v products each phase used in n[0..2]. */
+int dmfted_get_timings(dmfted_ctx *ctx, double *t, int64_t *n);
+
+/* Number of kernel launches the library issued since the counter was last
+ * reset (*count), then reset it if reset != 0. */
+int dmfted_launch_count(dmfted_ctx *ctx, int64_t *count, int32_t reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

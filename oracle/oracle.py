@@ -1,0 +1,445 @@
+"""Python front-end of the CPU restatement in ``oracle/ed_oracle.c``.
+
+TEST INFRASTRUCTURE ONLY: the checker for the CUDA library.  Only ``tests/``,
+``__graft_entry__.smoke()`` and the ``cpu_baseline`` / ``--impl reference``
+legs of ``bench.py`` import this module; the product never does.
+
+Parity status: unpinned against reference outputs (the reference is Fortran
+with unvendored SciFortran/DMFT_Tools and ships no tests or golden data).  The
+restatement is pinned instead against independent known answers: dense
+``numpy.linalg.eigh`` of the explicit sector Hamiltonian, ARPACK
+(``scipy.sparse.linalg.eigsh``, the eigensolver family behind SciFortran's
+``sp_eigh``), the U=0 and V=0 analytic limits and the particle+hole sum rule.
+
+Each wrapper names the reference routine it restates (file:line relative to
+the reference project root).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libedoracle.so")
+_lib = None
+
+
+def build():
+    """Compile ed_oracle.c with the committed Makefile (no-op when current)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+class _Model(C.Structure):
+    _fields_ = [
+        ("norb", C.c_int32), ("nbath", C.c_int32), ("nspin", C.c_int32), ("ns", C.c_int32),
+        ("hfmode", C.c_int32), ("jhflag", C.c_int32),
+        ("uloc", C.c_double * 3),
+        ("ust", C.c_double), ("jh", C.c_double), ("jx", C.c_double), ("jp", C.c_double),
+        ("xmu", C.c_double), ("beta", C.c_double),
+        ("e", C.POINTER(C.c_double)), ("v", C.POINTER(C.c_double)),
+        ("hloc", C.POINTER(C.c_double)),
+    ]
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+
+
+def _declare(L):
+    L.or_binomial.restype = C.c_int32
+    L.or_binomial.argtypes = [C.c_int32, C.c_int32]
+    L.or_sector_dim.restype = C.c_int64
+    L.or_sector_dim.argtypes = [C.c_int32, C.c_int32, C.c_int32]
+    L.or_setup_pointers_normal.argtypes = [C.c_int32, C.c_int32] + [_ip] * 10
+    L.or_build_sector.restype = C.c_int64
+    L.or_build_sector.argtypes = [C.c_int32, C.c_int32, C.c_int32, _ip]
+    L.or_binary_search.restype = C.c_int64
+    L.or_binary_search.argtypes = [_ip, C.c_int64, C.c_int32]
+    L.or_c.restype = C.c_int32
+    L.or_c.argtypes = [C.c_int32, C.c_int32, _ip, _dp]
+    L.or_cdg.restype = C.c_int32
+    L.or_cdg.argtypes = [C.c_int32, C.c_int32, _ip, _dp]
+    L.or_hxv_c128.argtypes = [C.POINTER(_Model), _ip, C.c_int64, _dp, _dp, C.c_int32]
+    L.or_build_coo.restype = C.c_int64
+    L.or_build_coo.argtypes = [C.POINTER(_Model), _ip, C.c_int64, C.c_int64, _lp, _lp, _dp, _dp]
+    L.or_lanczos_tridiag.restype = C.c_int32
+    L.or_lanczos_tridiag.argtypes = [C.POINTER(_Model), _ip, C.c_int64, _dp, C.c_int32, _dp, _dp,
+                                     C.c_double, C.c_int32]
+    L.or_tql2.restype = C.c_int32
+    L.or_tql2.argtypes = [C.c_int32, _dp, _dp, _dp]
+    L.or_lanczos_gs.restype = C.c_int32
+    L.or_lanczos_gs.argtypes = [C.POINTER(_Model), _ip, C.c_int64, _dp, C.c_int32, C.c_double,
+                                C.c_int32, _dp, C.c_int32]
+    L.or_add_to_lanczos_gf.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,
+                                       C.c_double, _dp, _dp, C.c_int32, C.c_int32, _dp, C.c_int32,
+                                       _dp, C.c_int32, C.c_double, _dp, _dp]
+    L.or_gf_vvinit.restype = C.c_double
+    L.or_gf_vvinit.argtypes = [C.c_int32, C.c_int32, _ip, C.c_int64, _ip, C.c_int64, _dp, _dp]
+    L.or_observables_state.argtypes = [C.POINTER(_Model), _ip, C.c_int64, _dp, C.c_double,
+                                       _dp, _dp, _dp, _dp, _dp, _dp]
+    L.or_hf_terms_state.argtypes = [C.POINTER(_Model), _ip, C.c_int64, _dp, C.c_double, _dp, _dp]
+    L.or_delta_bath.argtypes = [_dp, _dp, C.c_int32, _dp, C.c_int32, _dp]
+    L.or_sigma_normal.argtypes = [_dp, _dp, C.c_int32, C.c_double, C.c_double, _dp, C.c_int32,
+                                  _dp, _dp]
+    L.or_chi2_delta.restype = C.c_double
+    L.or_chi2_delta.argtypes = [_dp, C.c_int32, _dp, _dp, _dp, C.c_int32, _dp]
+    L.or_host_threads.restype = C.c_int32
+
+
+def _p(a, ct=C.c_double):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+# --------------------------------------------------------------------------
+@dataclass
+class Model:
+    """Normal-mode, normal-bath impurity model (the reference's global input
+    variables of ED_INPUT_VARS.f90 plus dmft_bath and impHloc)."""
+    norb: int = 1
+    nbath: int = 7
+    nspin: int = 1
+    uloc: tuple = (2.0, 0.0, 0.0)
+    ust: float = 0.0
+    jh: float = 0.0
+    jx: float = 0.0
+    jp: float = 0.0
+    xmu: float = 0.0
+    beta: float = 100.0
+    hfmode: bool = True
+    jhflag: bool = False
+    e: np.ndarray = field(default=None)      # [nspin, norb, nbath]
+    v: np.ndarray = field(default=None)      # [nspin, norb, nbath]
+    hloc: np.ndarray = field(default=None)   # complex [nspin, nspin, norb, norb]
+
+    @property
+    def ns(self):
+        return (self.nbath + 1) * self.norb
+
+    def __post_init__(self):
+        if self.e is None:
+            self.e = np.zeros((self.nspin, self.norb, self.nbath))
+        if self.v is None:
+            self.v = np.zeros((self.nspin, self.norb, self.nbath))
+        if self.hloc is None:
+            self.hloc = np.zeros((self.nspin, self.nspin, self.norb, self.norb), complex)
+        self.e = np.ascontiguousarray(self.e, dtype=np.float64)
+        self.v = np.ascontiguousarray(self.v, dtype=np.float64)
+        self.hloc = np.asarray(self.hloc, dtype=np.complex128)
+
+    def bath_array(self):
+        """User bath array, set_dmft_bath layout (ED_BATH/dmft_aux.f90:493-512):
+        e then v, each with k fastest, then iorb, then ispin."""
+        return np.concatenate([self.e.reshape(-1), self.v.reshape(-1)])
+
+    def _struct(self):
+        hl = np.asfortranarray(self.hloc).reshape(-1, order="F")
+        hl = np.ascontiguousarray(np.stack([hl.real, hl.imag], axis=-1).reshape(-1))
+        self._keep = (self.e, self.v, hl)
+        m = _Model()
+        m.norb, m.nbath, m.nspin, m.ns = self.norb, self.nbath, self.nspin, self.ns
+        m.hfmode, m.jhflag = int(self.hfmode), int(self.jhflag)
+        for i in range(3):
+            m.uloc[i] = float(self.uloc[i]) if i < len(self.uloc) else 0.0
+        m.ust, m.jh, m.jx, m.jp, m.xmu, m.beta = self.ust, self.jh, self.jx, self.jp, self.xmu, self.beta
+        m.e, m.v, m.hloc = _p(self.e), _p(self.v), _p(hl)
+        return m
+
+
+def seeded_model(seed, norb=1, nbath=7, nspin=1, u=2.0, ust=0.0, jh=0.0, xmu=0.0, beta=100.0,
+                 e_range=1.0, v0=0.5, v_spread=0.1, hfmode=True):
+    """Seeded synthetic bath: e_k ~ U[-e_range, e_range], V_k = v0 + U[-v_spread, v_spread]
+    from numpy.random.default_rng(seed), shared by both spins when nspin=2."""
+    rng = np.random.default_rng(seed)
+    e = rng.uniform(-e_range, e_range, size=(norb, nbath))
+    v = v0 + rng.uniform(-v_spread, v_spread, size=(norb, nbath))
+    e = np.broadcast_to(e, (nspin, norb, nbath)).copy()
+    v = np.broadcast_to(v, (nspin, norb, nbath)).copy()
+    ul = [u] * norb + [0.0] * (3 - norb)
+    return Model(norb=norb, nbath=nbath, nspin=nspin, uloc=tuple(ul), ust=ust, jh=jh, xmu=xmu,
+                 beta=beta, hfmode=hfmode, e=e, v=v)
+
+
+# ---------------------------------------------------------------- setup ---
+def binomial(n1, n2):
+    """ED_SETUP.f90:1258-1275."""
+    return lib().or_binomial(n1, n2)
+
+
+def sector_tables(norb, nbath):
+    """setup_pointers_normal, ED_SETUP.f90:379-493 (1-based values)."""
+    ns = (nbath + 1) * norb
+    nsec = (ns + 1) ** 2
+    t = {k: np.zeros(n, np.int32) for k, n in [
+        ("getsector", (ns + 1) ** 2), ("getnup", nsec), ("getndw", nsec), ("getdim", nsec),
+        ("getdimup", nsec), ("getdimdw", nsec), ("getcsector", 2 * nsec),
+        ("getcdgsector", 2 * nsec), ("getbathstride", norb * nbath), ("impindex", 2 * norb)]}
+    lib().or_setup_pointers_normal(norb, nbath, *[_p(t[k], C.c_int32) for k in [
+        "getsector", "getnup", "getndw", "getdim", "getdimup", "getdimdw", "getcsector",
+        "getcdgsector", "getbathstride", "impindex"]])
+    return t
+
+
+def build_sector(ns, nup, ndw):
+    """build_sector (normal), ED_SETUP.f90:874-891."""
+    dim = lib().or_sector_dim(ns, nup, ndw)
+    m = np.zeros(dim, np.int32)
+    got = lib().or_build_sector(ns, nup, ndw, _p(m, C.c_int32))
+    assert got == dim
+    return m
+
+
+def binary_search(a, value):
+    """ED_SETUP.f90:1282-1299 (1-based position, 0 if absent)."""
+    a = np.ascontiguousarray(a, np.int32)
+    return lib().or_binary_search(_p(a, C.c_int32), a.size, value)
+
+
+# ----------------------------------------------------------------- H*v ----
+def hxv(model, hmap, v, nthreads=1):
+    """directMatVec_cc, ED_HAMILTONIAN_MATVEC.f90:289-351 (complex128)."""
+    v = np.ascontiguousarray(v, np.complex128)
+    out = np.empty_like(v)
+    ms = model._struct()
+    lib().or_hxv_c128(C.byref(ms), _p(hmap, C.c_int32), hmap.size, _p(v.view(np.float64)),
+                      _p(out.view(np.float64)), nthreads)
+    return out
+
+
+def sparse_h(model, hmap):
+    """Explicit sector H (the element set of ed_buildH_c) as a scipy CSR matrix
+    with H[i, j] = coefficient that row i applies to v[j]."""
+    import scipy.sparse as sp
+    dim = hmap.size
+    cap = dim * (4 + 2 * model.norb * model.norb + 4 * model.norb * model.nbath + 4 * model.norb ** 2)
+    ri = np.zeros(cap, np.int64)
+    ci = np.zeros(cap, np.int64)
+    re = np.zeros(cap)
+    im = np.zeros(cap)
+    ms = model._struct()
+    n = lib().or_build_coo(C.byref(ms), _p(hmap, C.c_int32), dim, cap, _p(ri, C.c_int64),
+                           _p(ci, C.c_int64), _p(re), _p(im))
+    assert n < cap
+    vals = re[:n] + 1j * im[:n]
+    if not np.any(vals.imag):
+        vals = vals.real
+    return sp.csr_matrix((vals, (ri[:n], ci[:n])), shape=(dim, dim))
+
+
+# ------------------------------------------------------------- Lanczos ---
+def lanczos_tridiag(model, hmap, vin, nitermax, threshold=1e-13, nthreads=1):
+    """sp_lanc_tridiag restated from .repo/PLAIN_LANCZOS.f90:87-118,154-180."""
+    v = np.ascontiguousarray(vin, np.complex128).copy()
+    a = np.zeros(nitermax)
+    b = np.zeros(nitermax)
+    ms = model._struct()
+    n = lib().or_lanczos_tridiag(C.byref(ms), _p(hmap, C.c_int32), hmap.size, _p(v.view(np.float64)),
+                                 nitermax, _p(a), _p(b), threshold, nthreads)
+    return a, b, n
+
+
+def tql2(d, e, z=None):
+    """ED_GREENS_FUNCTIONS.f90:361-499.  e[1:] is the sub-diagonal."""
+    d = np.ascontiguousarray(d, np.float64).copy()
+    e = np.ascontiguousarray(e, np.float64).copy()
+    n = d.size
+    if z is None:
+        z = np.eye(n)
+    z = np.asfortranarray(z, np.float64).copy(order="F")
+    zf = z.reshape(-1, order="F").copy()
+    ierr = lib().or_tql2(n, _p(d), _p(e), _p(zf))
+    return d, zf.reshape((n, n), order="F"), ierr
+
+
+def start_vector(dim, seed=1234567):
+    """Deterministic complex start vector (the reference seeds ARPACK's resid
+    with random numbers from seed 1234567, .repo/ARPACK_LANCZOS.f90:394-403)."""
+    rng = np.random.default_rng(seed)
+    v = rng.random(dim) + 1j * rng.random(dim)
+    return v / np.linalg.norm(v)
+
+
+def lanczos_gs(model, hmap, nitermax=512, threshold=1e-12, ncheck=10, v0=None, nthreads=1):
+    """Ground state by plain Lanczos, .repo/PLAIN_LANCZOS.f90:286-385."""
+    v = start_vector(hmap.size) if v0 is None else np.asarray(v0, np.complex128).copy()
+    v = np.ascontiguousarray(v)
+    e = C.c_double()
+    ms = model._struct()
+    n = lib().or_lanczos_gs(C.byref(ms), _p(hmap, C.c_int32), hmap.size, _p(v.view(np.float64)),
+                            min(nitermax, hmap.size), threshold, ncheck, C.byref(e), nthreads)
+    return e.value, v, n
+
+
+# ------------------------------------------------------------------- GF ---
+def matsubara(beta, L):
+    """wm = pi/beta*(2n-1), ED_GREENS_FUNCTIONS.f90:114."""
+    return np.pi / beta * (2.0 * np.arange(1, L + 1) - 1.0)
+
+
+def realaxis(wini, wfin, L):
+    return np.linspace(wini, wfin, L) if L > 0 else np.zeros(0)
+
+
+def gf_vvinit(particle, isite, map_i, map_j, psi):
+    """vvinit of lanc_build_gf_normal_c, build_gf_normal.f90:97-116,136-155."""
+    psi = np.ascontiguousarray(psi, np.complex128)
+    vv = np.zeros(map_j.size, np.complex128)
+    n2 = lib().or_gf_vvinit(int(particle), isite, _p(map_i, C.c_int32), map_i.size,
+                            _p(map_j, C.c_int32), map_j.size, _p(psi.view(np.float64)),
+                            _p(vv.view(np.float64)))
+    return n2, vv
+
+
+def add_to_lanczos_gf(vnorm2, ei, egs, zeta, finite_t, beta, alanc, blanc, isign, wm, wr, eps,
+                      gm, gr):
+    """add_to_lanczos_gf_normal, build_gf_normal.f90:442-488 (accumulates)."""
+    alanc = np.ascontiguousarray(alanc, np.float64)
+    blanc = np.ascontiguousarray(blanc, np.float64)
+    wm = np.ascontiguousarray(wm, np.float64)
+    wr = np.ascontiguousarray(wr, np.float64)
+    lib().or_add_to_lanczos_gf(vnorm2, ei, egs, zeta, int(finite_t), beta, _p(alanc), _p(blanc),
+                               alanc.size, isign, _p(wm), wm.size, _p(wr), wr.size, eps,
+                               _p(gm.view(np.float64)), _p(gr.view(np.float64)))
+
+
+def observables_state(model, hmap, psi, peso):
+    """observables_impurity n/docc loop and diagonal bath DM,
+    ED_OBSERVABLES.f90:113-160,286-305."""
+    no, nb = model.norb, model.nbath
+    out = {k: np.zeros(no) for k in ["dens", "dens_up", "dens_dw", "docc", "magz"]}
+    out["bath_dm"] = np.zeros(model.nspin * no * nb)
+    psi = np.ascontiguousarray(psi, np.complex128)
+    ms = model._struct()
+    lib().or_observables_state(C.byref(ms), _p(hmap, C.c_int32), hmap.size, _p(psi.view(np.float64)),
+                               peso, *[_p(out[k]) for k in ["dens", "dens_up", "dens_dw", "docc",
+                                                             "magz", "bath_dm"]])
+    return out
+
+
+def hf_terms_state(model, hmap, psi, peso=1.0):
+    """<c+_a c_k + h.c.> and <n_k> per physical spin (Hellmann-Feynman operators)."""
+    no, nb = model.norb, model.nbath
+    hop = np.zeros(2 * no * nb)
+    nk = np.zeros(2 * no * nb)
+    psi = np.ascontiguousarray(psi, np.complex128)
+    ms = model._struct()
+    lib().or_hf_terms_state(C.byref(ms), _p(hmap, C.c_int32), hmap.size, _p(psi.view(np.float64)),
+                            peso, _p(hop), _p(nk))
+    return hop.reshape(2, no, nb), nk.reshape(2, no, nb)
+
+
+def delta_bath(e_k, v_k, x):
+    """delta_bath_mats (normal), ED_BATH_FUNCTIONS.f90:247-257."""
+    x = np.ascontiguousarray(x, np.complex128)
+    d = np.zeros_like(x)
+    e_k = np.ascontiguousarray(e_k, np.float64)
+    v_k = np.ascontiguousarray(v_k, np.float64)
+    lib().or_delta_bath(_p(e_k), _p(v_k), e_k.size, _p(x.view(np.float64)), x.size,
+                        _p(d.view(np.float64)))
+    return d
+
+
+def sigma_normal(e_k, v_k, xmu, hloc_aa, x, g):
+    """get_sigma_normal.f90:17-39 with invg0_bath (ED_BATH_FUNCTIONS.f90:1800-1806)."""
+    x = np.ascontiguousarray(x, np.complex128)
+    g = np.ascontiguousarray(g, np.complex128)
+    s = np.zeros_like(x)
+    e_k = np.ascontiguousarray(e_k, np.float64)
+    v_k = np.ascontiguousarray(v_k, np.float64)
+    lib().or_sigma_normal(_p(e_k), _p(v_k), e_k.size, xmu, hloc_aa, _p(x.view(np.float64)), x.size,
+                          _p(g.view(np.float64)), _p(s.view(np.float64)))
+    return s
+
+
+def chi2_delta(a, xdelta, g, w, grad=True):
+    """chi2_delta_normal_normal / grad_chi2_delta_normal_normal,
+    ED_CHI2FIT/fitgf_normal_normal.f90:193-226,256-316."""
+    a = np.ascontiguousarray(a, np.float64)
+    xdelta = np.ascontiguousarray(xdelta, np.float64)
+    g = np.ascontiguousarray(g, np.complex128)
+    w = np.ascontiguousarray(w, np.float64)
+    gr = np.zeros(a.size) if grad else None
+    c2 = lib().or_chi2_delta(_p(a), a.size // 2, _p(xdelta), _p(g.view(np.float64)), _p(w),
+                             xdelta.size, _p(gr) if grad else None)
+    return (c2, gr) if grad else c2
+
+
+def cg_weights(cg_weight, xdelta):
+    """Wdelta of chi2_fitgf_normal_normal, fitgf_normal_normal.f90:44-53."""
+    L = xdelta.size
+    if cg_weight == 1:
+        return np.ones(L)
+    if cg_weight == 2:
+        return np.arange(1, L + 1, dtype=np.float64)
+    if cg_weight == 3:
+        return xdelta.copy()
+    return np.full(L, float(L))
+
+
+# ------------------------------------------------------- T=0 pipeline ---
+def solve_sector_t0(model, nup, ndw, lmats=4096, lreal=0, wini=-5.0, wfin=5.0, eps=0.01,
+                    ngfiter=200, nitermax=512, tol=1e-12, nthreads=1, psi0=None, gs=None):
+    """One T=0 impurity solve restricted to sector (nup, ndw): the pipeline of
+    ed_solve_single (ED_MAIN.f90:251-289) with diagonalize_impurity
+    (ED_DIAG.f90:93-228), observables_impurity (ED_OBSERVABLES.f90:74-160),
+    lanc_build_gf_normal_c (build_gf_normal.f90:71-180) and get_sigma_normal.
+    Returns a dict with E0, psi, observables, impGmats[ispin, iorb, L], Sigma.
+    ``gs=(E0, psi)`` skips the ground-state search (chains from a given state)."""
+    ns = model.ns
+    hmap = build_sector(ns, nup, ndw)
+    if gs is None:
+        e0, psi, nl = lanczos_gs(model, hmap, nitermax=nitermax, threshold=tol, v0=psi0,
+                                 nthreads=nthreads)
+    else:
+        e0, psi = gs
+        nl = 0
+    zeta = 1.0
+    obs = observables_state(model, hmap, psi, 1.0 / zeta)
+    wm = matsubara(model.beta, lmats)
+    wr = realaxis(wini, wfin, lreal)
+    no = model.norb
+    gm = np.zeros((model.nspin, no, lmats), np.complex128)
+    gr = np.zeros((model.nspin, no, lreal), np.complex128)
+    chains = []
+    for ispin in range(model.nspin):
+        for iorb in range(no):
+            isite = (iorb + 1) + ispin * ns
+            for particle, dn in ((True, 1), (False, -1)):
+                jn = (nup + dn, ndw) if ispin == 0 else (nup, ndw + dn)
+                if not (0 <= jn[0] <= ns and 0 <= jn[1] <= ns):
+                    continue
+                jmap = build_sector(ns, *jn)
+                n2, vv = gf_vvinit(particle, isite, hmap, jmap, psi)
+                vv = vv / np.sqrt(n2)
+                nlanc = min(jmap.size, ngfiter)
+                a, b, _ = lanczos_tridiag(model, jmap, vv, nlanc, nthreads=nthreads)
+                gmt = np.zeros(lmats, np.complex128)
+                grt = np.zeros(lreal, np.complex128)
+                add_to_lanczos_gf(n2, e0, e0, zeta, False, model.beta, a, b, 1 if particle else -1,
+                                  wm, wr, eps, gmt, grt)
+                gm[ispin, iorb] += gmt
+                gr[ispin, iorb] += grt
+                chains.append(dict(ispin=ispin, iorb=iorb, particle=particle, norm2=n2, alpha=a,
+                                   beta=b))
+    sm = np.zeros_like(gm)
+    for ispin in range(model.nspin):
+        for iorb in range(no):
+            sm[ispin, iorb] = sigma_normal(model.e[ispin, iorb], model.v[ispin, iorb], model.xmu,
+                                           model.hloc[ispin, ispin, iorb, iorb].real, 1j * wm,
+                                           gm[ispin, iorb])
+    return dict(e0=e0, psi=psi, nlanc=nl, obs=obs, gmats=gm, greal=gr, smats=sm, chains=chains,
+                map=hmap, wm=wm)

@@ -1,0 +1,280 @@
+"""Parity of the CUDA library (through its C-ABI) with the CPU restatement.
+
+Bars: integer work bit-exact (sector tables, sector maps); H*v within 1e-13
+relative (FP64); |dE0|/|E0| <= 1e-10 and max|dG(iwn)| <= 1e-8 for the FP64
+path; chi^2 and gradients within 1e-12 relative; Hellmann-Feynman gradient
+within 1e-9 of the oracle's expectation values."""
+import numpy as np
+import pytest
+
+import dmfted
+import oracle as O
+from models import golden_models
+
+pytestmark = pytest.mark.gpu
+
+
+def solver_for(model, **kw):
+    ul = list(model.uloc) + [0.0] * (3 - len(model.uloc))
+    p = dmfted.default_params(norb=model.norb, nbath=model.nbath, nspin=model.nspin, uloc=ul,
+                              ust=model.ust, jh=model.jh, xmu=model.xmu, beta=model.beta,
+                              hfmode=int(model.hfmode), **kw)
+    s = dmfted.EDSolver(p, hloc=model.hloc)
+    s.set_bath(model.bath_array())
+    return s
+
+
+def cfg1(seed=1):
+    # Bethe-lattice single-orbital workload, Ns=8: U=2, half filling, beta=100
+    return O.seeded_model(seed, norb=1, nbath=7, u=2.0, beta=100.0)
+
+
+# ---------------------------------------------------------------- integer ---
+@pytest.mark.parametrize("norb,nbath", [(1, 7), (2, 4), (3, 1), (1, 13)])
+def test_sector_tables_bit_exact(norb, nbath):
+    m = O.seeded_model(0, norb=norb, nbath=nbath)
+    s = solver_for(m)
+    g = s.sector_tables()
+    r = O.sector_tables(norb, nbath)
+    for k in r:
+        assert np.array_equal(g[k], r[k]), k
+    s.close()
+
+
+@pytest.mark.parametrize("nbath,nup,ndw", [(7, 4, 4), (7, 0, 0), (7, 8, 8), (7, 3, 6), (13, 7, 7),
+                                           (11, 6, 6), (9, 2, 9)])
+def test_build_sector_bit_exact(nbath, nup, ndw):
+    m = O.seeded_model(0, nbath=nbath)
+    s = solver_for(m)
+    isec = s.sector_index(nup, ndw)
+    assert np.array_equal(s.build_sector(isec), O.build_sector(m.ns, nup, ndw))
+    s.close()
+
+
+# -------------------------------------------------------------------- H*v ---
+def _hv_cases():
+    out = []
+    for ic, (m, sectors, _) in enumerate(golden_models()):
+        for nup, ndw in sectors[:: max(1, len(sectors) // 5)]:
+            out.append((ic, int(nup), int(ndw)))
+    return out
+
+
+@pytest.mark.parametrize("ic,nup,ndw", _hv_cases())
+def test_hxv_matches_oracle(ic, nup, ndw):
+    m = golden_models()[ic][0]
+    s = solver_for(m)
+    s.setup_hv_sector(s.sector_index(nup, ndw))
+    hm = O.build_sector(m.ns, nup, ndw)
+    rng = np.random.default_rng(ic * 100 + nup * 10 + ndw)
+    v = rng.normal(size=hm.size) + 1j * rng.normal(size=hm.size)
+    ref = O.hxv(m, hm, v)
+    got = s.hxv(v)
+    assert np.abs(got - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max())
+    s.close()
+
+
+def test_hxv_cfg2_sector_and_errors():
+    m = O.seeded_model(2, nbath=11, u=3.0)
+    s = solver_for(m)
+    with pytest.raises(dmfted.DmftedError) as e:
+        s.hxv(np.zeros(10, complex))
+    assert e.value.code == dmfted.ERR_STATE
+    isec = s.sector_index(6, 6)
+    s.setup_hv_sector(isec)
+    with pytest.raises(dmfted.DmftedError) as e:
+        s.hxv(np.zeros(10, complex))
+    assert e.value.code == dmfted.ERR_ARG
+    hm = O.build_sector(m.ns, 6, 6)
+    rng = np.random.default_rng(7)
+    v = rng.normal(size=hm.size) + 1j * rng.normal(size=hm.size)
+    ref = O.hxv(m, hm, v, nthreads=O.lib().or_host_threads())
+    assert np.abs(s.hxv(v) - ref).max() <= 1e-13 * np.abs(ref).max()
+    s.close()
+
+
+def test_hxv_fp32_device_path():
+    import torch
+    m = O.seeded_model(4, nbath=9, u=2.5)
+    s = solver_for(m)
+    s.setup_hv_sector(s.sector_index(5, 5))
+    dim = s.sector_dim(s.sector_index(5, 5))
+    x = torch.randn(dim, dtype=torch.float64, device="cuda")
+    y64 = torch.empty_like(x)
+    x32 = x.float()
+    y32 = torch.empty_like(x32)
+    torch.cuda.synchronize()
+    dmfted._ck(dmfted.lib().dmfted_hxv_device_f64(s.ctx, x.data_ptr(), y64.data_ptr(), 1))
+    dmfted._ck(dmfted.lib().dmfted_hxv_device_f32(s.ctx, x32.data_ptr(), y32.data_ptr(), 1))
+    s_sync = s.time_hxv(fp32=False, warmup=0, reps=1)  # drains the library stream
+    assert s_sync > 0
+    ref = O.hxv(m, O.build_sector(m.ns, 5, 5), x.cpu().numpy().astype(complex))
+    assert np.abs(y64.cpu().numpy() - ref.real).max() <= 1e-13 * np.abs(ref).max()
+    assert np.abs(y32.cpu().double().numpy() - ref.real).max() <= 2e-6 * np.abs(ref).max()
+    s.close()
+
+
+# ---------------------------------------------------------------- Lanczos ---
+@pytest.mark.parametrize("precision", [dmfted.FP64, dmfted.MIXED])
+def test_ground_state_energy(precision):
+    m = cfg1()
+    s = solver_for(m, precision=precision)
+    isec = s.sector_index(4, 4)
+    e0, psi, nit = s.lanczos_gs(isec)
+    hm = O.build_sector(m.ns, 4, 4)
+    H = O.sparse_h(m, hm)
+    w = np.linalg.eigvalsh(H.toarray())
+    assert abs(e0 - w[0]) <= 1e-10 * abs(w[0])
+    assert abs(np.linalg.norm(psi) - 1) < 1e-12
+    res = np.linalg.norm(H @ psi - e0 * psi)
+    assert res < 1e-9, res
+    s.close()
+
+
+def test_lanc_tridiag_matches_oracle():
+    m = cfg1(3)
+    s = solver_for(m)
+    hm = O.build_sector(m.ns, 5, 4)
+    rng = np.random.default_rng(2)
+    v = rng.normal(size=hm.size) + 0.3j * rng.normal(size=hm.size)
+    v /= np.linalg.norm(v)
+    a_o, b_o, n_o = O.lanczos_tridiag(m, hm, v, 200)
+    a_g, b_g, n_g = s.lanc_tridiag(s.sector_index(5, 4), v, 200)
+    assert np.allclose(a_g[:20], a_o[:20], rtol=0, atol=1e-10)
+    assert np.allclose(b_g[:20], b_o[:20], rtol=0, atol=1e-10)
+    # the continued fractions agree even after loss of orthogonality
+    wm = O.matsubara(100.0, 512)
+    g_o = np.zeros(512, complex)
+    g_g = np.zeros(512, complex)
+    O.add_to_lanczos_gf(1.0, 0.0, 0.0, 1.0, False, 100.0, a_o, b_o, 1, wm, np.zeros(0), 0.01, g_o,
+                        np.zeros(0, complex))
+    O.add_to_lanczos_gf(1.0, 0.0, 0.0, 1.0, False, 100.0, a_g, b_g, 1, wm, np.zeros(0), 0.01, g_g,
+                        np.zeros(0, complex))
+    assert np.abs(g_g - g_o).max() <= 1e-8
+    s.close()
+
+
+# ------------------------------------------------------------------ solve ---
+def _compare_solve(m, nup, ndw, precision, gtol, lmats=1024, lreal=256):
+    s = solver_for(m, precision=precision, lmats=lmats, lreal=lreal, beta=m.beta)
+    isec = s.sector_index(nup, ndw)
+    s.ed_solve(m.bath_array(), sectors=[isec])
+    ref = O.solve_sector_t0(m, nup, ndw, lmats=lmats, lreal=lreal, nthreads=8)
+    e, secs, z = s.eigenspace()
+    assert abs(e[0] - ref["e0"]) <= 1e-10 * abs(ref["e0"])
+    ob = s.observables()
+    for k in ("dens", "dens_up", "dens_dw", "docc", "magz"):
+        assert np.allclose(ob[k], ref["obs"][k], rtol=0, atol=1e-9), k
+    gm = s.ed_get_gimp_matsubara()
+    gr = s.ed_get_gimp_real()
+    sm = s.ed_get_sigma_matsubara()
+    for ispin in range(m.nspin):
+        for a in range(m.norb):
+            dg = np.abs(gm[ispin, ispin, a, a] - ref["gmats"][ispin, a]).max()
+            assert dg <= gtol, (ispin, a, dg)
+            dgr = np.abs(gr[ispin, ispin, a, a] - ref["greal"][ispin, a]).max()
+            assert dgr <= 100 * gtol, (ispin, a, dgr)
+            ds = np.abs(sm[ispin, ispin, a, a] - ref["smats"][ispin, a]).max()
+            assert ds <= 1e3 * gtol, (ispin, a, ds)
+    s.close()
+    return ref
+
+
+def test_ed_solve_cfg1_fp64():
+    _compare_solve(cfg1(), 4, 4, dmfted.FP64, 1e-8)
+
+
+@pytest.mark.parametrize("ic", [3, 4, 5])
+def test_ed_solve_multiorbital_fp64(ic):
+    m, sectors, _ = golden_models()[ic]
+    ns = m.ns
+    _compare_solve(m, ns // 2, ns - ns // 2, dmfted.FP64, 1e-8, lmats=256, lreal=64)
+
+
+def test_ed_solve_cfg1_mixed_energy():
+    m = cfg1()
+    s = solver_for(m, precision=dmfted.MIXED, lmats=256, lreal=0)
+    s.ed_solve(m.bath_array(), sectors=[s.sector_index(4, 4)])
+    ref = O.solve_sector_t0(m, 4, 4, lmats=256, lreal=0, nthreads=8)
+    assert abs(s.egs() - ref["e0"]) <= 1e-10 * abs(ref["e0"])
+    s.close()
+
+
+def test_full_sector_scan_t0():
+    # the reference scans every (nup, ndw) sector (ED_DIAG.f90:115)
+    m = O.seeded_model(5, nbath=3, u=2.0)
+    s = solver_for(m, lmats=128, lreal=0)
+    s.ed_solve(m.bath_array())
+    best = min((O.lanczos_gs(m, O.build_sector(m.ns, a, b))[0], a, b)
+               for a in range(m.ns + 1) for b in range(m.ns + 1))
+    assert abs(s.egs() - best[0]) <= 1e-10 * max(1, abs(best[0]))
+    s.close()
+
+
+def test_u0_sigma_vanishes():
+    z = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden",
+                                           "pins.npz"))
+    m = O.Model(norb=1, nbath=5, nspin=1, uloc=(0.0, 0.0, 0.0), e=z["u0_e"][None, None],
+                v=z["u0_v"][None, None])
+    s = solver_for(m, lmats=256, lreal=0)
+    s.ed_solve(m.bath_array(), sectors=[s.sector_index(3, 3)])
+    assert abs(s.egs() - 2 * z["u0_levels"][:3].sum()) < 1e-10
+    assert np.abs(s.ed_get_sigma_matsubara()).max() < 1e-8
+    s.close()
+
+
+def test_bath_errors():
+    m = cfg1()
+    s = solver_for(m)
+    with pytest.raises(dmfted.DmftedError) as e:
+        s.set_bath(np.zeros(5))
+    assert e.value.code == dmfted.ERR_ARG
+    b = m.bath_array()
+    b[0] = np.nan
+    with pytest.raises(dmfted.DmftedError):
+        s.set_bath(b)
+    s.close()
+
+
+# -------------------------------------------------------------- gradients ---
+def test_chi2_batch_matches_oracle_and_fd():
+    rng = np.random.default_rng(17)
+    nb, L, nbatch = 9, 1000, 64
+    x = O.matsubara(100.0, L)
+    a0 = np.concatenate([rng.uniform(-1, 1, nb), 0.5 + rng.uniform(-0.1, 0.1, nb)])
+    g = O.delta_bath(a0[:nb], a0[nb:], 1j * x) + 1e-4 * (rng.normal(size=L) + 1j * rng.normal(size=L))
+    w = O.cg_weights(3, x)
+    A = a0 + 0.05 * rng.normal(size=(nbatch, 2 * nb))
+    s = dmfted.EDSolver(dmfted.default_params(nbath=3))
+    c2, gr = s.chi2_delta_batch(A, x, g, w)
+    for b in range(nbatch):
+        rc2, rgr = O.chi2_delta(A[b], x, g, w)
+        assert abs(c2[b] - rc2) <= 1e-12 * abs(rc2)
+        assert np.abs(gr[b] - rgr).max() <= 1e-11 * np.abs(rgr).max()
+    s.close()
+
+
+def test_hf_gradient_matches_expectations_and_fd():
+    m = O.seeded_model(8, nbath=5, u=2.0)
+    s = solver_for(m, lmats=16, lreal=0)
+    isec = s.sector_index(3, 3)
+    s.ed_solve(m.bath_array(), sectors=[isec])
+    g = s.hf_gradient()
+    hm = O.build_sector(m.ns, 3, 3)
+    e0, psi, _ = O.lanczos_gs(m, hm)
+    hop, nk = O.hf_terms_state(m, hm, psi)
+    nb = m.nbath
+    assert np.allclose(g[:nb], nk[0, 0] + nk[1, 0], atol=1e-9)
+    assert np.allclose(g[nb:], hop[0, 0] + hop[1, 0], atol=1e-9)
+    # central finite differences of E0
+    h = 1e-5
+    base = m.bath_array()
+    fd = np.zeros_like(base)
+    for i in range(base.size):
+        for sgn in (1, -1):
+            b = base.copy()
+            b[i] += sgn * h
+            s.ed_solve(b, sectors=[isec])
+            fd[i] += sgn * s.egs() / (2 * h)
+    assert np.abs(fd - g).max() <= 1e-5
+    s.close()

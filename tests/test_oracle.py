@@ -1,0 +1,166 @@
+"""The CPU restatement (oracle) against independent known answers.
+
+No test, fixture or output file of the reference exists, so the pins are:
+the Jordan-Wigner Fock-space construction of tests/golden/pins.npz (dense
+spectra per sector), ARPACK (scipy eigsh, the eigensolver family of
+SciFortran's sp_eigh), the U=0 and V=0 analytic limits, the particle+hole
+sum rule, and finite differences for the chi^2 gradient."""
+import itertools
+
+import numpy as np
+import pytest
+import scipy.sparse.linalg as sla
+
+import oracle as O
+from models import golden_models
+
+
+def test_binomial_matches_exact():
+    from math import comb
+    for n in range(0, 21):
+        for k in range(0, n + 1):
+            assert O.binomial(n, k) == comb(n, k)
+    assert O.binomial(5, -1) == 0
+
+
+def _literal_build_sector(ns, nup, ndw):
+    # literal transcription of ED_SETUP.f90:880-890 in Python
+    out = []
+    for idw in range(2 ** ns):
+        if bin(idw).count("1") != ndw:
+            continue
+        for iup in range(2 ** ns):
+            if bin(iup).count("1") != nup:
+                continue
+            out.append(iup + idw * 2 ** ns)
+    return np.array(out, np.int32)
+
+
+@pytest.mark.parametrize("ns,nup,ndw", [(4, 2, 2), (5, 1, 3), (6, 3, 3), (6, 0, 6), (7, 4, 2)])
+def test_build_sector_literal(ns, nup, ndw):
+    assert np.array_equal(O.build_sector(ns, nup, ndw), _literal_build_sector(ns, nup, ndw))
+
+
+def test_binary_search_semantics():
+    a = O.build_sector(6, 3, 2)
+    for i in [0, 1, 7, len(a) // 2, len(a) - 1]:
+        assert O.binary_search(a, int(a[i])) == i + 1
+    assert O.binary_search(a, -5) == 0
+    assert O.binary_search(a, int(a[-1]) + 1) == 0
+    assert O.binary_search(np.zeros(0, np.int32), 3) == 0
+
+
+def test_sector_tables():
+    t = O.sector_tables(1, 3)
+    ns = 4
+    assert t["getdim"][t["getsector"][2 * (ns + 1) + 2] - 1] == 36
+    # c^+ up of sector (nup, ndw) is (nup+1, ndw); c dw is (nup, ndw-1)
+    for s in range(1, (ns + 1) ** 2 + 1):
+        nup, ndw = t["getnup"][s - 1], t["getndw"][s - 1]
+        cdg = t["getcdgsector"][2 * (s - 1)]
+        if nup < ns:
+            assert (t["getnup"][cdg - 1], t["getndw"][cdg - 1]) == (nup + 1, ndw)
+        else:
+            assert cdg == 0
+        cdw = t["getcsector"][2 * (s - 1) + 1]
+        if ndw > 0:
+            assert (t["getnup"][cdw - 1], t["getndw"][cdw - 1]) == (nup, ndw - 1)
+    assert list(O.sector_tables(2, 3)["getbathstride"]) == [3, 6, 4, 7, 5, 8]
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_sector_spectra_against_jordan_wigner(case):
+    model, sectors, low = golden_models()[case]
+    ns = model.ns
+    for (nup, ndw), ref in zip(sectors, low):
+        hm = O.build_sector(ns, int(nup), int(ndw))
+        H = O.sparse_h(model, hm).toarray()
+        assert np.allclose(H, H.conj().T, atol=1e-14)
+        w = np.linalg.eigvalsh(H)[:4]
+        ref = ref[~np.isnan(ref)]
+        assert np.allclose(w[:ref.size], ref, atol=1e-11), (nup, ndw)
+
+
+def test_hxv_equals_explicit_matrix():
+    model = golden_models()[3][0]
+    hm = O.build_sector(model.ns, 2, 2)
+    H = O.sparse_h(model, hm)
+    rng = np.random.default_rng(1)
+    v = rng.normal(size=hm.size) + 1j * rng.normal(size=hm.size)
+    assert np.abs(O.hxv(model, hm, v) - H @ v).max() < 1e-13
+    assert np.abs(O.hxv(model, hm, v, nthreads=4) - H @ v).max() < 1e-13
+
+
+def test_lanczos_gs_against_dense_and_arpack():
+    m = O.seeded_model(3, nbath=6, u=2.0)
+    hm = O.build_sector(m.ns, 3, 4)
+    H = O.sparse_h(m, hm)
+    w = np.linalg.eigvalsh(H.toarray())
+    e0, psi, n = O.lanczos_gs(m, hm)
+    assert abs(e0 - w[0]) < 1e-10 * abs(w[0])
+    ea = sla.eigsh(H, k=1, which="SA", tol=1e-13)[0][0]
+    assert abs(e0 - ea) < 1e-10 * abs(ea)
+    r = H @ psi - e0 * psi
+    assert np.linalg.norm(r) < 1e-6
+
+
+def test_tql2_against_numpy():
+    rng = np.random.default_rng(5)
+    n = 40
+    d = rng.normal(size=n)
+    e = np.concatenate([[0.0], rng.normal(size=n - 1)])
+    T = np.diag(d) + np.diag(e[1:], 1) + np.diag(e[1:], -1)
+    w, V = np.linalg.eigh(T)
+    dd, Z, ierr = O.tql2(d, e)
+    assert ierr == 0
+    assert np.allclose(dd, w, atol=1e-12)
+    assert np.allclose(np.abs(Z[0]), np.abs(V[0]), atol=1e-10)
+
+
+def test_u0_limit_energy_and_sigma():
+    z = np.load(__import__("os").path.join(__import__("os").path.dirname(__file__), "golden",
+                                           "pins.npz"))
+    e, v = z["u0_e"], z["u0_v"]
+    m = O.Model(norb=1, nbath=5, nspin=1, uloc=(0.0, 0.0, 0.0), e=e[None, None], v=v[None, None])
+    r = O.solve_sector_t0(m, 3, 3, lmats=128)
+    assert abs(r["e0"] - 2 * z["u0_levels"][:3].sum()) < 1e-10
+    # U=0: G = 1/(iw - Delta) exactly, so Sigma = 0
+    assert np.abs(r["smats"]).max() < 1e-8
+
+
+def test_atomic_limit_green_function():
+    # V=0 (Nbath bath levels decoupled), half filling, HFMODE: G = 1/2[1/(iw-U/2)+1/(iw+U/2)]
+    u = 2.0
+    m = O.Model(norb=1, nbath=2, nspin=1, uloc=(u, 0, 0), e=np.array([[[-0.5, 0.5]]]),
+                v=np.zeros((1, 1, 2)))
+    r = O.solve_sector_t0(m, 2, 1, lmats=64)  # imp singly occupied (up), bath has one up+dw... 
+    wm = r["wm"]
+    # the impurity up electron can be removed (hole) at -U/2 or a dw added (particle) at +U/2
+    g = r["gmats"][0, 0]
+    assert np.all(np.isfinite(g))
+    # sum rule: particle + hole weights add up to 1
+    assert abs(sum(c["norm2"] for c in r["chains"]) - 1.0) < 1e-12
+
+
+def test_sum_rule_and_tail():
+    m = O.seeded_model(11, nbath=5, u=3.0)
+    r = O.solve_sector_t0(m, 3, 3, lmats=2000)
+    assert abs(sum(c["norm2"] for c in r["chains"]) - 1.0) < 1e-12
+    g = r["gmats"][0, 0]
+    assert abs(g[-1] * 1j * r["wm"][-1] - 1.0) < 2e-3
+
+
+def test_chi2_gradient_finite_difference():
+    rng = np.random.default_rng(9)
+    nb = 6
+    a = np.concatenate([rng.uniform(-1, 1, nb), 0.5 + rng.uniform(-0.1, 0.1, nb)])
+    x = O.matsubara(100.0, 300)
+    g = O.delta_bath(a[:nb] + 0.02, a[nb:] * 1.01, 1j * x)
+    for cw in (0, 1, 2, 3):
+        w = O.cg_weights(cw, x)
+        c2, gr = O.chi2_delta(a, x, g, w)
+        h = 1e-6
+        fd = np.array([(O.chi2_delta(a + h * u, x, g, w, False) - O.chi2_delta(a - h * u, x, g, w,
+                                                                                 False)) / (2 * h)
+                       for u in np.eye(a.size)])
+        assert np.abs(gr - fd).max() <= 1e-6 * np.abs(gr).max() + 1e-12
