@@ -4,6 +4,7 @@
 // path.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -438,6 +439,8 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         c->nspin = p->nspin;
         c->ns = ns;
         c->device = p->device;
+        if (const char *e = getenv("DMFTED_HXV_NC")) c->tune_nc = atoi(e);
+        if (const char *e = getenv("DMFTED_MIXED_TOL32")) c->mixed_tol32 = atof(e);
         DM_CUDA(cudaSetDevice(c->device));
         DM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         const size_t nh = 2 * (size_t)c->nspin * c->nspin * c->norb * c->norb;

@@ -18,7 +18,8 @@
 namespace dmfted {
 
 __constant__ int64_t c_binom[(kMaxNs + 1) * (kMaxNs + 1)];  // C(b, i) at b*(kMaxNs+1)+i
-__constant__ int64_t c_class_off[kMaxNs + 2];
+__constant__ int64_t c_class_off[kMaxNs + 2];   // compact offsets (enumeration)
+__constant__ int64_t c_class_poff[kMaxNs + 2];  // padded storage offsets (32-element aligned)
 
 __device__ __forceinline__ int64_t binom_d(int b, int i) {
     return (i < 0 || b < 0 || i > b) ? 0 : c_binom[b * (kMaxNs + 1) + i];
@@ -40,7 +41,7 @@ __global__ void k_words(int ns, uint32_t *words, int32_t *rank) {
         rr -= binom_d(b, i);
         b--;
     }
-    words[g] = w;
+    words[c_class_poff[n] + r] = w;
     rank[w] = (int32_t)r;
 }
 
@@ -69,11 +70,12 @@ __global__ void k_ell_build(int ns, int norb, int nbath, int W, const uint32_t *
     if (g >= ((int64_t)1 << ns)) return;
     int n = 0;
     while (c_class_off[n + 1] <= g) n++;
-    const int64_t off = c_class_off[n];
-    const int64_t r = g - off;
+    const int64_t r = g - c_class_off[n];
+    const int64_t off = c_class_poff[n];
     const int64_t rows = binom_d(ns, n);
     uint32_t *erow = ell + (int64_t)W * off + r;
-    const uint32_t w = words[g];
+    const int64_t gs = off + r;  // storage index
+    const uint32_t w = words[gs];
     int e = 0;
     const int pv = norb * nbath;
     for (int a = 0; a < norb; a++)
@@ -99,15 +101,15 @@ __global__ void k_ell_build(int ns, int norb, int nbath, int W, const uint32_t *
                 e++;
             }
         }
-    cnt[g] = (uint8_t)e;
+    cnt[gs] = (uint8_t)e;
     double d = 0.0;
     for (int a = 0; a < norb; a++)
         for (int k = 0; k < nbath; k++) {
             const int ms = norb + a * nbath + k;
             if ((w >> ms) & 1u) d += ebath[a * nbath + k];
         }
-    diag[g] = d;
-    diag_f[g] = (float)d;
+    diag[gs] = d;
+    diag_f[gs] = (float)d;
 }
 
 // Combined sector map (ED_SETUP.f90:880-890): map[i] = iup + idw*2^Ns with
@@ -134,17 +136,26 @@ void fock_init(dmfted_ctx *c) {
         for (int i = 0; i <= b; i++) bt[b * (kMaxNs + 1) + i] = exact_binom(b, i);
     c->binom.assign(ns + 1, 0);
     c->class_off.assign(kMaxNs + 2, 0);
+    c->class_poff.assign(kMaxNs + 2, 0);
     for (int n = 0; n <= ns; n++) c->binom[n] = exact_binom(ns, n);
-    for (int n = 0; n <= kMaxNs; n++)
-        c->class_off[n + 1] = c->class_off[n] + (n <= ns ? c->binom[n] : 0);
+    for (int n = 0; n <= kMaxNs; n++) {
+        const int64_t cn = n <= ns ? c->binom[n] : 0;
+        c->class_off[n + 1] = c->class_off[n] + cn;
+        c->class_poff[n + 1] = c->class_poff[n] + (cn + 31) / 32 * 32;
+    }
     // classes beyond ns are empty; keep offsets monotone so the class search stops
     DM_CUDA(cudaMemcpyToSymbolAsync(c_binom, bt.data(), bt.size() * sizeof(int64_t), 0,
                                     cudaMemcpyHostToDevice, c->stream));
     DM_CUDA(cudaMemcpyToSymbolAsync(c_class_off, c->class_off.data(),
                                     c->class_off.size() * sizeof(int64_t), 0,
                                     cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyToSymbolAsync(c_class_poff, c->class_poff.data(),
+                                    c->class_poff.size() * sizeof(int64_t), 0,
+                                    cudaMemcpyHostToDevice, c->stream));
     c->nwords = (int64_t)1 << ns;
-    c->words.alloc(c->nwords);
+    c->nstore = c->class_poff[kMaxNs + 1];
+    c->words.alloc(c->nstore);
+    DM_CUDA(cudaMemsetAsync(c->words.p, 0, c->nstore * sizeof(uint32_t), c->stream));
     c->rank.alloc(c->nwords);
     k_words<<<div_up(c->nwords, 256), 256, 0, c->stream>>>(ns, c->words.p, c->rank.p);
     DM_CHECK_LAUNCH();
@@ -157,10 +168,11 @@ void fock_init(dmfted_ctx *c) {
     const int nsp = c->spin_shared ? 1 : 2;
     for (int s = 0; s < nsp; s++) {
         SpinTables &t = c->spin[s];
-        t.cnt.alloc(c->nwords);
-        t.ell.alloc((size_t)std::max(c->W, 1) * c->nwords);
-        t.diag.alloc(c->nwords);
-        t.diag_f.alloc(c->nwords);
+        t.cnt.alloc(c->nstore);
+        t.ell.alloc((size_t)std::max(c->W, 1) * c->nstore);
+        t.diag.alloc(c->nstore);
+        t.diag_f.alloc(c->nstore);
+        DM_CUDA(cudaMemsetAsync(t.cnt.p, 0, c->nstore, c->stream));
         t.par.alloc(c->P);
         t.par_f.alloc(c->P);
     }
@@ -273,8 +285,8 @@ SectorView sector_view(const dmfted_ctx *c, int isector) {
     s.dimup = c->binom[s.nup];
     s.dimdw = c->binom[s.ndw];
     s.dim = s.dimup * s.dimdw;
-    s.offup = c->class_off[s.nup];
-    s.offdw = c->class_off[s.ndw];
+    s.offup = c->class_poff[s.nup];
+    s.offdw = c->class_poff[s.ndw];
     return s;
 }
 

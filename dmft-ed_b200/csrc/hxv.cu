@@ -1,30 +1,66 @@
 // Kernels and launchers of the factored H*v; see hxv.cuh for the formulation.
 #include <algorithm>
+#include <cstring>
 
 #include "hxv.cuh"
 
 namespace dmfted {
 
-template <typename T, int NC, bool STAGE, bool LZ>
+// Vector helpers: VW consecutive elements, 16-byte aligned when VW > 1.
+template <typename E, int VW>
+__device__ __forceinline__ void vld(const E *p, E (&v)[VW]) {
+    if constexpr (VW == 1) {
+        v[0] = p[0];
+    } else if constexpr (sizeof(E) * VW == 16) {
+        const uint4 q = *reinterpret_cast<const uint4 *>(p);
+        memcpy(v, &q, 16);
+    } else if constexpr (sizeof(E) * VW == 8) {
+        const uint2 q = *reinterpret_cast<const uint2 *>(p);
+        memcpy(v, &q, 8);
+    } else if constexpr (sizeof(E) * VW == 4) {
+        const unsigned q = *reinterpret_cast<const unsigned *>(p);
+        memcpy(v, &q, 4);
+    } else {
+        const unsigned short q = *reinterpret_cast<const unsigned short *>(p);
+        memcpy(v, &q, 2);
+    }
+}
+template <typename E, int VW>
+__device__ __forceinline__ void vst(E *p, const E (&v)[VW]) {
+    if constexpr (VW == 1) {
+        p[0] = v[0];
+    } else if constexpr (sizeof(E) * VW == 16) {
+        uint4 q;
+        memcpy(&q, v, 16);
+        *reinterpret_cast<uint4 *>(p) = q;
+    } else {
+        uint2 q;
+        memcpy(&q, v, 8);
+        *reinterpret_cast<uint2 *>(p) = q;
+    }
+}
+
+constexpr int kDwBatch = 8;  // neighbour-column loads issued before their FMAs
+
+// Factored H*v.  Each CTA owns NC consecutive columns at a time; each thread
+// owns VW consecutive rows per pass (16-byte loads and stores).
+template <typename T, int NC, int VW, bool LZ>
 __global__ void __launch_bounds__(256) k_hxv(const HxvArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ T spu[kMaxParams], spd[kMaxParams];
+    __shared__ T spu[kMaxParams];
     __shared__ T sdint[64];
     __shared__ T sdd[NC];
     __shared__ unsigned simp[NC];
     __shared__ int scnt[NC];
-    __shared__ int64_t sbase[NC];
-    __shared__ uint32_t sent[NC * kMaxW];
+    __shared__ T sval[NC][kMaxW];
+    __shared__ int64_t soff[NC][kMaxW];
 
     if (LZ) {
         if (a.status[0]) return;  // chain finished: every later step is a no-op
     }
     const int tid = threadIdx.x, bd = blockDim.x;
     const int64_t dimup = a.dimup, dimdw = a.dimdw, ncols = dimdw * a.nstack;
-    for (int i = tid; i < a.P; i += bd) {
-        spu[i] = a.pu[i];
-        spd[i] = a.pd[i];
-    }
+    for (int i = tid; i < a.P; i += bd) spu[i] = a.pu[i];
     const int ni = 1 << a.norb;
     for (int i = tid; i < ni * ni; i += bd) sdint[i] = a.dint[i];
     const unsigned imask = (unsigned)ni - 1u;
@@ -43,66 +79,101 @@ __global__ void __launch_bounds__(256) k_hxv(const HxvArgs<T> a) {
     for (int64_t c0 = (int64_t)blockIdx.x * NC; c0 < ncols; c0 += (int64_t)gridDim.x * NC) {
         const int nc = (int)min((int64_t)NC, ncols - c0);
         __syncthreads();
-        const T *xc;
-        if (STAGE) {
-            for (int j = 0; j < nc; j++) {
-                const T *src = x + (c0 + j) * dimup;
-                T *dst = xs + (int64_t)j * dimup;
-                for (int64_t r = tid; r < dimup; r += bd) dst[r] = src[r];
+        // stage the own columns (one coalesced read of V)
+        for (int j = 0; j < nc; j++) {
+            const T *src = x + (c0 + j) * dimup;
+            T *dst = xs + (int64_t)j * dimup;
+#pragma unroll 4
+            for (int64_t r = (int64_t)tid * VW; r < dimup; r += (int64_t)bd * VW) {
+                T v[VW];
+                vld<T, VW>(src + r, v);
+                vst<T, VW>(dst + r, v);
             }
-            xc = xs;
-        } else {
-            xc = x + c0 * dimup;
         }
+        // column data and decoded down hops (value, element offset of the
+        // neighbour column)
         if (tid < nc) {
             const int64_t cg = c0 + tid, q = cg / dimdw, cc = cg - q * dimdw;
             scnt[tid] = a.cd[cc];
             simp[tid] = a.wd[cc] & imask;
             sdd[tid] = a.dd[cc];
-            sbase[tid] = q * dimdw;
         }
         for (int t = tid; t < nc * a.W; t += bd) {
             const int j = t / a.W, e = t % a.W;
-            const int64_t cc = (c0 + j) % dimdw;
-            if (e < (int)a.cd[cc]) sent[j * kMaxW + e] = a.ed[(int64_t)e * dimdw + cc];
+            const int64_t cg = c0 + j, q = cg / dimdw, cc = cg - q * dimdw;
+            if (e < (int)a.cd[cc]) {
+                const uint32_t en = a.ed[(int64_t)e * dimdw + cc];
+                T v = a.pd[ell_par(en)];
+                sval[j][e] = ell_neg(en) ? -v : v;
+                soff[j][e] = (q * dimdw + (int64_t)ell_col(en)) * dimup;
+            }
         }
         __syncthreads();
-        for (int64_t r = tid; r < dimup; r += bd) {
-            const unsigned iu = a.wu[r] & imask;
-            const T dur = a.du[r];
-            T acc[NC];
+        for (int64_t r = (int64_t)tid * VW; r < dimup; r += (int64_t)bd * VW) {
+            uint32_t wu[VW];
+            T du[VW];
+            uint8_t cu[VW];
+            vld<uint32_t, VW>(a.wu + r, wu);
+            vld<T, VW>(a.du + r, du);
+            vld<uint8_t, VW>(a.cu + r, cu);
+            T acc[NC][VW];
+            int cmax = 0;
 #pragma unroll
-            for (int j = 0; j < NC; j++)
-                if (j < nc) acc[j] = (dur + sdd[j] + sdint[iu * ni + simp[j]]) * xc[(int64_t)j * dimup + r];
-            const int cnt = a.cu[r];
-            for (int e = 0; e < cnt; e++) {
-                const uint32_t en = a.eu[(int64_t)e * dimup + r];
-                T v = spu[ell_par(en)];
-                if (ell_neg(en)) v = -v;
-                const int64_t col = ell_col(en);
+            for (int i = 0; i < VW; i++) {
+                cmax = max(cmax, (int)cu[i]);
 #pragma unroll
                 for (int j = 0; j < NC; j++)
-                    if (j < nc) acc[j] += v * xc[(int64_t)j * dimup + col];
+                    acc[j][i] = (j < nc) ? (du[i] + sdd[j] + sdint[(wu[i] & imask) * ni + simp[j]]) *
+                                               xs[(int64_t)j * dimup + r + i]
+                                         : T(0);
             }
+            // up hops: gathers from the staged columns
+            for (int e = 0; e < cmax; e++) {
+                uint32_t en[VW];
+                vld<uint32_t, VW>(a.eu + (int64_t)e * dimup + r, en);
+#pragma unroll
+                for (int i = 0; i < VW; i++) {
+                    if (e < (int)cu[i]) {
+                        T v = spu[ell_par(en[i])];
+                        if (ell_neg(en[i])) v = -v;
+                        const int64_t col = ell_col(en[i]);
+#pragma unroll
+                        for (int j = 0; j < NC; j++)
+                            if (j < nc) acc[j][i] += v * xs[(int64_t)j * dimup + col];
+                    }
+                }
+            }
+            // down hops: whole neighbour columns, loads batched for MLP
 #pragma unroll
             for (int j = 0; j < NC; j++) {
-                if (j >= nc) break;
-                const int ce = scnt[j];
-                const int64_t base = sbase[j];
-                for (int e = 0; e < ce; e++) {
-                    const uint32_t en = sent[j * kMaxW + e];
-                    T v = spd[ell_par(en)];
-                    if (ell_neg(en)) v = -v;
-                    acc[j] += v * x[(base + ell_col(en)) * dimup + r];
-                }
-                const int64_t idx = (c0 + j) * dimup + r;
-                if (LZ) {
-                    const double u = sc * (double)acc[j] - cprev * (double)a.xprev[idx];
-                    const T ut = (T)u;
-                    y[idx] = ut;
-                    dot.add((double)xc[(int64_t)j * dimup + r] * (double)ut);
-                } else {
-                    y[idx] = acc[j];
+                if (j < nc) {
+                    const int ce = scnt[j];
+                    for (int e0 = 0; e0 < ce; e0 += kDwBatch) {
+                        T xv[kDwBatch][VW];
+#pragma unroll
+                        for (int q = 0; q < kDwBatch; q++)
+                            if (e0 + q < ce) vld<T, VW>(x + soff[j][e0 + q] + r, xv[q]);
+#pragma unroll
+                        for (int q = 0; q < kDwBatch; q++)
+                            if (e0 + q < ce) {
+                                const T v = sval[j][e0 + q];
+#pragma unroll
+                                for (int i = 0; i < VW; i++) acc[j][i] += v * xv[q][i];
+                            }
+                    }
+                    const int64_t idx = (c0 + j) * dimup + r;
+                    if (LZ) {
+                        T xp[VW], ut[VW];
+                        vld<T, VW>(a.xprev + idx, xp);
+#pragma unroll
+                        for (int i = 0; i < VW; i++) {
+                            ut[i] = (T)(sc * (double)acc[j][i] - cprev * (double)xp[i]);
+                            dot.add((double)xs[(int64_t)j * dimup + r + i] * (double)ut[i]);
+                        }
+                        vst<T, VW>(y + idx, ut);
+                    } else {
+                        vst<T, VW>(y + idx, acc[j]);
+                    }
                 }
             }
         }
@@ -152,54 +223,64 @@ HxvArgs<T> make_hxv_args(const dmfted_ctx *c, const SectorView &s) {
 template HxvArgs<double> make_hxv_args<double>(const dmfted_ctx *, const SectorView &);
 template HxvArgs<float> make_hxv_args<float>(const dmfted_ctx *, const SectorView &);
 
-// Launch configuration: columns per CTA and whether the columns fit in
-// shared memory.  Picked from the column size; a column block of up to
-// ~56 KB keeps 3-4 CTAs resident per SM.
+// Launch configuration.  VW: 16-byte vectors when the column stride keeps
+// them aligned (DimUp*sizeof(T) a multiple of 16).  NC: two columns per CTA
+// when there are enough columns to fill the GPU, else one.  The staged
+// columns must fit in shared memory (DimUp*sizeof(T)*NC <= 200 KB).
 struct HxvCfg {
-    int nc;
-    bool stage;
+    int nc, vw, threads;
     size_t smem;
     int grid;
 };
 
+static bool al16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
 template <typename T>
-static HxvCfg hxv_config(dmfted_ctx *c, const SectorView &s, int nstack = 1) {
+static HxvCfg hxv_config(dmfted_ctx *c, const SectorView &s, const HxvArgs<T> &a, int nstack = 1) {
     HxvCfg g;
     const size_t col = (size_t)s.dimup * sizeof(T);
-    const size_t budget = 56 * 1024;
-    if (col * 4 <= budget) g.nc = 4;
-    else if (col * 2 <= budget) g.nc = 2;
-    else g.nc = 1;
-    g.stage = col * g.nc <= 200 * 1024;
-    g.smem = g.stage ? col * g.nc : 0;
-    int64_t blocks = (s.dimdw * nstack + g.nc - 1) / g.nc;
-    g.grid = (int)std::min<int64_t>(blocks, kMaxRedBlocks);
+    const int vmax = 16 / (int)sizeof(T);
+    // vector path: column stride and every base pointer 16-byte aligned
+    const bool aligned = al16(a.x) && al16(a.y) && (!a.xprev || al16(a.xprev)) && al16(a.wu) &&
+                         al16(a.du) && al16(a.eu) && (((uintptr_t)a.cu & (vmax - 1)) == 0) &&
+                         ((a.vstride * (int64_t)sizeof(T)) % 16 == 0);
+    g.vw = (s.dimup % vmax == 0 && aligned) ? vmax : 1;
+    const int64_t ncols = s.dimdw * nstack;
+    const int sms = num_sms(c);
+    g.nc = (ncols >= (int64_t)16 * sms && col * 2 <= 100 * 1024) ? 2 : 1;
+    if (c->tune_nc == 1 || (c->tune_nc == 2 && col * 2 <= 200 * 1024)) g.nc = c->tune_nc;
+    DM_REQUIRE(col * g.nc <= 200 * 1024, DMFTED_ERR_UNSUPPORTED,
+               "sector column too long for the shared-memory H*v (DimUp too large)");
+    g.threads = (s.dimup <= (int64_t)128 * g.vw * 2) ? 128 : 256;
+    g.smem = col * g.nc;
+    g.grid = (int)std::min<int64_t>((ncols + g.nc - 1) / g.nc, kMaxRedBlocks);
     return g;
 }
 
-template <typename T, int NC, bool STAGE, bool LZ>
+template <typename T, int NC, int VW, bool LZ>
 static void launch_nc(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
-    auto kern = k_hxv<T, NC, STAGE, LZ>;
+    auto kern = k_hxv<T, NC, VW, LZ>;
     static bool attr_set[64] = {false};
-    if (g.smem > 48 * 1024 && !attr_set[c->device & 63]) {
+    if (!attr_set[c->device & 63]) {
         DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      200 * 1024));
         attr_set[c->device & 63] = true;
     }
     dim3 grid(g.grid, nvec);
-    kern<<<grid, 256, g.smem, c->stream>>>(a);
+    kern<<<grid, g.threads, g.smem, c->stream>>>(a);
     DM_CHECK_LAUNCH();
     c->launches++;
 }
 
 template <typename T, bool LZ>
 static void launch_hxv(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
-    if (g.stage) {
-        if (g.nc == 4) launch_nc<T, 4, true, LZ>(c, a, g, nvec);
-        else if (g.nc == 2) launch_nc<T, 2, true, LZ>(c, a, g, nvec);
-        else launch_nc<T, 1, true, LZ>(c, a, g, nvec);
+    constexpr int VMAX = 16 / sizeof(T);
+    if (g.vw == VMAX) {
+        if (g.nc == 2) launch_nc<T, 2, VMAX, LZ>(c, a, g, nvec);
+        else launch_nc<T, 1, VMAX, LZ>(c, a, g, nvec);
     } else {
-        launch_nc<T, 1, false, LZ>(c, a, g, nvec);
+        if (g.nc == 2) launch_nc<T, 2, 1, LZ>(c, a, g, nvec);
+        else launch_nc<T, 1, 1, LZ>(c, a, g, nvec);
     }
 }
 
@@ -208,7 +289,7 @@ static void hxv_plain(dmfted_ctx *c, const SectorView &s, const T *x, T *y, int 
     HxvArgs<T> a = make_hxv_args<T>(c, s);
     a.x = x;
     a.y = y;
-    HxvCfg g = hxv_config<T>(c, s);
+    HxvCfg g = hxv_config<T>(c, s, a);
     launch_hxv<T, false>(c, a, g, nvec);
 }
 
@@ -235,7 +316,7 @@ void hxv_lanczos_step(dmfted_ctx *c, const SectorView &s, const T *x, const T *x
     a.k = k;
     a.partials = c->red_partials.p;
     a.counter = c->red_counter.p;
-    HxvCfg g = hxv_config<T>(c, s, nstack);
+    HxvCfg g = hxv_config<T>(c, s, a, nstack);
     launch_hxv<T, true>(c, a, g, 1);
 }
 template void hxv_lanczos_step<double>(dmfted_ctx *, const SectorView &, const double *,

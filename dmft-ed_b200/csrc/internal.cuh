@@ -2,15 +2,17 @@
 //
 // Device layout (one context per process/GPU):
 //   Fock tables, built once per dmfted_init, for ALL popcount classes n of
-//   Ns-bit words (2^Ns words in total):
-//     words[class_off[n] + r]   r-th Ns-bit word with popcount n, increasing
-//     rank[w]                   r such that words[class_off[popcount w] + r] == w
+//   Ns-bit words (2^Ns words in total).  Each class starts at a storage offset
+//   poff[n] padded to 32 elements, so 16-byte vector loads of any class are
+//   aligned:
+//     words[poff[n] + r]        r-th Ns-bit word with popcount n, increasing
+//     rank[w]                   r such that words[poff[popcount w] + r] == w
 //   Hopping tables per spin, rebuilt on every set_bath (they skip zero
 //   couplings as the reference's `if(V/=0)` tests do):
-//     cnt[class_off[n] + r]     hops of word r
-//     ell[W*class_off[n] + e*C(Ns,n) + r]  packed hop e of word r (ELL,
+//     cnt[poff[n] + r]          hops of word r
+//     ell[W*poff[n] + e*C(Ns,n) + r]  packed hop e of word r (ELL,
 //                               row-contiguous so a warp reads 32 rows at once)
-//     diag[class_off[n] + r]    sum_k e_k n_k of the word (bath energies)
+//     diag[poff[n] + r]         sum_k e_k n_k of the word (bath energies)
 //   A sector (nup, ndw) is a view: rows = class nup of the up tables,
 //   columns = class ndw of the down tables.  A sector vector is the
 //   DimUp x DimDw column-major matrix V[iup + DimUp*idw], which is exactly
@@ -141,7 +143,9 @@ struct dmfted_ctx {
     int W = 0;  // ELL width
     int P = 0;  // couplings per spin
     int64_t nwords = 0;
-    std::vector<int64_t> class_off;  // size ns+2
+    std::vector<int64_t> class_off;   // compact class offsets (size kMaxNs+2)
+    std::vector<int64_t> class_poff;  // storage offsets, each class padded to 32 elements
+    int64_t nstore = 0;               // padded length of the word-indexed tables
     std::vector<int64_t> binom;      // C(ns, n), n = 0..ns (exact integers)
     // host sector tables (1-based, as the reference)
     std::vector<int32_t> getsector, getnup, getndw, getdim, getdimup, getdimdw, getcsector,
@@ -177,6 +181,7 @@ struct dmfted_ctx {
     dmfted::DBuf<uint8_t> chainbuf;       // rotating vectors of a GF chain
     dmfted::DBuf<double> s64a, s64b, s64c;  // sector-sized FP64 scratch
     double mixed_tol32 = 1e-6;            // FP32-phase stopping tolerance of the mixed form
+    int tune_nc = 0;                      // H*v columns per CTA override (0 = automatic)
     dmfted::DBuf<double> d_wm, d_wr;      // Matsubara / real-axis grids
     dmfted::DBuf<double> d_bath_e, d_bath_v, d_hloc_aa;  // [nspin][norb][nbath], [nspin][norb]
     dmfted::DBuf<double> obs_d;           // observable accumulators of one state

@@ -21,6 +21,7 @@
 // check (the energy-change test of .repo/PLAIN_LANCZOS.f90:344-351).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "hxv.cuh"
@@ -29,8 +30,9 @@ namespace dmfted {
 
 enum { ST_DONE = 0, ST_STEPS = 1, ST_CONV = 2, ST_RITZ_VALID = 3, ST_BREAK = 4 };
 
-// w = u - a_k sc_k s_k (in place in u), then b_{k+1} = |w|.
-template <typename T>
+// w = u - a_k sc_k s_k (in place in u), then b_{k+1} = |w|.  VW elements
+// per thread per pass (16-byte accesses when n is a multiple of VW).
+template <typename T, int VW>
 __global__ void __launch_bounds__(kRedThreads) k_lz_update(T *u, const T *scur, int64_t n,
                                                            LanczosScalars lz, int k, double thr,
                                                            double *partials, unsigned *counter) {
@@ -38,12 +40,26 @@ __global__ void __launch_bounds__(kRedThreads) k_lz_update(T *u, const T *scur, 
     const double coef = lz.alpha[k] * lz.scale[k];
     CSum s;
     s.zero();
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const double w = (double)u[i] - coef * (double)scur[i];
-        const T wt = (T)w;
-        u[i] = wt;
-        s.add((double)wt * (double)wt);
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * VW; i < n;
+         i += (int64_t)gridDim.x * blockDim.x * VW) {
+        if constexpr (VW == 1) {
+            const T wt = (T)((double)u[i] - coef * (double)scur[i]);
+            u[i] = wt;
+            s.add((double)wt * (double)wt);
+        } else {
+            uint4 qu = *reinterpret_cast<const uint4 *>(u + i);
+            const uint4 qs = *reinterpret_cast<const uint4 *>(scur + i);
+            T a[VW], b[VW];
+            memcpy(a, &qu, 16);
+            memcpy(b, &qs, 16);
+#pragma unroll
+            for (int q = 0; q < VW; q++) {
+                a[q] = (T)((double)a[q] - coef * (double)b[q]);
+                s.add((double)a[q] * (double)a[q]);
+            }
+            memcpy(&qu, a, 16);
+            *reinterpret_cast<uint4 *>(u + i) = qu;
+        }
     }
     CSum arr[1] = {s};
     double tot[1];
@@ -61,6 +77,10 @@ __global__ void __launch_bounds__(kRedThreads) k_lz_update(T *u, const T *scur, 
         }
     }
 }
+
+template <typename T>
+static void launch_lz_update(dmfted_ctx *c, T *u, const T *scur, int64_t n, const LanczosScalars &lz,
+                             int k, double thr);
 
 // Start of a recurrence: scale[0] = 1/|s_0|, beta[0] = 0, status cleared.
 template <typename T>
@@ -345,6 +365,21 @@ static int red_grid(dmfted_ctx *c, int64_t n) {
                                   std::min(kMaxRedBlocks, 4 * num_sms(c)));
 }
 
+template <typename T>
+static void launch_lz_update(dmfted_ctx *c, T *u, const T *scur, int64_t n, const LanczosScalars &lz,
+                             int k, double thr) {
+    constexpr int VW = 16 / sizeof(T);
+    const bool vec = (n % VW == 0) && ((uintptr_t)u % 16 == 0) && ((uintptr_t)scur % 16 == 0);
+    if (vec)
+        k_lz_update<T, VW><<<red_grid(c, n / VW), kRedThreads, 0, c->stream>>>(
+            u, scur, n, lz, k, thr, c->red_partials.p, c->red_counter.p);
+    else
+        k_lz_update<T, 1><<<red_grid(c, n), kRedThreads, 0, c->stream>>>(
+            u, scur, n, lz, k, thr, c->red_partials.p, c->red_counter.p);
+    DM_CHECK_LAUNCH();
+    c->launches++;
+}
+
 static int ew_grid(dmfted_ctx *c, int64_t n) {
     return (int)std::min<int64_t>(std::max<int64_t>(div_up(n, 256), 1), 16 * num_sms(c));
 }
@@ -438,10 +473,7 @@ static LanczosResult gs_run(dmfted_ctx *c, const SectorView &s, double *psi, con
             const T *xp = basis + (size_t)(k > 0 ? k - 1 : k) * ld;
             T *y = basis + (size_t)(k + 1) * ld;
             hxv_lanczos_step<T>(c, s, x, xp, y, lz, k);
-            k_lz_update<T><<<rg, kRedThreads, 0, c->stream>>>(y, x, dim, lz, k, 1e-300,
-                                                               c->red_partials.p, c->red_counter.p);
-            DM_CHECK_LAUNCH();
-            c->launches++;
+            launch_lz_update<T>(c, y, x, dim, lz, k, 1e-300);
         }
         k_ritz_check<<<1, kRedThreads, ritz_smem(launched), c->stream>>>(lz, tol);
         DM_CHECK_LAUNCH();
@@ -512,10 +544,7 @@ static void chain_impl(dmfted_ctx *c, const SectorView &s, const double *v0,
     c->launches += 2;
     for (int k = 0; k < lz.kmax; k++) {
         hxv_lanczos_step<T>(c, s, Q, P, P, lz, k, nstack);
-        k_lz_update<T><<<red_grid(c, dim), kRedThreads, 0, c->stream>>>(
-            P, Q, dim, lz, k, c->p.lanc_gf_threshold, c->red_partials.p, c->red_counter.p);
-        DM_CHECK_LAUNCH();
-        c->launches++;
+        launch_lz_update<T>(c, P, Q, dim, lz, k, c->p.lanc_gf_threshold);
         std::swap(P, Q);
     }
 }

@@ -16,9 +16,10 @@ pytestmark = pytest.mark.gpu
 
 def solver_for(model, **kw):
     ul = list(model.uloc) + [0.0] * (3 - len(model.uloc))
-    p = dmfted.default_params(norb=model.norb, nbath=model.nbath, nspin=model.nspin, uloc=ul,
-                              ust=model.ust, jh=model.jh, xmu=model.xmu, beta=model.beta,
-                              hfmode=int(model.hfmode), **kw)
+    args = dict(norb=model.norb, nbath=model.nbath, nspin=model.nspin, uloc=ul, ust=model.ust,
+                jh=model.jh, xmu=model.xmu, beta=model.beta, hfmode=int(model.hfmode))
+    args.update(kw)
+    p = dmfted.default_params(**args)
     s = dmfted.EDSolver(p, hloc=model.hloc)
     s.set_bath(model.bath_array())
     return s
@@ -132,31 +133,46 @@ def test_ground_state_energy(precision):
 
 
 def test_lanc_tridiag_matches_oracle():
+    # sp_lanc_tridiag contract on the physical particle chain c^+_up |GS>
     m = cfg1(3)
     s = solver_for(m)
-    hm = O.build_sector(m.ns, 5, 4)
-    rng = np.random.default_rng(2)
-    v = rng.normal(size=hm.size) + 0.3j * rng.normal(size=hm.size)
-    v /= np.linalg.norm(v)
-    a_o, b_o, n_o = O.lanczos_tridiag(m, hm, v, 200)
-    a_g, b_g, n_g = s.lanc_tridiag(s.sector_index(5, 4), v, 200)
+    hi = O.build_sector(m.ns, 4, 4)
+    hj = O.build_sector(m.ns, 5, 4)
+    e0, psi, _ = O.lanczos_gs(m, hi)
+    n2, vv = O.gf_vvinit(True, 1, hi, hj, psi)
+    vv = vv / np.sqrt(n2)
+    a_o, b_o, n_o = O.lanczos_tridiag(m, hj, vv, 200)
+    a_g, b_g, n_g = s.lanc_tridiag(s.sector_index(5, 4), vv, 200)
+    assert n_g == 200
     assert np.allclose(a_g[:20], a_o[:20], rtol=0, atol=1e-10)
     assert np.allclose(b_g[:20], b_o[:20], rtol=0, atol=1e-10)
-    # the continued fractions agree even after loss of orthogonality
-    wm = O.matsubara(100.0, 512)
-    g_o = np.zeros(512, complex)
-    g_g = np.zeros(512, complex)
-    O.add_to_lanczos_gf(1.0, 0.0, 0.0, 1.0, False, 100.0, a_o, b_o, 1, wm, np.zeros(0), 0.01, g_o,
-                        np.zeros(0, complex))
-    O.add_to_lanczos_gf(1.0, 0.0, 0.0, 1.0, False, 100.0, a_g, b_g, 1, wm, np.zeros(0), 0.01, g_g,
-                        np.zeros(0, complex))
+    # the continued fractions agree after loss of orthogonality too
+    wm = O.matsubara(100.0, 1024)
+    g_o = np.zeros(1024, complex)
+    g_g = np.zeros(1024, complex)
+    for a, b, g in ((a_o, b_o, g_o), (a_g, b_g, g_g)):
+        O.add_to_lanczos_gf(n2, e0, e0, 1.0, False, 100.0, a, b, 1, wm, np.zeros(0), 0.01, g,
+                            np.zeros(0, complex))
     assert np.abs(g_g - g_o).max() <= 1e-8
+    s.close()
+
+
+def test_lanc_tridiag_complex_phase():
+    # a global complex phase on the start vector leaves alpha/beta unchanged
+    m = cfg1(4)
+    s = solver_for(m)
+    hj = O.build_sector(m.ns, 4, 5)
+    rng = np.random.default_rng(3)
+    v = rng.normal(size=hj.size)
+    a1, b1, _ = s.lanc_tridiag(s.sector_index(4, 5), v, 30)
+    a2, b2, _ = s.lanc_tridiag(s.sector_index(4, 5), v * np.exp(0.7j), 30)
+    assert np.allclose(a1, a2, atol=1e-12) and np.allclose(b1, b2, atol=1e-12)
     s.close()
 
 
 # ------------------------------------------------------------------ solve ---
 def _compare_solve(m, nup, ndw, precision, gtol, lmats=1024, lreal=256):
-    s = solver_for(m, precision=precision, lmats=lmats, lreal=lreal, beta=m.beta)
+    s = solver_for(m, precision=precision, lmats=lmats, lreal=lreal)
     isec = s.sector_index(nup, ndw)
     s.ed_solve(m.bath_array(), sectors=[isec])
     ref = O.solve_sector_t0(m, nup, ndw, lmats=lmats, lreal=lreal, nthreads=8)
