@@ -1,0 +1,334 @@
+"""Benchmark of the exact-diagonalization impurity solve on B200.
+
+Workload (one step): one impurity solve of the single-orbital Hubbard model on
+a Bethe-lattice bath, Ns=14 (Nbath=13), U=3, beta=100, half filling, sector
+nup=ndw=7 (dim 11,778,624): Lanczos ground state to the ARPACK-style residual
+tolerance 1e-12, observables, particle and hole Green's-function chains of 200
+steps, G and Sigma on Lmats=4096 Matsubara points.  Seeded synthetic bath:
+e_k ~ U[-1,1], V_k = 0.5 + U[-0.1,0.1] (numpy default_rng(seed)).
+
+The timed form is the mixed-precision solver (FP32 vectors, compensated FP64
+alpha/beta, FP64 refinement of the ground state, FP64 continued fractions);
+the plain-FP64 drop-in path is timed beside it on the same inputs and their
+differences are reported.
+
+Output: one JSON line (rank 0).  Multi-GPU: independent replicas (one solve
+per rank per step, weak scaling), launched with torch.distributed.run.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dmft-ed_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = ("DMFT-step solve time & H·v GB/s at Ns=14: mixed vs FP64 GPU, "
+          "|ΔE0|/|E0|≤1e-10")
+UNIT = "DMFT-steps/s"
+NBATH, U, BETA, LMATS, NGF, SEED = 13, 3.0, 100.0, 4096, 200, 1
+NUP = NDW = 7
+
+
+def seeded_bath(seed=SEED, nbath=NBATH):
+    rng = np.random.default_rng(seed)
+    e = rng.uniform(-1.0, 1.0, size=nbath)
+    v = 0.5 + rng.uniform(-0.1, 0.1, size=nbath)
+    return np.concatenate([e, v])
+
+
+def measured_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(name):
+    """Per-launch DRAM bytes of a kernel from its committed ncu summary
+    (profiles/<name>.md line 'dram_bytes_per_launch: N')."""
+    p = os.path.join(ROOT, "profiles", name + ".md")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def l2_flush(dev):
+    """Write a 256 MB buffer (> 126 MB L2) between timed steps."""
+    import torch
+    buf = getattr(l2_flush, "buf", None)
+    if buf is None:
+        buf = l2_flush.buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    buf.fill_(1.0)
+    torch.cuda.synchronize(dev)
+
+
+def make_solver(dmfted, precision, device):
+    p = dmfted.default_params(nbath=NBATH, uloc=[U], beta=BETA, xmu=0.0, lmats=LMATS, lreal=0,
+                              lanc_ngfiter=NGF, precision=precision, device=device)
+    return dmfted.EDSolver(p)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import dmfted
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    bath = seeded_bath()
+    pinned = torch.from_numpy(bath).pin_memory()
+    solvers = {prec: make_solver(dmfted, prec, local_rank) for prec in (dmfted.MIXED, dmfted.FP64)}
+    isec = solvers[dmfted.MIXED].sector_index(NUP, NDW)
+
+    def step(s):
+        s.ed_solve(pinned.numpy(), sectors=[isec])
+        return s.timings()["total_ms"]
+
+    def e2e_step(s):
+        # the public API with host buffers: bath from pinned host memory in,
+        # G, Sigma and the observables back to the host
+        t0 = time.perf_counter()
+        s.ed_solve(pinned.numpy(), sectors=[isec])
+        g = s.ed_get_gimp_matsubara()
+        sg = s.ed_get_sigma_matsubara()
+        ob = s.observables()
+        return (time.perf_counter() - t0) * 1e3, g, sg, ob
+
+    res = {}
+    for prec, s in solvers.items():
+        for _ in range(args.warmup):
+            step(s)
+            l2_flush(dev)
+        s.launch_count(reset=True)
+        dist_barrier(world)
+        ms = []
+        with ClockSampler(local_rank) as clk:
+            for _ in range(args.steps):
+                ms.append(step(s))
+                l2_flush(dev)
+        launches = s.launch_count(reset=True)
+        dist_barrier(world)
+        e2e = [e2e_step(s) for _ in range(max(1, min(args.steps, 3)))]
+        res[prec] = dict(ms=ms, clocks=clk.summary(), launches=launches, e2e_ms=[x[0] for x in e2e],
+                         g=e2e[-1][1], e0=s.egs(), obs=e2e[-1][3], tm=s.timings())
+    # H*v of the sector alone, both precisions (device events on the library stream)
+    s = solvers[dmfted.MIXED]
+    s.setup_hv_sector(isec)
+    dim = s.sector_dim(isec)
+    hv32 = s.time_hxv(fp32=True, warmup=5, reps=50)
+    hv64 = s.time_hxv(fp32=False, warmup=5, reps=50)
+    for sv in solvers.values():
+        sv.close()
+    return res, dim, hv32, hv64
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_sample(nthreads, n_hv):
+    """The oracle (CPU restatement of directMatVec_cc with the combined map and
+    binary search, complex128) on the same sector: n_hv products."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    m = O.seeded_model(SEED, nbath=NBATH, u=U, beta=BETA)
+    t0 = time.perf_counter()
+    hm = O.build_sector(m.ns, NUP, NDW)
+    t_map = time.perf_counter() - t0
+    v = O.start_vector(hm.size)
+    t0 = time.perf_counter()
+    for _ in range(n_hv):
+        v = O.hxv(m, hm, v, nthreads=nthreads)
+        v /= np.linalg.norm(v)
+    t_hv = (time.perf_counter() - t0) / n_hv
+    return t_map, t_hv
+
+
+def cpu_step_seconds(t_map, t_hv, hv_per_step):
+    return 3 * t_map + t_hv * hv_per_step
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    nthreads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        # the reference's algorithm on the host cores (the CPU restatement; the
+        # Fortran reference cannot be built here), rank 0 only
+        if rank != 0:
+            return
+        # one DMFT step of the reference = the H*v products of the GPU run's
+        # step (GS iterations, the eigenvector replay pass, 2 x 200 chain steps)
+        hv_per_step = 2 * 170 + 2 * NGF
+        samples = []
+        for i in range(args.warmup + args.steps):
+            t_map, t_hv = cpu_sample(nthreads, 1)
+            if i >= args.warmup:
+                samples.append(cpu_step_seconds(t_map, t_hv, hv_per_step))
+        sec = statistics.mean(samples)
+        val = 1.0 / sec
+        line = dict(metric=METRIC, value=val, unit=UNIT, n_gpus=args.gpus, steps=args.steps,
+                    warmup=args.warmup, ms_per_step=sec * 1e3, higher_is_better=True,
+                    scaling="weak", vs_baseline=None, dtype="c128", data="synthetic",
+                    impl="reference",
+                    config={"workload": "impurity solve Ns=14 (Nbath=13) sector 7/7 dim 11778624, "
+                                        "GS + G(iwn) Lmats=4096, 200-step chains",
+                            "parallelism": "host threads"},
+                    cpu_baseline=dict(value=val, unit=UNIT, cores=nthreads, kind="port",
+                                      sample=f"per step: 1 oracle directMatVec_cc (complex128, "
+                                             f"binary-search map) on the 7/7 sector with {nthreads} "
+                                             f"threads + the map build, scaled to {hv_per_step} "
+                                             f"H*v per DMFT step"),
+                    e2e=dict(value=val, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+        print(json.dumps(line))
+        return
+
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    import dmfted
+    res, dim, hv32, hv64 = run_ours(args, rank, world, local_rank)
+    mixed, fp64 = res[dmfted.MIXED], res[dmfted.FP64]
+    t_mixed = max_over_ranks(sum(mixed["ms"]) / 1e3, world)
+    t_fp64 = max_over_ranks(sum(fp64["ms"]) / 1e3, world)
+    t_e2e = max_over_ranks(statistics.mean(mixed["e2e_ms"]) / 1e3, world)
+    value = world * args.steps / t_mixed
+    peak, peak_kind = measured_peak_gbs()
+    hv_bytes32 = 2 * dim * 4
+    achieved = hv_bytes32 / (hv32 * 1e-3) / 1e9
+    traffic = ncu_traffic("k_hxv_ns14_fp32")
+    g_err = float(np.abs(mixed["g"] - fp64["g"]).max())
+    e_err = abs(mixed["e0"] - fp64["e0"]) / abs(fp64["e0"])
+    if world > 1:
+        dist_barrier(world)
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    line = dict(
+        metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps,
+        warmup=args.warmup, ms_per_step=t_mixed / args.steps * 1e3, higher_is_better=True,
+        scaling="weak", vs_baseline=None, dtype="f32+f64", data="synthetic",
+        config={"workload": "impurity solve Ns=14 (Nbath=13, U=3, beta=100) sector 7/7 "
+                            "dim 11778624: Lanczos GS (residual tol 1e-12) + observables + "
+                            "particle/hole chains (200 steps) + G, Sigma on Lmats=4096",
+                "precision": "mixed (FP32 vectors, compensated FP64 alpha/beta, FP64 refinement)",
+                "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between steps",
+                "seed": SEED},
+        fp64_dropin=dict(ms_per_step=t_fp64 / args.steps * 1e3,
+                         speedup_mixed_vs_fp64=t_fp64 / t_mixed,
+                         mixed_vs_fp64_dE0_rel=e_err, mixed_vs_fp64_max_dG=g_err),
+        hv=dict(dim=dim, fp32_us=hv32 * 1e3, fp64_us=hv64 * 1e3,
+                fp32_gbs=hv_bytes32 / (hv32 * 1e-3) / 1e9,
+                fp64_gbs=2 * dim * 8 / (hv64 * 1e-3) / 1e9,
+                hv_per_sec_fp32=1e3 / hv32),
+        phases_ms=dict(mixed=mixed["tm"], fp64=fp64["tm"]),
+        roofline=dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s",
+                      frac=achieved / peak, traffic=traffic, kernel="k_hxv<float> (plain H*v)",
+                      peak_source=peak_kind,
+                      bytes_per_launch=hv_bytes32),
+        e2e=dict(value=world / t_e2e, unit=UNIT, h2d_bytes_per_step=2 * NBATH * 8,
+                 d2h_bytes_per_step=2 * LMATS * 16 + 5 * 8),
+        gpu_launches=int(mixed["launches"]),
+        clocks=mixed["clocks"],
+    )
+    if not args.no_cpu_baseline and world == 1:
+        hv_per_step = 2 * 170 + 2 * NGF
+        t_map, t_hv = cpu_sample(nthreads, 2)
+        sec = cpu_step_seconds(t_map, t_hv, hv_per_step)
+        line["cpu_baseline"] = dict(
+            value=1.0 / sec, unit=UNIT, cores=nthreads, kind="port",
+            sample=f"2 oracle directMatVec_cc products (complex128, binary-search map, "
+                   f"{nthreads} threads) on the 7/7 sector + the map build, scaled to "
+                   f"{hv_per_step} H*v per DMFT step; {t_hv:.2f} s per H*v")
+    print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

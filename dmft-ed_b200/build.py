@@ -32,9 +32,10 @@ def _stale():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False):
-    """Compile every .cu file to an object and link libdmfted.so."""
-    if not force and not _stale():
+def build(force=False, verbose=False, checked=False):
+    """Compile every .cu file to an object and link libdmfted.so.  checked=True
+    adds the device-side index checks (-DDMFTED_DEVICE_CHECKS)."""
+    if not force and not checked and not _stale():
         return OUT
     nvcc = os.environ.get("NVCC", "nvcc")
     objdir = os.path.join(HERE, "_build")
@@ -42,7 +43,8 @@ def build(force=False, verbose=False):
     objs = []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c",
+        extra = ["-DDMFTED_DEVICE_CHECKS"] if checked else []
+        cmd = [nvcc, *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-c",
                os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
@@ -54,5 +56,6 @@ def build(force=False, verbose=False):
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    build(force="--force" in sys.argv or "--checked" in sys.argv, verbose="-v" in sys.argv,
+          checked="--checked" in sys.argv)
     print(OUT)

@@ -129,14 +129,15 @@ static int64_t states_used(const dmfted_ctx *c) {
 }
 
 static void states_add(dmfted_ctx *c, double e, int isector, const double *psi, int64_t dim) {
-    const int64_t off = (states_used(c) + 31) / 32 * 32;
+    const int64_t used = states_used(c);        // elements in use (<= states64.n)
+    const int64_t off = (used + 31) / 32 * 32;  // 256-byte aligned start of the new vector
     if ((size_t)(off + dim) > c->states64.n) {
         const size_t cap = std::max<size_t>((size_t)(off + dim), c->states64.n * 2);
         double *np = nullptr;
         cudaError_t err = cudaMalloc((void **)&np, cap * sizeof(double));
         DM_REQUIRE(err == cudaSuccess, DMFTED_ERR_NOMEM, "cudaMalloc for the eigenspace failed");
-        if (c->states64.p && off > 0)
-            DM_CUDA(cudaMemcpyAsync(np, c->states64.p, off * sizeof(double),
+        if (c->states64.p && used > 0)
+            DM_CUDA(cudaMemcpyAsync(np, c->states64.p, used * sizeof(double),
                                     cudaMemcpyDeviceToDevice, c->stream));
         DM_CUDA(cudaStreamSynchronize(c->stream));
         c->states64.release();
@@ -145,6 +146,7 @@ static void states_add(dmfted_ctx *c, double e, int isector, const double *psi, 
     }
     DM_CUDA(cudaMemcpyAsync(c->states64.p + off, psi, dim * sizeof(double), cudaMemcpyDeviceToDevice,
                             c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));  // psi is a scratch buffer the next sector reuses
     // energy-ordered insertion after equal energies (es_insert_state_c,
     // ED_EIGENSPACE.f90:157-213: traverse until e <= next)
     auto it = c->states.begin();
@@ -489,10 +491,14 @@ int dmfted_free(dmfted_ctx *c) {
     API_BEGIN
     if (!c) return DMFTED_OK;
     cudaSetDevice(c->device);
-    if (c->stream) cudaStreamSynchronize(c->stream);
+    // a device error still pending from this context's last work is reported
+    // here rather than left for the next context to trip over
+    cudaError_t pending = c->stream ? cudaStreamSynchronize(c->stream) : cudaSuccess;
     cudaStream_t st = c->stream;
     delete c;
     if (st) cudaStreamDestroy(st);
+    DM_REQUIRE(pending == cudaSuccess, DMFTED_ERR_CUDA,
+               std::string("device error pending at free: ") + cudaGetErrorString(pending));
     API_END
 }
 

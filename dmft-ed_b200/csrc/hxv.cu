@@ -41,9 +41,13 @@ __device__ __forceinline__ void vst(E *p, const E (&v)[VW]) {
 }
 
 constexpr int kDwBatch = 8;  // neighbour-column loads issued before their FMAs
+constexpr int kUpBatch = 8;  // hopping-table entries prefetched per row vector
 
-// Factored H*v.  Each CTA owns NC consecutive columns at a time; each thread
-// owns VW consecutive rows per pass (16-byte loads and stores).
+// Factored H*v.  A CTA owns a tile of NC consecutive columns, staged in
+// shared memory row-interleaved (xs[row*NC + j]) so that one up-hop gather is
+// a single NC-wide load serving all NC columns.  Each thread owns VW
+// consecutive rows per pass (16-byte global loads and stores).  The down hops
+// stream whole neighbour columns from L2/HBM with kDwBatch loads in flight.
 template <typename T, int NC, int VW, bool LZ>
 __global__ void __launch_bounds__(256) k_hxv(const HxvArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -72,40 +76,56 @@ __global__ void __launch_bounds__(256) k_hxv(const HxvArgs<T> a) {
     }
     const T *x = a.x + (int64_t)blockIdx.y * a.vstride;
     T *y = a.y + (int64_t)blockIdx.y * a.vstride;
-    T *xs = reinterpret_cast<T *>(smem_raw);
+    T *xs = reinterpret_cast<T *>(smem_raw);  // [dimup][NC]
     CSum dot;
     dot.zero();
 
     for (int64_t c0 = (int64_t)blockIdx.x * NC; c0 < ncols; c0 += (int64_t)gridDim.x * NC) {
         const int nc = (int)min((int64_t)NC, ncols - c0);
         __syncthreads();
-        // stage the own columns (one coalesced read of V)
-        for (int j = 0; j < nc; j++) {
-            const T *src = x + (c0 + j) * dimup;
-            T *dst = xs + (int64_t)j * dimup;
-#pragma unroll 4
-            for (int64_t r = (int64_t)tid * VW; r < dimup; r += (int64_t)bd * VW) {
-                T v[VW];
-                vld<T, VW>(src + r, v);
-                vst<T, VW>(dst + r, v);
+        // stage the tile: NC column loads per row vector, transposed in registers
+        for (int64_t r = (int64_t)tid * VW; r < dimup; r += (int64_t)bd * VW) {
+            T v[NC][VW];
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                if (j < nc && DM_IN((c0 + j) * dimup + r + VW - 1, ncols * dimup)) {
+                    vld<T, VW>(x + (c0 + j) * dimup + r, v[j]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < VW; i++) v[j][i] = T(0);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < VW; i++) {
+                T row[NC];
+#pragma unroll
+                for (int j = 0; j < NC; j++) row[j] = v[j][i];
+                if (DM_IN((r + i) * NC + NC - 1, dimup * NC)) vst<T, NC>(xs + (r + i) * NC, row);
             }
         }
         // column data and decoded down hops (value, element offset of the
         // neighbour column)
         if (tid < nc) {
-            const int64_t cg = c0 + tid, q = cg / dimdw, cc = cg - q * dimdw;
+            const int64_t cg = c0 + tid, q = cg / dimdw;
+            const int64_t cc = DM_IN(cg - q * dimdw, dimdw) ? cg - q * dimdw : 0;
             scnt[tid] = a.cd[cc];
             simp[tid] = a.wd[cc] & imask;
             sdd[tid] = a.dd[cc];
+        } else if (tid < NC) {
+            // unused columns of a partial tile: defined values, never stored
+            scnt[tid] = 0;
+            simp[tid] = 0;
+            sdd[tid] = T(0);
         }
         for (int t = tid; t < nc * a.W; t += bd) {
             const int j = t / a.W, e = t % a.W;
             const int64_t cg = c0 + j, q = cg / dimdw, cc = cg - q * dimdw;
-            if (e < (int)a.cd[cc]) {
+            if (e < (int)a.cd[cc] && DM_IN(e, kMaxW) && DM_IN(e, a.W)) {
                 const uint32_t en = a.ed[(int64_t)e * dimdw + cc];
-                T v = a.pd[ell_par(en)];
+                const bool ok = DM_IN(ell_par(en), a.P) && DM_IN(ell_col(en), dimdw);
+                T v = ok ? a.pd[ell_par(en)] : T(0);
                 sval[j][e] = ell_neg(en) ? -v : v;
-                soff[j][e] = (q * dimdw + (int64_t)ell_col(en)) * dimup;
+                soff[j][e] = ok ? (q * dimdw + (int64_t)ell_col(en)) * dimup : 0;
             }
         }
         __syncthreads();
@@ -113,6 +133,7 @@ __global__ void __launch_bounds__(256) k_hxv(const HxvArgs<T> a) {
             uint32_t wu[VW];
             T du[VW];
             uint8_t cu[VW];
+            if (!DM_IN(r + VW - 1, dimup)) break;
             vld<uint32_t, VW>(a.wu + r, wu);
             vld<T, VW>(a.du + r, du);
             vld<uint8_t, VW>(a.cu + r, cu);
@@ -121,25 +142,32 @@ __global__ void __launch_bounds__(256) k_hxv(const HxvArgs<T> a) {
 #pragma unroll
             for (int i = 0; i < VW; i++) {
                 cmax = max(cmax, (int)cu[i]);
+                T xr[NC];
+                vld<T, NC>(xs + (r + i) * NC, xr);
 #pragma unroll
                 for (int j = 0; j < NC; j++)
-                    acc[j][i] = (j < nc) ? (du[i] + sdd[j] + sdint[(wu[i] & imask) * ni + simp[j]]) *
-                                               xs[(int64_t)j * dimup + r + i]
-                                         : T(0);
+                    acc[j][i] = (du[i] + sdd[j] + sdint[(wu[i] & imask) * ni + (simp[j] & imask)]) * xr[j];
             }
-            // up hops: gathers from the staged columns
-            for (int e = 0; e < cmax; e++) {
-                uint32_t en[VW];
-                vld<uint32_t, VW>(a.eu + (int64_t)e * dimup + r, en);
+            // up hops: table entries prefetched, then NC-wide gathers
+            for (int e0 = 0; e0 < cmax; e0 += kUpBatch) {
+                uint32_t en[kUpBatch][VW];
 #pragma unroll
-                for (int i = 0; i < VW; i++) {
-                    if (e < (int)cu[i]) {
-                        T v = spu[ell_par(en[i])];
-                        if (ell_neg(en[i])) v = -v;
-                        const int64_t col = ell_col(en[i]);
+                for (int q = 0; q < kUpBatch; q++)
+                    if (e0 + q < cmax && DM_IN(e0 + q, a.W))
+                        vld<uint32_t, VW>(a.eu + (int64_t)(e0 + q) * dimup + r, en[q]);
 #pragma unroll
-                        for (int j = 0; j < NC; j++)
-                            if (j < nc) acc[j][i] += v * xs[(int64_t)j * dimup + col];
+                for (int q = 0; q < kUpBatch; q++) {
+#pragma unroll
+                    for (int i = 0; i < VW; i++) {
+                        if (e0 + q < (int)cu[i] && DM_IN(ell_col(en[q][i]), dimup) &&
+                            DM_IN(ell_par(en[q][i]), a.P)) {
+                            T v = spu[ell_par(en[q][i])];
+                            if (ell_neg(en[q][i])) v = -v;
+                            T xg[NC];
+                            vld<T, NC>(xs + (int64_t)ell_col(en[q][i]) * NC, xg);
+#pragma unroll
+                            for (int j = 0; j < NC; j++) acc[j][i] += v * xg[j];
+                        }
                     }
                 }
             }
@@ -152,7 +180,8 @@ __global__ void __launch_bounds__(256) k_hxv(const HxvArgs<T> a) {
                         T xv[kDwBatch][VW];
 #pragma unroll
                         for (int q = 0; q < kDwBatch; q++)
-                            if (e0 + q < ce) vld<T, VW>(x + soff[j][e0 + q] + r, xv[q]);
+                            if (e0 + q < ce && DM_IN(soff[j][e0 + q] + r + VW - 1, ncols * dimup))
+                                vld<T, VW>(x + soff[j][e0 + q] + r, xv[q]);
 #pragma unroll
                         for (int q = 0; q < kDwBatch; q++)
                             if (e0 + q < ce) {
@@ -162,13 +191,14 @@ __global__ void __launch_bounds__(256) k_hxv(const HxvArgs<T> a) {
                             }
                     }
                     const int64_t idx = (c0 + j) * dimup + r;
+                    if (!DM_IN(idx + VW - 1, ncols * dimup)) continue;
                     if (LZ) {
                         T xp[VW], ut[VW];
                         vld<T, VW>(a.xprev + idx, xp);
 #pragma unroll
                         for (int i = 0; i < VW; i++) {
                             ut[i] = (T)(sc * (double)acc[j][i] - cprev * (double)xp[i]);
-                            dot.add((double)xs[(int64_t)j * dimup + r + i] * (double)ut[i]);
+                            dot.add((double)xs[(r + i) * NC + j] * (double)ut[i]);
                         }
                         vst<T, VW>(y + idx, ut);
                     } else {
@@ -233,26 +263,27 @@ struct HxvCfg {
     int grid;
 };
 
-static bool al16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+static bool aligned_to(const void *p, size_t b) { return ((uintptr_t)p % b) == 0; }
 
 template <typename T>
 static HxvCfg hxv_config(dmfted_ctx *c, const SectorView &s, const HxvArgs<T> &a, int nstack = 1) {
     HxvCfg g;
-    const size_t col = (size_t)s.dimup * sizeof(T);
-    const int vmax = 16 / (int)sizeof(T);
-    // vector path: column stride and every base pointer 16-byte aligned
-    const bool aligned = al16(a.x) && al16(a.y) && (!a.xprev || al16(a.xprev)) && al16(a.wu) &&
-                         al16(a.du) && al16(a.eu) && (((uintptr_t)a.cu & (vmax - 1)) == 0) &&
-                         ((a.vstride * (int64_t)sizeof(T)) % 16 == 0);
-    g.vw = (s.dimup % vmax == 0 && aligned) ? vmax : 1;
+    // two rows per thread-vector: 8-byte (FP32) or 16-byte (FP64) accesses;
+    // needs DimUp even and every base pointer aligned to the vector size
+    const size_t vb = 2 * sizeof(T);
+    const bool aligned = aligned_to(a.x, vb) && aligned_to(a.y, vb) &&
+                         (!a.xprev || aligned_to(a.xprev, vb)) && aligned_to(a.wu, 8) &&
+                         aligned_to(a.du, vb) && aligned_to(a.eu, 8) && aligned_to(a.cu, 2) &&
+                         ((a.vstride * (int64_t)sizeof(T)) % vb == 0);
+    g.vw = (s.dimup % 2 == 0 && aligned) ? 2 : 1;
     const int64_t ncols = s.dimdw * nstack;
-    const int sms = num_sms(c);
-    g.nc = (ncols >= (int64_t)16 * sms && col * 2 <= 100 * 1024) ? 2 : 1;
-    if (c->tune_nc == 1 || (c->tune_nc == 2 && col * 2 <= 200 * 1024)) g.nc = c->tune_nc;
-    DM_REQUIRE(col * g.nc <= 200 * 1024, DMFTED_ERR_UNSUPPORTED,
+    g.nc = 16 / (int)sizeof(T);  // one 16-byte gather serves the whole tile
+    const size_t tile = (size_t)s.dimup * sizeof(T) * g.nc;
+    DM_REQUIRE(tile <= 200 * 1024, DMFTED_ERR_UNSUPPORTED,
                "sector column too long for the shared-memory H*v (DimUp too large)");
     g.threads = (s.dimup <= (int64_t)128 * g.vw * 2) ? 128 : 256;
-    g.smem = col * g.nc;
+    g.smem = tile;
     g.grid = (int)std::min<int64_t>((ncols + g.nc - 1) / g.nc, kMaxRedBlocks);
     return g;
 }
@@ -274,14 +305,9 @@ static void launch_nc(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int n
 
 template <typename T, bool LZ>
 static void launch_hxv(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
-    constexpr int VMAX = 16 / sizeof(T);
-    if (g.vw == VMAX) {
-        if (g.nc == 2) launch_nc<T, 2, VMAX, LZ>(c, a, g, nvec);
-        else launch_nc<T, 1, VMAX, LZ>(c, a, g, nvec);
-    } else {
-        if (g.nc == 2) launch_nc<T, 2, 1, LZ>(c, a, g, nvec);
-        else launch_nc<T, 1, 1, LZ>(c, a, g, nvec);
-    }
+    constexpr int NCT = 16 / sizeof(T);
+    if (g.vw == 2) launch_nc<T, NCT, 2, LZ>(c, a, g, nvec);
+    else launch_nc<T, NCT, 1, LZ>(c, a, g, nvec);
 }
 
 template <typename T>

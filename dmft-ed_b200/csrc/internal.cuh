@@ -64,6 +64,22 @@ const char *last_error();
 
 #define DM_CHECK_LAUNCH() DM_CUDA(cudaGetLastError())
 
+// Device-side index checks of a checked build (-DDMFTED_DEVICE_CHECKS): an
+// out-of-range index is reported with printf and the access is skipped, so a
+// bad launch shows where it went wrong instead of faulting.  Compiles to
+// `true` in the normal build.
+#ifdef DMFTED_DEVICE_CHECKS
+__device__ __forceinline__ bool dm_in(int64_t i, int64_t n, int line) {
+    if (i >= 0 && i < n) return true;
+    printf("dmfted device check failed: line %d block %d thread %d index %lld extent %lld\n", line,
+           (int)blockIdx.x, (int)threadIdx.x, (long long)i, (long long)n);
+    return false;
+}
+#define DM_IN(i, n) ::dmfted::dm_in((int64_t)(i), (int64_t)(n), __LINE__)
+#else
+#define DM_IN(i, n) true
+#endif
+
 #define DM_REQUIRE(cond, code, msg)                                  \
     do {                                                             \
         if (!(cond)) throw ::dmfted::StatusError{(code), (msg)};     \
@@ -95,7 +111,12 @@ struct DBuf {
         n = count;
     }
     void release() {
-        if (p) cudaFree(p);
+        // The context works on a non-blocking stream, so nothing orders a free
+        // after that stream's queued work: wait for the device first.
+        if (p) {
+            cudaDeviceSynchronize();
+            cudaFree(p);
+        }
         p = nullptr;
         n = 0;
     }

@@ -224,6 +224,7 @@ __global__ void k_ritz_check(LanczosScalars lz, double tol) {
     extern __shared__ double rs[];
     const int n = lz.status[ST_STEPS];
     if (n <= 0) return;
+    if (!DM_IN(n, kLzMax)) return;
     double *sa = rs, *sb = rs + n, *yv = rs + 2 * n, *ws = rs + 3 * n;
     unsigned char *sw = reinterpret_cast<unsigned char *>(rs + 8 * n);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -274,7 +275,8 @@ __global__ void k_basis_combine(const T *basis, int64_t ld, int n, const double 
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < dim;
          i += (int64_t)gridDim.x * blockDim.x) {
         double acc = v0 ? sc[0] * v0[i] : sc[0] * (double)basis[i];
-        for (int k = 1; k < n; k++) acc += sc[k] * (double)basis[k * ld + i];
+        for (int k = 1; k < n; k++)
+            if (DM_IN(k, kLzMax)) acc += sc[k] * (double)basis[k * ld + i];
         psi[i] = acc;
     }
 }
