@@ -40,7 +40,12 @@ __device__ __forceinline__ void vst(E *p, const E (&v)[VW]) {
     }
 }
 
-constexpr int kDwBatch = 8;  // neighbour-column loads issued before their FMAs
+// Occupancy: 3 CTAs of 256 threads per SM (register cap 85) measured best on
+// B200 for the Ns=14 sectors; the down-hop load batch is 8 columns for FP32
+// and 4 for FP64 (register pressure).
+constexpr int kHxvMinBlocks = 3;
+template <typename T>
+constexpr int dw_batch() { return sizeof(T) == 8 ? 4 : 8; }
 constexpr int kUpBatch = 8;  // hopping-table entries prefetched per row vector
 
 // Factored H*v.  A CTA owns a tile of NC consecutive columns, staged in
@@ -49,7 +54,8 @@ constexpr int kUpBatch = 8;  // hopping-table entries prefetched per row vector
 // consecutive rows per pass (16-byte global loads and stores).  The down hops
 // stream whole neighbour columns from L2/HBM with kDwBatch loads in flight.
 template <typename T, int NC, int VW, bool LZ>
-__global__ void __launch_bounds__(256) k_hxv(const HxvArgs<T> a) {
+__global__ void __launch_bounds__(256, kHxvMinBlocks) k_hxv(const HxvArgs<T> a) {
+    constexpr int kDwBatch = dw_batch<T>();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ T spu[kMaxParams];
     __shared__ T sdint[64];

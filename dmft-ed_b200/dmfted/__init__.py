@@ -18,7 +18,7 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = os.path.join(os.path.dirname(_HERE), "libdmfted.so")
+_LIB = os.environ.get("DMFTED_LIB") or os.path.join(os.path.dirname(_HERE), "libdmfted.so")
 _lib = None
 
 OK = 0
