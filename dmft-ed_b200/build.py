@@ -11,7 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libdmfted.so")
-SOURCES = ["api.cu", "fock.cu", "hxv.cu", "lanczos.cu", "gf.cu", "observables.cu", "chi2.cu"]
+SOURCES = ["api.cu", "fock.cu", "hxv.cu", "lanczos.cu", "gf.cu", "observables.cu", "chi2.cu",
+           "noalloc.cu"]
 HEADERS = ["internal.cuh", "reduce.cuh", "hxv.cuh"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -357,3 +357,31 @@ template void hxv_lanczos_step<float>(dmfted_ctx *, const SectorView &, const fl
                                       const float *, float *, const LanczosScalars &, int, int);
 
 }  // namespace dmfted
+
+namespace dmfted {
+
+// Fused Lanczos step whose reduction scratch is supplied by the caller (the
+// context's own scratch is not touched).
+template <typename T>
+void hxv_lanczos_step_scratch(dmfted_ctx *c, const SectorView &s, const T *x, const T *xprev, T *y,
+                              const LanczosScalars &lz, int k, double *partials,
+                              unsigned *counter) {
+    HxvArgs<T> a = make_hxv_args<T>(c, s);
+    a.x = x;
+    a.y = y;
+    a.xprev = xprev;
+    a.alpha = lz.alpha;
+    a.beta = lz.beta;
+    a.scale = lz.scale;
+    a.status = lz.status;
+    a.k = k;
+    a.partials = partials;
+    a.counter = counter;
+    HxvCfg g = hxv_config<T>(c, s, a, 1);
+    launch_hxv<T, true>(c, a, g, 1);
+}
+template void hxv_lanczos_step_scratch<double>(dmfted_ctx *, const SectorView &, const double *,
+                                               const double *, double *, const LanczosScalars &,
+                                               int, double *, unsigned *);
+
+}  // namespace dmfted

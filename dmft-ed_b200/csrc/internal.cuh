@@ -259,6 +259,14 @@ LanczosResult lanczos_gs(dmfted_ctx *c, const SectorView &s, double *psi, const 
 // nstack = 2 runs a complex vector as its stacked re/im halves (length 2*dim).
 void lanczos_chain(dmfted_ctx *c, const SectorView &s, const double *v0, int precision,
                    const LanczosScalars &lz, int nstack = 1);
+// The same recurrence (FP64) on caller-owned vectors and caller-supplied
+// reduction scratch; allocates nothing.
+template <typename T>
+void hxv_lanczos_step_scratch(dmfted_ctx *c, const SectorView &s, const T *x, const T *xprev, T *y,
+                              const LanczosScalars &lz, int k, double *partials,
+                              unsigned *counter);
+void lanczos_chain_fixed(dmfted_ctx *c, const SectorView &s, const double *v0, double *work,
+                         const LanczosScalars &lz, double *partials, unsigned *counter);
 
 // ---- gf.cu ---------------------------------------------------------------
 // vv = c^+_{iorb,ispin} psi (particle) or c psi (hole) in sector sj;

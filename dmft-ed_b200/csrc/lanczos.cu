@@ -558,3 +558,36 @@ void lanczos_chain(dmfted_ctx *c, const SectorView &s, const double *v0, int pre
 }
 
 }  // namespace dmfted
+
+namespace dmfted {
+
+// Tridiagonalisation (FP64) on caller-owned vectors, with the reduction
+// scratch and the Lanczos scalars supplied by the caller: nothing here
+// allocates.  work holds the two rotating vectors (2*dim doubles).
+void lanczos_chain_fixed(dmfted_ctx *c, const SectorView &s, const double *v0, double *work,
+                         const LanczosScalars &lz, double *partials, unsigned *counter) {
+    const int64_t dim = s.dim;
+    double *P = work, *Q = work + dim;
+    const int eg = ew_grid(c, dim);
+    const int rg = red_grid(c, dim);
+    DM_CUDA(cudaMemsetAsync(P, 0, dim * sizeof(double), c->stream));
+    k_convert<double, double><<<eg, 256, 0, c->stream>>>(v0, Q, dim);
+    k_lz_init<double><<<rg, kRedThreads, 0, c->stream>>>(Q, dim, lz, partials, counter);
+    DM_CHECK_LAUNCH();
+    c->launches += 2;
+    for (int k = 0; k < lz.kmax; k++) {
+        hxv_lanczos_step_scratch<double>(c, s, Q, P, P, lz, k, partials, counter);
+        const bool vec = (dim % 2 == 0) && ((uintptr_t)P % 16 == 0) && ((uintptr_t)Q % 16 == 0);
+        if (vec)
+            k_lz_update<double, 2><<<red_grid(c, dim / 2), kRedThreads, 0, c->stream>>>(
+                P, Q, dim, lz, k, c->p.lanc_gf_threshold, partials, counter);
+        else
+            k_lz_update<double, 1><<<rg, kRedThreads, 0, c->stream>>>(
+                P, Q, dim, lz, k, c->p.lanc_gf_threshold, partials, counter);
+        DM_CHECK_LAUNCH();
+        c->launches++;
+        std::swap(P, Q);
+    }
+}
+
+}  // namespace dmfted

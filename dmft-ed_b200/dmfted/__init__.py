@@ -79,6 +79,7 @@ EXPORTS = {
     "dmfted_hxv_device_f32": (C.c_int, [_vp, _vp, _vp, C.c_int32]),
     "dmfted_lanczos_gs": (C.c_int, [_vp, C.c_int32, _dp, _dp, _ip]),
     "dmfted_lanc_tridiag": (C.c_int, [_vp, C.c_int32, _dp, C.c_int32, _dp, _dp, _ip]),
+    "dmfted_lanc_tridiag_noalloc": (C.c_int, [_vp, C.c_int32, _vp, C.c_int32, _vp, _vp, _vp, _vp]),
     "dmfted_ed_solve": (C.c_int, [_vp, _dp, C.c_int32, _ip, C.c_int32]),
     "dmfted_get_gimp_matsubara": (C.c_int, [_vp, _dp]),
     "dmfted_get_gimp_real": (C.c_int, [_vp, _dp]),

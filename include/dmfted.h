@@ -160,6 +160,25 @@ int dmfted_lanczos_gs(dmfted_ctx *ctx, int32_t isector, double *e0, double *psi,
 int dmfted_lanc_tridiag(dmfted_ctx *ctx, int32_t isector, const double *vvinit, int32_t nlanc,
                         double *alanc, double *blanc, int32_t *nused);
 
+/* No counterpart in the reference.  The tridiagonalisation of
+ * dmfted_lanc_tridiag (FP64) for callers that cannot allocate device memory at
+ * the time of the call -- a host whose device memory belongs to its own pool
+ * manager, or a latency-critical loop where cudaMalloc must not run.  The
+ * caller owns every buffer the call touches: d_v0 (real start vector of
+ * length getdim(isector), any norm), d_work (2*getdim(isector) doubles for the
+ * two rotating Lanczos vectors), d_alanc[nlanc], d_blanc[nlanc] (same
+ * convention as dmfted_lanc_tridiag) and d_nused, all device pointers.  The
+ * reduction scratch is a fixed array inside the library (about 90 KB per GPU,
+ * held until the process exits); the call allocates and frees nothing.
+ * Limit: 1 <= nlanc <= 1022, else DMFTED_ERR_ARG.  Calls on one device share
+ * the array and must not overlap on the GPU.  The first call on a device
+ * looks up the array's device address; make it before any stream capture.
+ * Returns after the results are written (the context's stream is
+ * synchronised). */
+int dmfted_lanc_tridiag_noalloc(dmfted_ctx *ctx, int32_t isector, const double *d_v0,
+                                int32_t nlanc, double *d_work, double *d_alanc, double *d_blanc,
+                                int32_t *d_nused);
+
 /* ---- the solve ------------------------------------------------------------
  * ed_solve_single (ED_MAIN.f90:251-289) for the normal mode:
  * set_dmft_bath, diagonalize_impurity (ED_DIAG.f90:78-398), the observables
