@@ -184,6 +184,74 @@ static void real_to_host_c128(dmfted_ctx *c, const double *d, int64_t n, double 
     DM_CUDA(cudaStreamSynchronize(c->stream));
 }
 
+// es_add_state with a size limit (ED_EIGENSPACE.f90:126-151): below the
+// limit insert; at the limit insert only below the highest energy, which is
+// popped first (es_pop_state, :219-299).
+static void states_add_capped(dmfted_ctx *c, double e, int isector, const double *psi, int64_t dim,
+                              int size) {
+    if ((int)c->states.size() < size) {
+        states_add(c, e, isector, psi, dim);
+    } else if (!c->states.empty() && e < c->states.back().e) {
+        c->states.pop_back();
+        states_add(c, e, isector, psi, dim);
+    }
+}
+
+// ed_diag_c, finite-temperature branch (ED_DIAG.f90:93-228): for every sector
+// the lowest Neigen = min(dim, neigen_sector) eigenpairs go into the list of
+// at most lanc_nstates_total states.
+static int64_t ed_diag_finite_t(dmfted_ctx *c, const std::vector<int> &list) {
+    const dmfted_params &p = c->p;
+    states_reset(c);
+    int64_t hv = 0;
+    std::vector<double> ev(kLzMax + 8);
+    for (int isector : list) {
+        SectorView s = sector_view(c, isector);
+        const int neigen = (int)std::min<int64_t>(s.dim, c->neigen_sector[isector - 1]);
+        if (neigen <= 0) continue;
+        const int nit = (int)std::min<int64_t>(s.dim, p.lanc_niter);
+        c->eigvecs.alloc((size_t)neigen * s.dim);
+        int steps = 0;
+        const int m = lanczos_eigs(c, s, neigen, p.precision, p.lanc_tolerance, nit, ev.data(),
+                                   c->eigvecs.p, &steps);
+        hv += steps;
+        for (int i = 0; i < m; i++)
+            states_add_capped(c, ev[i], isector, c->eigvecs.p + (size_t)i * s.dim, s.dim,
+                              c->nstates_total);
+    }
+    return hv;
+}
+
+// ed_analysis, finite-temperature part (ED_DIAG.f90:248-398): Z from the full
+// list, then the per-sector Neigen adaptation and the cutoff trimming /
+// lanc_nstates_total growth that the next solve uses.
+static void ed_analysis_finite_t(dmfted_ctx *c) {
+    const dmfted_params &p = c->p;
+    c->egs = c->states.front().e;
+    double z = 0.0;
+    for (auto &st : c->states) z += std::exp(-p.beta * (st.e - c->egs));
+    c->zeta = z;
+    std::vector<int> count(c->nsectors, 0);
+    for (auto &st : c->states) count[st.isector - 1]++;
+    for (int i = 0; i < c->nsectors; i++) {
+        int &ne = c->neigen_sector[i];
+        if (count[i] > 0) ne++;
+        else ne--;
+        if (ne > count[i]) ne = count[i] + 1;
+        if (ne <= 0) ne = 1;
+    }
+    const double ec = c->states.back().e;
+    if (std::exp(-p.beta * (ec - c->egs)) > p.cutoff) {
+        c->nstates_total += p.lanc_nstates_step;
+    } else {
+        while (c->states.size() > 1 &&
+               std::exp(-p.beta * (c->states.back().e - c->egs)) <= p.cutoff)
+            c->states.pop_back();
+        c->nstates_total =
+            std::max<int>((int)c->states.size(), p.lanc_nstates_step) + p.lanc_nstates_step;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // The solve.  Mirrors ed_solve_single (ED_MAIN.f90:251-289):
 //   diagonalize_impurity -> ed_diag_c (sector loop and state selection,
@@ -195,8 +263,6 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "ed_solve: bath not set");
     const dmfted_params &p = c->p;
     c->finite_t = p.lanc_nstates_total != 1;  // ED_SETUP.f90:242-246
-    DM_REQUIRE(!c->finite_t, DMFTED_ERR_UNSUPPORTED,
-               "finite temperature (lanc_nstates_total > 1) is not available in this build");
     DM_REQUIRE(!p.ed_twin, DMFTED_ERR_UNSUPPORTED, "ed_twin is not available in this build");
     std::vector<int> list;
     if (sectors && nsect_list > 0) {
@@ -217,7 +283,8 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     double oldzero = 1000.0;
     const double gsth = p.gs_threshold;
     int64_t hv_diag = 0;
-    for (int isector : list) {
+    if (c->finite_t) hv_diag = ed_diag_finite_t(c, list);
+    for (int isector : (c->finite_t ? std::vector<int>() : list)) {
         SectorView s = sector_view(c, isector);
         c->s64a.alloc(s.dim);
         const int nit = (int)std::min<int64_t>(s.dim, p.lanc_niter);
@@ -235,9 +302,13 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
         }
     }
     DM_REQUIRE(!c->states.empty(), DMFTED_ERR_NOTCONV, "ed_solve: no state kept");
-    c->egs = c->states.front().e;
-    for (auto &st : c->states) c->egs = std::min(c->egs, st.e);
-    c->zeta = (double)c->states.size();  // T=0: Z = number of ground states
+    if (c->finite_t) {
+        ed_analysis_finite_t(c);
+    } else {
+        c->egs = c->states.front().e;
+        for (auto &st : c->states) c->egs = std::min(c->egs, st.e);
+        c->zeta = (double)c->states.size();  // T=0: Z = number of ground states
+    }
     DM_CUDA(cudaEventRecord(ev[1], c->stream));
     // ---- observables -------------------------------------------------------
     const int na = obs_count(c);
@@ -245,7 +316,9 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     std::vector<double> acc(na, 0.0), one(na);
     for (auto &st : c->states) {
         SectorView s = sector_view(c, st.isector);
-        const double peso = 1.0 / c->zeta;
+        // ED_OBSERVABLES.f90:128-129
+        const double peso =
+            (c->finite_t ? std::exp(-p.beta * (st.e - c->egs)) : 1.0) / c->zeta;
         observables_raw(c, s, c->states64.p + st.off, c->obs_d.p);
         DM_CUDA(cudaMemcpyAsync(one.data(), c->obs_d.p, na * sizeof(double), cudaMemcpyDeviceToHost,
                                 c->stream));
@@ -286,6 +359,7 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
             weight = 1.0 / c->zeta;
         else
             weight = 0.0;
+        if (weight == 0.0) continue;  // pesoBZ = 0: the chains add nothing
         for (int ispin = 0; ispin < c->nspin; ispin++)
             for (int iorb = 0; iorb < no; iorb++) {
                 double *gmo = c->gm.p + 2 * (size_t)(ispin * no + iorb) * p.lmats;
@@ -451,6 +525,13 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
             check_hloc(c, hloc);
             std::copy(hloc, hloc + nh, c->hloc.begin());
         }
+        // ED_SETUP.f90:242-260: T=0 iff lanc_nstates_total==1; at finite T
+        // both state counts are made even (doublets are kept together)
+        if (c->p.lanc_nstates_total != 1) {
+            if (c->p.lanc_nstates_sector % 2 != 0) c->p.lanc_nstates_sector++;
+            if (c->p.lanc_nstates_total % 2 != 0) c->p.lanc_nstates_total++;
+        }
+        c->nstates_total = c->p.lanc_nstates_total;
         setup_pointers_normal(c);
         fock_init(c);
         c->red_partials.alloc((size_t)2 * 64 * kMaxRedBlocks);

@@ -206,6 +206,8 @@ struct dmfted_ctx {
     dmfted::DBuf<double> d_wm, d_wr;      // Matsubara / real-axis grids
     dmfted::DBuf<double> d_bath_e, d_bath_v, d_hloc_aa;  // [nspin][norb][nbath], [nspin][norb]
     dmfted::DBuf<double> obs_d;           // observable accumulators of one state
+    dmfted::DBuf<double> eig_aux;         // Ritz values, vectors of T, coefficients, dots
+    dmfted::DBuf<double> eigvecs;         // eigenvectors of one sector (Neigen x dim)
     int64_t launches = 0;
     // results of the last solve (device and host)
     struct State {
@@ -217,6 +219,7 @@ struct dmfted_ctx {
     dmfted::DBuf<double> states64;
     double zeta = 1.0, egs = 0.0;
     bool finite_t = false;
+    int nstates_total = 1;  // lanc_nstates_total, adapted by ed_analysis between solves
     dmfted::DBuf<double> gm, gr, g0m, sm, sr;  // complex (nspin,norb,L) blocks
     std::vector<double> obs;                   // dens, up, dw, docc, magz (norb each)
     std::vector<double> hf_terms;              // nk[2][norb][nbath], hop[2][norb][nbath]
@@ -267,6 +270,12 @@ void hxv_lanczos_step_scratch(dmfted_ctx *c, const SectorView &s, const T *x, co
                               unsigned *counter);
 void lanczos_chain_fixed(dmfted_ctx *c, const SectorView &s, const double *v0, double *work,
                          const LanczosScalars &lz, double *partials, unsigned *counter);
+
+// Lowest neigen eigenpairs of sector s (full reorthogonalisation).  vecs:
+// device, neigen*dim FP64 (row j = eigenvector j, normalised); evals_h host.
+// Returns the number of pairs found (min(neigen, dim, steps)).
+int lanczos_eigs(dmfted_ctx *c, const SectorView &s, int neigen, int precision, double tol,
+                 int nitermax, double *evals_h, double *vecs, int *steps);
 
 // ---- gf.cu ---------------------------------------------------------------
 // vv = c^+_{iorb,ispin} psi (particle) or c psi (hole) in sector sj;

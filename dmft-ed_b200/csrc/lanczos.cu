@@ -591,3 +591,225 @@ void lanczos_chain_fixed(dmfted_ctx *c, const SectorView &s, const double *v0, d
 }
 
 }  // namespace dmfted
+
+// ===========================================================================
+// Lowest Neigen eigenpairs of a sector (the finite-temperature call of sp_eigh,
+// ED_DIAG.f90:169-183, and the dense small-sector branch :184-194): Lanczos
+// with full reorthogonalisation against the stored basis (classical
+// Gram-Schmidt, twice), as ARPACK keeps its Krylov basis orthogonal.  Every
+// ncheck steps one CTA finds the lowest Neigen Ritz values of T_n by Sturm
+// multisection and their Ritz estimates by inverse iteration; all must pass
+// ARPACK's test.  A single start vector sees one copy of each degenerate
+// eigenvalue.
+namespace dmfted {
+
+// d_i = <s_i, w> for the nv stored vectors; one CTA per basis vector.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_reorth_dots(const T *basis, int64_t ld, int nv,
+                                                             const T *w, int64_t n, double *dots) {
+    __shared__ double sm[64];
+    const int i = blockIdx.x;
+    if (i >= nv) return;
+    CSum s;
+    s.zero();
+    const T *b = basis + (int64_t)i * ld;
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) s.add((double)b[j] * (double)w[j]);
+    CSum arr[1] = {s};
+    block_reduce<1>(arr, sm);
+    if (threadIdx.x == 0) dots[i] = arr[0].value();
+}
+
+// w -= sum_i <v_i, w> v_i with v_i = sc_i s_i, i.e. coefficient d_i sc_i^2.
+template <typename T>
+__global__ void k_reorth_update(const T *basis, int64_t ld, int nv, const double *dots,
+                                const double *scale, T *w, int64_t n) {
+    __shared__ double cf[kLzMax + 8];
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) cf[i] = dots[i] * scale[i] * scale[i];
+    __syncthreads();
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        double acc = (double)w[j];
+        for (int i = 0; i < nv; i++) acc -= cf[i] * (double)basis[(int64_t)i * ld + j];
+        w[j] = (T)acc;
+    }
+}
+
+// b_{k+1} = |w| after reorthogonalisation; scale, step count, done flags.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_lz_renorm(const T *w, int64_t n, LanczosScalars lz,
+                                                           int k, double thr, double *partials,
+                                                           unsigned *counter) {
+    if (lz.status[ST_DONE] && lz.status[ST_STEPS] != k + 1) return;
+    CSum s;
+    s.zero();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = (double)w[i];
+        s.add(v * v);
+    }
+    CSum arr[1] = {s};
+    double tot[1];
+    if (grid_reduce<1>(arr, partials, counter, tot)) {
+        if (threadIdx.x == 0) {
+            const double b = sqrt(tot[0]);
+            lz.beta[k + 1] = b;
+            lz.scale[k + 1] = b > 0.0 ? 1.0 / b : 0.0;
+            lz.status[ST_STEPS] = k + 1;
+            lz.status[ST_DONE] = 0;
+            if (b < thr) {
+                lz.status[ST_DONE] = 1;
+                lz.status[ST_BREAK] = 1;
+            }
+            if (k + 1 >= lz.kmax) lz.status[ST_DONE] = 1;
+        }
+    }
+}
+
+// Lowest m Ritz pairs of T_n.  evals[j] (j < m), Y[j*n + i] = eigenvector j
+// (inverse iteration, re-orthogonalised against the lower ones in the small
+// space), est[j] = b_n |Y[j*n + n-1]|.  Converged when every estimate passes
+// ARPACK's test or the recurrence broke down.  Dynamic shared memory:
+// ritz_smem(n).  Y lives in global memory (m*n doubles).
+__global__ void k_ritz_multi(LanczosScalars lz, double tol, int mwant, double *evals, double *Y,
+                             double *est, int final_pass) {
+    extern __shared__ double rs[];
+    const int n = lz.status[ST_STEPS];
+    if (n <= 0) return;
+    double *sa = rs, *sb = rs + n, *yv = rs + 2 * n, *ws = rs + 3 * n;
+    unsigned char *sw = reinterpret_cast<unsigned char *>(rs + 8 * n);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        sa[i] = lz.alpha[i];
+        sb[i] = i > 0 ? lz.beta[i] : 0.0;
+    }
+    __syncthreads();
+    const int m = min(mwant, n);
+    bool ok = true;
+    for (int j = 0; j < m; j++) {
+        const double e = tridiag_eig(sa, sb, n, j);
+        if (threadIdx.x == 0) {
+            tridiag_evec(sa, sb, n, e, yv, ws, sw);
+            // orthogonalise against the lower eigenvectors (close eigenvalues)
+            for (int q = 0; q < j; q++) {
+                double d = 0.0;
+                for (int i = 0; i < n; i++) d += Y[(int64_t)q * n + i] * yv[i];
+                for (int i = 0; i < n; i++) yv[i] -= d * Y[(int64_t)q * n + i];
+            }
+            double nr = 0.0;
+            for (int i = 0; i < n; i++) nr += yv[i] * yv[i];
+            nr = 1.0 / sqrt(nr);
+            const double sg = yv[0] < 0.0 ? -nr : nr;
+            for (int i = 0; i < n; i++) Y[(int64_t)j * n + i] = yv[i] * sg;
+            evals[j] = e;
+            est[j] = fabs(lz.beta[n]) * fabs(Y[(int64_t)j * n + n - 1]);
+            const double eps23 = 3.666852862501036e-11;
+            if (!(est[j] <= tol * fmax(eps23, fabs(e)))) ok = false;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && !final_pass) {
+        if (lz.status[ST_BREAK] || (ok && n >= m && m == mwant) || (ok && n == lz.kmax)) {
+            lz.status[ST_CONV] = 1;
+            lz.status[ST_DONE] = 1;
+        }
+    }
+}
+
+// coef[j*n + i] = Y[j*n + i] * scale_i
+__global__ void k_ritz_coefs(const double *Y, const double *scale, int m, int n, double *coef) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < m * n; t += gridDim.x * blockDim.x)
+        coef[t] = Y[t] * scale[t % n];
+}
+
+template <typename T>
+static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, int nitermax,
+                    int ncheck, double *evals_h, double *vecs) {
+    const int64_t dim = s.dim;
+    const int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
+    const size_t ld = (size_t)((dim + 31) / 32 * 32);
+    c->work.alloc(ld * sizeof(T) * (size_t)(kmax + 1));
+    T *basis = reinterpret_cast<T *>(c->work.p);
+    LanczosScalars lz = lz_slot(c, 0, kmax);
+    ritz_attr(c);
+    static bool attr[64] = {false};
+    if (!attr[c->device & 63]) {
+        DM_CUDA(cudaFuncSetAttribute(k_ritz_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)ritz_smem(kLzMax)));
+        attr[c->device & 63] = true;
+    }
+    const int m = std::min<int64_t>(neigen, dim);
+    c->eig_aux.alloc((size_t)64 * 2 + (size_t)m * (kLzMax + 2) * 2 + kLzMax + 8);
+    double *d_evals = c->eig_aux.p, *d_est = d_evals + 64, *d_Y = d_est + 64;
+    double *d_coef = d_Y + (size_t)m * (kLzMax + 2), *d_dots = d_coef + (size_t)m * (kLzMax + 2);
+    const int eg = ew_grid(c, dim);
+    const int rg = red_grid(c, dim);
+    c->s64b.alloc(dim);
+    k_random_start<<<eg, 256, 0, c->stream>>>(c->s64b.p, dim, 1234567ull);
+    k_convert<T, double><<<eg, 256, 0, c->stream>>>(c->s64b.p, basis, dim);
+    k_lz_init<T><<<rg, kRedThreads, 0, c->stream>>>(basis, dim, lz, c->red_partials.p,
+                                                     c->red_counter.p);
+    DM_CHECK_LAUNCH();
+    c->launches += 3;
+    int hst[8] = {0};
+    int launched = 0;
+    while (launched < kmax) {
+        for (int j = 0; j < ncheck && launched < kmax; j++, launched++) {
+            const int k = launched;
+            T *x = basis + (size_t)k * ld;
+            const T *xp = basis + (size_t)(k > 0 ? k - 1 : k) * ld;
+            T *y = basis + (size_t)(k + 1) * ld;
+            hxv_lanczos_step<T>(c, s, x, xp, y, lz, k);
+            launch_lz_update<T>(c, y, x, dim, lz, k, 1e-300);
+            for (int pass = 0; pass < 2; pass++) {
+                k_reorth_dots<T><<<k + 1, kRedThreads, 0, c->stream>>>(basis, (int64_t)ld, k + 1, y,
+                                                                       dim, d_dots);
+                k_reorth_update<T><<<eg, 256, 0, c->stream>>>(basis, (int64_t)ld, k + 1, d_dots,
+                                                             lz.scale, y, dim);
+            }
+            k_lz_renorm<T><<<rg, kRedThreads, 0, c->stream>>>(y, dim, lz, k, 1e-300,
+                                                              c->red_partials.p, c->red_counter.p);
+            DM_CHECK_LAUNCH();
+            c->launches += 5;
+        }
+        k_ritz_multi<<<1, kRedThreads, ritz_smem(launched), c->stream>>>(lz, tol, m, d_evals, d_Y,
+                                                                         d_est, 0);
+        DM_CHECK_LAUNCH();
+        c->launches++;
+        DM_CUDA(cudaMemcpyAsync(hst, lz.status, sizeof(hst), cudaMemcpyDeviceToHost, c->stream));
+        DM_CUDA(cudaStreamSynchronize(c->stream));
+        if (hst[ST_DONE]) break;
+    }
+    const int n = hst[ST_STEPS];
+    const int mm = std::min(m, n);
+    k_ritz_multi<<<1, kRedThreads, ritz_smem(n), c->stream>>>(lz, tol, mm, d_evals, d_Y, d_est, 1);
+    k_ritz_coefs<<<div_up((int64_t)mm * n, 256), 256, 0, c->stream>>>(d_Y, lz.scale, mm, n, d_coef);
+    for (int j = 0; j < mm; j++) {
+        double *v = vecs + (size_t)j * dim;
+        k_basis_combine<T><<<eg, 256, 0, c->stream>>>(basis, (int64_t)ld, n, d_coef + (size_t)j * n,
+                                                       nullptr, v, dim);
+        norm2_device(c, v, dim, c->red_out.p + 3);
+        k_scale_by_invsqrt<<<eg, 256, 0, c->stream>>>(v, dim, c->red_out.p + 3);
+    }
+    DM_CHECK_LAUNCH();
+    c->launches += 2 + 3 * mm;
+    DM_CUDA(cudaMemcpyAsync(evals_h, d_evals, mm * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    return mm;
+}
+
+int lanczos_eigs(dmfted_ctx *c, const SectorView &s, int neigen, int precision, double tol,
+                 int nitermax, double *evals_h, double *vecs, int *steps) {
+    const int ncheck = std::max(1, c->p.lanc_ncheck);
+    int m;
+    if (precision == DMFTED_FP64)
+        m = eigs_run<double>(c, s, neigen, tol, nitermax, ncheck, evals_h, vecs);
+    else
+        m = eigs_run<float>(c, s, neigen, std::max(tol, c->mixed_tol32), nitermax, ncheck, evals_h,
+                            vecs);
+    int st[8];
+    DM_CUDA(cudaMemcpy(st, lz_slot(c, 0, 1).status, sizeof(st), cudaMemcpyDeviceToHost));
+    if (steps) *steps = st[ST_STEPS];
+    return m;
+}
+
+}  // namespace dmfted

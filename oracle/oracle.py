@@ -443,3 +443,102 @@ def solve_sector_t0(model, nup, ndw, lmats=4096, lreal=0, wini=-5.0, wfin=5.0, e
                                            gm[ispin, iorb])
     return dict(e0=e0, psi=psi, nlanc=nl, obs=obs, gmats=gm, greal=gr, smats=sm, chains=chains,
                 map=hmap, wm=wm)
+
+
+# ------------------------------------------------ finite-T pipeline ---
+def _sector_eigs(model, hmap, k):
+    """Lowest k eigenpairs of the sector H: dense eigh (the reference's small-
+    sector branch, ED_DIAG.f90:184-194) or ARPACK eigsh ('SA')."""
+    H = sparse_h(model, hmap)
+    if hmap.size <= 2500:
+        w, V = np.linalg.eigh(H.toarray())
+        return w[:k], V[:, :k]
+    import scipy.sparse.linalg as sla
+    w, V = sla.eigsh(H, k=k, which="SA", tol=1e-14)
+    o = np.argsort(w)
+    return w[o], V[:, o]
+
+
+def solve_finite_t(model, lmats=256, lreal=0, wini=-5.0, wfin=5.0, eps=0.01, ngfiter=200,
+                   nstates_sector=6, nstates_total=16, nstates_step=2, cutoff=1e-9, nthreads=1):
+    """Finite-temperature solve over every sector: ed_diag_c (ED_DIAG.f90:93-228,
+    finite-T branch with es_add_state's size cap, ED_EIGENSPACE.f90:126-151),
+    ed_analysis (ED_DIAG.f90:248-398: Z before trimming, Neigen adaptation,
+    cutoff trimming), observables with Boltzmann weights and the GF chains of
+    every kept state (build_gf_normal.f90:71-180,442-488)."""
+    ns = model.ns
+    if nstates_total != 1:
+        nstates_sector += nstates_sector % 2
+        nstates_total += nstates_total % 2
+    secs = [(a, b) for a in range(ns + 1) for b in range(ns + 1)]
+    from math import comb
+    neigen = [min(comb(ns, a) * comb(ns, b), nstates_sector) for a, b in secs]
+    states = []  # [e, isector(1-based), psi]
+
+    def insert(e, isec, v):
+        i = 0
+        while i < len(states) and not (e <= states[i][0]):
+            i += 1
+        states.insert(i, [e, isec, v])
+
+    for isec0, (a, b) in enumerate(secs):
+        hm = build_sector(ns, a, b)
+        k = min(hm.size, neigen[isec0])
+        w, V = _sector_eigs(model, hm, k)
+        for i in range(k):
+            e = float(w[i])
+            if len(states) < nstates_total:
+                insert(e, isec0 + 1, V[:, i])
+            elif e < states[-1][0]:
+                states.pop()
+                insert(e, isec0 + 1, V[:, i])
+    egs = states[0][0]
+    zeta = sum(np.exp(-model.beta * (s[0] - egs)) for s in states)
+    count = np.zeros(len(secs), int)
+    for s in states:
+        count[s[1] - 1] += 1
+    new_neigen = []
+    for i in range(len(secs)):
+        ne = neigen[i] + (1 if count[i] > 0 else -1)
+        if ne > count[i]:
+            ne = count[i] + 1
+        new_neigen.append(max(ne, 1))
+    if np.exp(-model.beta * (states[-1][0] - egs)) > cutoff:
+        new_total = nstates_total + nstates_step
+    else:
+        while len(states) > 1 and np.exp(-model.beta * (states[-1][0] - egs)) <= cutoff:
+            states.pop()
+        new_total = max(len(states), nstates_step) + nstates_step
+    no = model.norb
+    obs = {k: np.zeros(no) for k in ["dens", "dens_up", "dens_dw", "docc", "magz"]}
+    wm = matsubara(model.beta, lmats)
+    wr = realaxis(wini, wfin, lreal)
+    gm = np.zeros((model.nspin, no, lmats), np.complex128)
+    gr = np.zeros((model.nspin, no, lreal), np.complex128)
+    for e, isec, psi in states:
+        a, b = secs[isec - 1]
+        hm = build_sector(ns, a, b)
+        peso = np.exp(-model.beta * (e - egs)) / zeta
+        o = observables_state(model, hm, psi.astype(np.complex128), peso)
+        for k in obs:
+            obs[k] += o[k]
+        for ispin in range(model.nspin):
+            for iorb in range(no):
+                isite = (iorb + 1) + ispin * ns
+                for particle, dn in ((True, 1), (False, -1)):
+                    jn = (a + dn, b) if ispin == 0 else (a, b + dn)
+                    if not (0 <= jn[0] <= ns and 0 <= jn[1] <= ns):
+                        continue
+                    jmap = build_sector(ns, *jn)
+                    n2, vv = gf_vvinit(particle, isite, hm, jmap, psi.astype(np.complex128))
+                    vv = vv / np.sqrt(n2)
+                    nlanc = min(jmap.size, ngfiter)
+                    al, bl, _ = lanczos_tridiag(model, jmap, vv, nlanc, nthreads=nthreads)
+                    gmt = np.zeros(lmats, np.complex128)
+                    grt = np.zeros(lreal, np.complex128)
+                    add_to_lanczos_gf(n2, e, egs, zeta, True, model.beta, al, bl,
+                                      1 if particle else -1, wm, wr, eps, gmt, grt)
+                    gm[ispin, iorb] += gmt
+                    gr[ispin, iorb] += grt
+    return dict(states=[(s[0], s[1]) for s in states], egs=egs, zeta=zeta, obs=obs, gmats=gm,
+                greal=gr, neigen=new_neigen, nstates_total=new_total)
