@@ -901,20 +901,37 @@ int dmfted_chi2_delta_batch(dmfted_ctx *c, int32_t nbatch, int32_t nbath, int32_
     API_END
 }
 
-int dmfted_time_hxv(dmfted_ctx *c, int32_t fp32, int32_t warmup, int32_t reps, double *ms) {
+int dmfted_time_hxv(dmfted_ctx *c, int32_t flags, int32_t warmup, int32_t reps, double *ms) {
     API_BEGIN
     DM_REQUIRE(c && ms && reps >= 1 && warmup >= 0, DMFTED_ERR_ARG, "bad argument");
     DM_REQUIRE(c->cur_sector != 0, DMFTED_ERR_STATE, "time_hxv: Hsector NOT set");
     DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "time_hxv: bath not set");
     DM_CUDA(cudaSetDevice(c->device));
+    const bool fp32 = (flags & 1) != 0, fused = (flags & 2) != 0;
     SectorView s = sector_view(c, c->cur_sector);
     const size_t es = fp32 ? 4 : 8;
-    c->chainbuf.alloc(2 * (size_t)s.dim * es);
-    DM_CUDA(cudaMemsetAsync(c->chainbuf.p, 0, 2 * (size_t)s.dim * es, c->stream));
-    void *x = c->chainbuf.p, *y = c->chainbuf.p + (size_t)s.dim * es;
+    const size_t ld = (size_t)((s.dim + 31) / 32 * 32);
+    c->chainbuf.alloc(3 * ld * es);
+    DM_CUDA(cudaMemsetAsync(c->chainbuf.p, 0, 3 * ld * es, c->stream));
+    void *x = c->chainbuf.p, *y = c->chainbuf.p + ld * es, *xp = c->chainbuf.p + 2 * ld * es;
+    LanczosScalars lz = lz_slot(c, 3, kLzMax);
+    if (fused) {
+        // step k = 1 of a recurrence with unit scales and b_1 = 0.5
+        std::vector<double> init(kLzStride, 0.0);
+        for (int i = 0; i < kLzMax + 2; i++) init[2 * (kLzMax + 2) + i] = 1.0;  // scale
+        init[(kLzMax + 2) + 1] = 0.5;                                           // beta[1]
+        DM_CUDA(cudaMemcpyAsync(lz.alpha, init.data(), kLzStride * sizeof(double),
+                                cudaMemcpyHostToDevice, c->stream));
+        DM_CUDA(cudaMemsetAsync(lz.status, 0, 8 * sizeof(int), c->stream));
+    }
     auto run = [&]() {
-        if (fp32) hxv_f32(c, s, (const float *)x, (float *)y, 1);
-        else hxv_f64(c, s, (const double *)x, (double *)y, 1);
+        if (fused) {
+            if (fp32) hxv_lanczos_step<float>(c, s, (const float *)x, (const float *)xp, (float *)y, lz, 1);
+            else hxv_lanczos_step<double>(c, s, (const double *)x, (const double *)xp, (double *)y, lz, 1);
+        } else {
+            if (fp32) hxv_f32(c, s, (const float *)x, (float *)y, 1);
+            else hxv_f64(c, s, (const double *)x, (double *)y, 1);
+        }
     };
     for (int i = 0; i < warmup; i++) run();
     cudaEvent_t e0, e1;

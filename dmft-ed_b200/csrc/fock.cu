@@ -112,6 +112,52 @@ __global__ void k_ell_build(int ns, int norb, int nbath, int W, const uint32_t *
     diag_f[gs] = (float)d;
 }
 
+// Bank-quad balancing of the hopping table of one class.  In the H*v the up
+// hops are gathers of 16-byte rows of the staged tile; row t sits in shared-
+// memory bank quad t % 8, and one warp-wide gather serves the rows of one
+// group: 64 consecutive rows split by parity when a thread owns two rows
+// (vw == 2), 32 consecutive rows otherwise.  Which slot of a row's list holds
+// which hop is free, so each group reorders its rows' entries greedily, slot by
+// slot, putting on every row the hop whose target quad is least used so far in
+// that slot.  Balanced quads mean fewer shared-memory wavefronts per gather;
+// the set of hops of a row is unchanged.  One thread per group.
+__global__ void k_ell_balance(int ns, int n, int W, int vw, const uint8_t *cnt, uint32_t *ell) {
+    const int64_t rows = binom_d(ns, n);
+    const int64_t span = vw == 2 ? 64 : 32;
+    const int64_t ngroups = ((rows + span - 1) / span) * vw;
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= ngroups) return;
+    const int64_t blk = g / vw, par = g % vw;
+    const int64_t off = c_class_poff[n];
+    uint32_t *e = ell + (int64_t)W * off;
+    int load[kMaxW][8];
+    const int wmax = W < kMaxW ? W : kMaxW;
+    for (int q = 0; q < wmax; q++)
+        for (int b = 0; b < 8; b++) load[q][b] = 0;
+    for (int l = 0; l < 32; l++) {
+        const int64_t r = blk * span + (int64_t)l * vw + par;
+        if (r >= rows) break;
+        const int c = cnt[off + r];
+        // selection sort of this row's entries by current quad load, slot by slot
+        for (int q = 0; q < c; q++) {
+            int best = q, bl = 1 << 30;
+            for (int k = q; k < c; k++) {
+                const int quad = (int)(ell_col(e[(int64_t)k * rows + r]) & 7u);
+                if (load[q][quad] < bl) {
+                    bl = load[q][quad];
+                    best = k;
+                }
+            }
+            if (best != q) {
+                const uint32_t t = e[(int64_t)q * rows + r];
+                e[(int64_t)q * rows + r] = e[(int64_t)best * rows + r];
+                e[(int64_t)best * rows + r] = t;
+            }
+            load[q][ell_col(e[(int64_t)q * rows + r]) & 7u]++;
+        }
+    }
+}
+
 // Combined sector map (ED_SETUP.f90:880-890): map[i] = iup + idw*2^Ns with
 // i = rank_up + DimUp*rank_dw.
 __global__ void k_build_map(int ns, int64_t dimup, int64_t dim, const uint32_t *wu,
@@ -257,6 +303,15 @@ void fock_set_couplings(dmfted_ctx *c) {
             t.ell.p, t.diag.p, t.diag_f.p);
         DM_CHECK_LAUNCH();
         c->launches++;
+        // gather grouping of the H*v: two rows per thread for even class sizes
+        for (int n = 0; n <= c->ns; n++) {
+            const int vw = (c->binom[n] % 2 == 0) ? 2 : 1;
+            const int64_t ng = ((c->binom[n] + (vw == 2 ? 63 : 31)) / (vw == 2 ? 64 : 32)) * vw;
+            k_ell_balance<<<div_up(ng, 64), 64, 0, c->stream>>>(c->ns, n, std::max(c->W, 1), vw,
+                                                                t.cnt.p, t.ell.p);
+            DM_CHECK_LAUNCH();
+            c->launches++;
+        }
         DM_CUDA(cudaStreamSynchronize(c->stream));
         d_eb.release();
     }

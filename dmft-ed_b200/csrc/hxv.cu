@@ -48,6 +48,43 @@ template <typename T>
 constexpr int dw_batch() { return sizeof(T) == 8 ? 4 : 8; }
 constexpr int kUpBatch = 8;  // hopping-table entries prefetched per row vector
 
+// Loads of neighbour columns: cached in L2 only (no reuse inside the CTA, and
+// L1 is kept for the hopping tables).  Output stores: evict-first, so the
+// input vector stays resident in L2 for the neighbour reads of other CTAs.
+template <typename E, int VW>
+__device__ __forceinline__ void vld_cg(const E *p, E (&v)[VW]) {
+    if constexpr (sizeof(E) * VW == 16) {
+        const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(p));
+        memcpy(v, &q, 16);
+    } else if constexpr (sizeof(E) * VW == 8) {
+        const uint2 q = __ldcg(reinterpret_cast<const uint2 *>(p));
+        memcpy(v, &q, 8);
+    } else if constexpr (sizeof(E) * VW == 4) {
+        const unsigned q = __ldcg(reinterpret_cast<const unsigned *>(p));
+        memcpy(v, &q, 4);
+    } else {
+        v[0] = __ldcg(p);
+    }
+}
+template <typename E, int VW>
+__device__ __forceinline__ void vst_cs(E *p, const E (&v)[VW]) {
+    if constexpr (sizeof(E) * VW == 16) {
+        uint4 q;
+        memcpy(&q, v, 16);
+        __stcs(reinterpret_cast<uint4 *>(p), q);
+    } else if constexpr (sizeof(E) * VW == 8) {
+        uint2 q;
+        memcpy(&q, v, 8);
+        __stcs(reinterpret_cast<uint2 *>(p), q);
+    } else if constexpr (sizeof(E) * VW == 4) {
+        unsigned q;
+        memcpy(&q, v, 4);
+        __stcs(reinterpret_cast<unsigned *>(p), q);
+    } else {
+        __stcs(p, v[0]);
+    }
+}
+
 // Factored H*v.  A CTA owns a tile of NC consecutive columns, staged in
 // shared memory row-interleaved (xs[row*NC + j]) so that one up-hop gather is
 // a single NC-wide load serving all NC columns.  Each thread owns VW
@@ -187,7 +224,7 @@ __global__ void __launch_bounds__(256, kHxvMinBlocks) k_hxv(const HxvArgs<T> a) 
 #pragma unroll
                         for (int q = 0; q < kDwBatch; q++)
                             if (e0 + q < ce && DM_IN(soff[j][e0 + q] + r + VW - 1, ncols * dimup))
-                                vld<T, VW>(x + soff[j][e0 + q] + r, xv[q]);
+                                vld_cg<T, VW>(x + soff[j][e0 + q] + r, xv[q]);
 #pragma unroll
                         for (int q = 0; q < kDwBatch; q++)
                             if (e0 + q < ce) {
@@ -206,9 +243,9 @@ __global__ void __launch_bounds__(256, kHxvMinBlocks) k_hxv(const HxvArgs<T> a) 
                             ut[i] = (T)(sc * (double)acc[j][i] - cprev * (double)xp[i]);
                             dot.add((double)xs[(r + i) * NC + j] * (double)ut[i]);
                         }
-                        vst<T, VW>(y + idx, ut);
+                        vst_cs<T, VW>(y + idx, ut);
                     } else {
-                        vst<T, VW>(y + idx, acc[j]);
+                        vst_cs<T, VW>(y + idx, acc[j]);
                     }
                 }
             }

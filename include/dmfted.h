@@ -234,9 +234,11 @@ int dmfted_chi2_delta_batch_device(dmfted_ctx *ctx, int32_t nbatch, int32_t nbat
 
 /* ---- timing helpers (device time on the context's stream) ------------ */
 /* Average device milliseconds of one H*v on the current sector over reps
- * launches after warmup launches (fp32 != 0: float32 vectors).  The vectors
- * are the context's own work buffers. */
-int dmfted_time_hxv(dmfted_ctx *ctx, int32_t fp32, int32_t warmup, int32_t reps, double *ms);
+ * launches after warmup launches.  flags: bit 0 = float32 vectors (else
+ * float64), bit 1 = the fused Lanczos-step variant (H*v - b v_prev and the
+ * alpha dot product) instead of the plain product.  The vectors are the
+ * context's own work buffers. */
+int dmfted_time_hxv(dmfted_ctx *ctx, int32_t flags, int32_t warmup, int32_t reps, double *ms);
 
 /* Device milliseconds of the last dmfted_ed_solve, split into phases:
  * t[0]=diagonalisation, t[1]=observables, t[2]=Green's functions,
