@@ -369,7 +369,7 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
                     const int js = particle ? c->getcdgsector[2 * (st.isector - 1) + ispin]
                                             : c->getcsector[2 * (st.isector - 1) + ispin];
                     if (js == 0) continue;
-                    SectorView sj = sector_view(c, js);
+                    SectorView sj = chain_view(c, js);
                     c->s64b.alloc(sj.dim);
                     gf_apply_op(c, si, sj, iorb, ispin, particle, psi, c->s64b.p, c->red_out.p + 2);
                     const int nl = (int)std::min<int64_t>(sj.dim, p.lanc_ngfiter);
@@ -908,7 +908,7 @@ int dmfted_time_hxv(dmfted_ctx *c, int32_t flags, int32_t warmup, int32_t reps, 
     DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "time_hxv: bath not set");
     DM_CUDA(cudaSetDevice(c->device));
     const bool fp32 = (flags & 1) != 0, fused = (flags & 2) != 0;
-    SectorView s = sector_view(c, c->cur_sector);
+    SectorView s = (flags & 4) ? chain_view(c, c->cur_sector) : sector_view(c, c->cur_sector);
     const size_t es = fp32 ? 4 : 8;
     const size_t ld = (size_t)((s.dim + 31) / 32 * 32);
     c->chainbuf.alloc(3 * ld * es);

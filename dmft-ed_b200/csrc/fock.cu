@@ -345,6 +345,12 @@ SectorView sector_view(const dmfted_ctx *c, int isector) {
     return s;
 }
 
+SectorView chain_view(const dmfted_ctx *c, int isector) {
+    SectorView s = sector_view(c, isector);
+    s.swapped = s.dimup % 2 == 1 && s.dimdw % 2 == 0 && s.dimdw * 16 <= 200 * 1024;
+    return s;
+}
+
 void fock_build_map(dmfted_ctx *c, int isector, int32_t *d_map) {
     SectorView s = sector_view(c, isector);
     k_build_map<<<div_up(s.dim, 256), 256, 0, c->stream>>>(c->ns, s.dimup, s.dim,

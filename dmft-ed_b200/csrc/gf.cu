@@ -26,7 +26,7 @@ namespace dmfted {
 __global__ void __launch_bounds__(kRedThreads) k_apply_op(int ispin, int iorb, int particle,
                                                           int nup_i, int64_t dimup_i,
                                                           int64_t dimup_j, int64_t dim_j,
-                                                          const uint32_t *wu_j, const uint32_t *wd_j,
+                                                          int swap_j, const uint32_t *wu_j, const uint32_t *wd_j,
                                                           const int32_t *rank, const double *psi,
                                                           double *vv, double *norm2,
                                                           double *partials, unsigned *counter) {
@@ -35,7 +35,11 @@ __global__ void __launch_bounds__(kRedThreads) k_apply_op(int ispin, int iorb, i
     s.zero();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < dim_j;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t rj = i % dimup_j, cj = i / dimup_j;
+        // (up rank, down rank) of target element i; a swapped target stores
+        // idw + DimDw*iup
+        const int64_t dimdw_j = dim_j / dimup_j;
+        const int64_t rj = swap_j ? i / dimdw_j : i % dimup_j;
+        const int64_t cj = swap_j ? i % dimdw_j : i / dimup_j;
         const uint32_t wj = ispin == 0 ? wu_j[rj] : wd_j[cj];
         double val = 0.0;
         // particle: the target holds the site; hole: the target lacks it
@@ -143,10 +147,12 @@ __global__ void k_sigma(int nspin, int norb, int nbath, const double *e, const d
 
 void gf_apply_op(dmfted_ctx *c, const SectorView &si, const SectorView &sj, int iorb, int ispin,
                  bool particle, const double *psi, double *vv, double *d_norm2) {
+    DM_REQUIRE(!si.swapped, DMFTED_ERR_ARG, "apply_op: the source state is in the reference order");
     const int grid = (int)std::min<int64_t>(std::max<int64_t>(div_up(sj.dim, kRedThreads), 1),
                                             std::min(kMaxRedBlocks, 8 * num_sms(c)));
     k_apply_op<<<grid, kRedThreads, 0, c->stream>>>(
-        ispin, iorb, particle ? 1 : 0, si.nup, si.dimup, sj.dimup, sj.dim, c->words.p + sj.offup,
+        ispin, iorb, particle ? 1 : 0, si.nup, si.dimup, sj.dimup, sj.dim, sj.swapped ? 1 : 0,
+        c->words.p + sj.offup,
         c->words.p + sj.offdw, c->rank.p, psi, vv, d_norm2, c->red_partials.p, c->red_counter.p);
     DM_CHECK_LAUNCH();
     c->launches++;

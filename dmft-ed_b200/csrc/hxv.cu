@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256, kHxvMinBlocks) k_hxv(const HxvArgs<T> a) 
     const int64_t dimup = a.dimup, dimdw = a.dimdw, ncols = dimdw * a.nstack;
     for (int i = tid; i < a.P; i += bd) spu[i] = a.pu[i];
     const int ni = 1 << a.norb;
-    for (int i = tid; i < ni * ni; i += bd) sdint[i] = a.dint[i];
+    for (int i = tid; i < ni * ni; i += bd) sdint[i] = a.dint[a.dswap ? (i % ni) * ni + i / ni : i];
     const unsigned imask = (unsigned)ni - 1u;
 
     double sc = 1.0, cprev = 0.0;
@@ -117,6 +117,11 @@ __global__ void __launch_bounds__(256, kHxvMinBlocks) k_hxv(const HxvArgs<T> a) 
         sc = a.scale[a.k];
         cprev = a.k > 0 ? a.beta[a.k] * a.scale[a.k - 1] : 0.0;
     }
+    // u = sc*acc - cprev*xprev in the vector precision; for FP32 vectors both
+    // scalars are split into a float pair (hi + lo) so that they enter with
+    // full FP64 accuracy and only the final fused multiply-add rounds.
+    const T sch = (T)sc, scl = (T)(sc - (double)sch);
+    const T cph = (T)cprev, cpl = (T)(cprev - (double)cph);
     const T *x = a.x + (int64_t)blockIdx.y * a.vstride;
     T *y = a.y + (int64_t)blockIdx.y * a.vstride;
     T *xs = reinterpret_cast<T *>(smem_raw);  // [dimup][NC]
@@ -219,6 +224,15 @@ __global__ void __launch_bounds__(256, kHxvMinBlocks) k_hxv(const HxvArgs<T> a) 
             for (int j = 0; j < NC; j++) {
                 if (j < nc) {
                     const int ce = scnt[j];
+                    const int64_t idx = (c0 + j) * dimup + r;
+                    // v_{k-1} is loaded ahead of the down hops so that its
+                    // latency overlaps theirs (except FP64 two-row vectors,
+                    // where the extra live registers spill)
+                    constexpr bool kEarly = !(sizeof(T) == 8 && VW == 2);
+                    T xp[VW];
+                    if (LZ && kEarly) {
+                        if (DM_IN(idx + VW - 1, ncols * dimup)) vld<T, VW>(a.xprev + idx, xp);
+                    }
                     for (int e0 = 0; e0 < ce; e0 += kDwBatch) {
                         T xv[kDwBatch][VW];
 #pragma unroll
@@ -233,21 +247,38 @@ __global__ void __launch_bounds__(256, kHxvMinBlocks) k_hxv(const HxvArgs<T> a) 
                                 for (int i = 0; i < VW; i++) acc[j][i] += v * xv[q][i];
                             }
                     }
-                    const int64_t idx = (c0 + j) * dimup + r;
                     if (!DM_IN(idx + VW - 1, ncols * dimup)) continue;
                     if (LZ) {
-                        T xp[VW], ut[VW];
-                        vld<T, VW>(a.xprev + idx, xp);
+                        if (!kEarly) vld<T, VW>(a.xprev + idx, xp);
 #pragma unroll
                         for (int i = 0; i < VW; i++) {
-                            ut[i] = (T)(sc * (double)acc[j][i] - cprev * (double)xp[i]);
-                            dot.add((double)xs[(r + i) * NC + j] * (double)ut[i]);
+                            if constexpr (sizeof(T) == 8) {
+                                acc[j][i] = sc * acc[j][i] - cprev * xp[i];
+                            } else {
+                                T t = -cpl * xp[i];
+                                t = fmaf(-cph, xp[i], t);
+                                t = fmaf(scl, acc[j][i], t);
+                                acc[j][i] = fmaf(sch, acc[j][i], t);
+                            }
                         }
-                        vst_cs<T, VW>(y + idx, ut);
-                    } else {
-                        vst_cs<T, VW>(y + idx, acc[j]);
                     }
+                    vst_cs<T, VW>(y + idx, acc[j]);
                 }
+            }
+            if (LZ) {
+                // <x, u> over this row vector: the staged rows are re-read
+                // as NC-wide vectors; products of two floats are exact in
+                // FP64, and one compensated add per row vector
+                double part = 0.0;
+#pragma unroll
+                for (int i = 0; i < VW; i++) {
+                    T xr[NC];
+                    vld<T, NC>(xs + (r + i) * NC, xr);
+#pragma unroll
+                    for (int j = 0; j < NC; j++)
+                        if (j < nc) part = fma((double)xr[j], (double)acc[j][i], part);
+                }
+                dot.add(part);
             }
         }
     }
@@ -263,30 +294,37 @@ __global__ void __launch_bounds__(256, kHxvMinBlocks) k_hxv(const HxvArgs<T> a) 
 template <typename T>
 HxvArgs<T> make_hxv_args(const dmfted_ctx *c, const SectorView &s) {
     HxvArgs<T> a{};
+    // rows (r) and columns (q) of the stored vector: up and down spin in the
+    // reference order, exchanged for a swapped view (H = H_up + H_dw + D is
+    // symmetric in the two factors; the hop signs depend on one spin only)
+    const bool sw = s.swapped;
     const SpinTables &tu = c->spin[0];
     const SpinTables &td = c->spin_shared ? c->spin[0] : c->spin[1];
-    a.dimup = s.dimup;
-    a.dimdw = s.dimdw;
+    const SpinTables &tr = sw ? td : tu, &tq = sw ? tu : td;
+    const int64_t offr = sw ? s.offdw : s.offup, offq = sw ? s.offup : s.offdw;
+    a.dimup = sw ? s.dimdw : s.dimup;
+    a.dimdw = sw ? s.dimup : s.dimdw;
     a.norb = c->norb;
     a.P = c->P;
     a.W = std::max(c->W, 1);
-    a.wu = c->words.p + s.offup;
-    a.wd = c->words.p + s.offdw;
-    a.cu = tu.cnt.p + s.offup;
-    a.cd = td.cnt.p + s.offdw;
-    a.eu = tu.ell.p + (int64_t)a.W * s.offup;
-    a.ed = td.ell.p + (int64_t)a.W * s.offdw;
+    a.wu = c->words.p + offr;
+    a.wd = c->words.p + offq;
+    a.cu = tr.cnt.p + offr;
+    a.cd = tq.cnt.p + offq;
+    a.eu = tr.ell.p + (int64_t)a.W * offr;
+    a.ed = tq.ell.p + (int64_t)a.W * offq;
+    a.dswap = sw ? 1 : 0;
     if constexpr (sizeof(T) == 8) {
-        a.du = (const T *)tu.diag.p + s.offup;
-        a.dd = (const T *)td.diag.p + s.offdw;
-        a.pu = (const T *)tu.par.p;
-        a.pd = (const T *)td.par.p;
+        a.du = (const T *)tr.diag.p + offr;
+        a.dd = (const T *)tq.diag.p + offq;
+        a.pu = (const T *)tr.par.p;
+        a.pd = (const T *)tq.par.p;
         a.dint = (const T *)c->dint.p;
     } else {
-        a.du = (const T *)tu.diag_f.p + s.offup;
-        a.dd = (const T *)td.diag_f.p + s.offdw;
-        a.pu = (const T *)tu.par_f.p;
-        a.pd = (const T *)td.par_f.p;
+        a.du = (const T *)tr.diag_f.p + offr;
+        a.dd = (const T *)tq.diag_f.p + offq;
+        a.pu = (const T *)tr.par_f.p;
+        a.pd = (const T *)tq.par_f.p;
         a.dint = (const T *)c->dint_f.p;
     }
     a.vstride = s.dim;
@@ -313,19 +351,19 @@ template <typename T>
 static HxvCfg hxv_config(dmfted_ctx *c, const SectorView &s, const HxvArgs<T> &a, int nstack = 1) {
     HxvCfg g;
     // two rows per thread-vector: 8-byte (FP32) or 16-byte (FP64) accesses;
-    // needs DimUp even and every base pointer aligned to the vector size
+    // needs an even row count and every base pointer aligned to the vector size
     const size_t vb = 2 * sizeof(T);
     const bool aligned = aligned_to(a.x, vb) && aligned_to(a.y, vb) &&
                          (!a.xprev || aligned_to(a.xprev, vb)) && aligned_to(a.wu, 8) &&
                          aligned_to(a.du, vb) && aligned_to(a.eu, 8) && aligned_to(a.cu, 2) &&
                          ((a.vstride * (int64_t)sizeof(T)) % vb == 0);
-    g.vw = (s.dimup % 2 == 0 && aligned) ? 2 : 1;
-    const int64_t ncols = s.dimdw * nstack;
+    g.vw = (a.dimup % 2 == 0 && aligned) ? 2 : 1;
+    const int64_t ncols = a.dimdw * nstack;
     g.nc = 16 / (int)sizeof(T);  // one 16-byte gather serves the whole tile
-    const size_t tile = (size_t)s.dimup * sizeof(T) * g.nc;
+    const size_t tile = (size_t)a.dimup * sizeof(T) * g.nc;
     DM_REQUIRE(tile <= 200 * 1024, DMFTED_ERR_UNSUPPORTED,
                "sector column too long for the shared-memory H*v (DimUp too large)");
-    g.threads = (s.dimup <= (int64_t)128 * g.vw * 2) ? 128 : 256;
+    g.threads = (a.dimup <= (int64_t)128 * g.vw * 2) ? 128 : 256;
     g.smem = tile;
     g.grid = (int)std::min<int64_t>((ncols + g.nc - 1) / g.nc, kMaxRedBlocks);
     return g;

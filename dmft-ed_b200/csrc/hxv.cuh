@@ -37,12 +37,12 @@ struct HxvArgs {
     const uint32_t *eu, *ed;   // ELL (row stride dimup / dimdw)
     const T *pu, *pd;          // coupling values
     const T *dint;             // (1<<norb)^2 impurity diagonal
+    int dswap;                 // rows are down words: dint is indexed [dw][up]
     const T *x;
     T *y;
     int64_t vstride;           // batched plain products: elements between vectors
     int nstack;                // copies of the sector stacked as extra columns
                                // (a complex vector = re and im halves, since H is real)
-    // Jhflag spin-exchange / pair-hopping (plain H*v only, see hxv_jh)
     // fused Lanczos step
     const T *xprev;
     double *alpha, *beta, *scale;

@@ -147,6 +147,11 @@ struct SectorView {
     int nup, ndw;
     int64_t dimup, dimdw, dim;
     int64_t offup, offdw;  // class offsets into word-indexed arrays
+    // Vectors of this view are stored transposed, idw + DimDw*iup, instead of
+    // the reference order iup + DimUp*idw.  Only for device-internal vectors
+    // (Green's-function chains) of sectors with odd DimUp and even DimDw, so
+    // that the H*v rows pair into aligned two-element vectors.
+    bool swapped = false;
 };
 
 // Per-phase timing / counting of the last solve.
@@ -233,6 +238,7 @@ namespace dmfted {
 void fock_init(dmfted_ctx *c);              // words, rank, class offsets
 void fock_set_couplings(dmfted_ctx *c);     // cnt/ell/diag/par for both spins, dint
 SectorView sector_view(const dmfted_ctx *c, int isector);
+SectorView chain_view(const dmfted_ctx *c, int isector);
 void fock_build_map(dmfted_ctx *c, int isector, int32_t *d_map);  // combined map
 
 // ---- hxv.cu --------------------------------------------------------------

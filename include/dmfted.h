@@ -236,8 +236,9 @@ int dmfted_chi2_delta_batch_device(dmfted_ctx *ctx, int32_t nbatch, int32_t nbat
 /* Average device milliseconds of one H*v on the current sector over reps
  * launches after warmup launches.  flags: bit 0 = float32 vectors (else
  * float64), bit 1 = the fused Lanczos-step variant (H*v - b v_prev and the
- * alpha dot product) instead of the plain product.  The vectors are the
- * context's own work buffers. */
+ * alpha dot product) instead of the plain product, bit 2 = the vector order
+ * used by Green's-function chains (down rank fastest when DimUp is odd and
+ * DimDw even).  The vectors are the context's own work buffers. */
 int dmfted_time_hxv(dmfted_ctx *ctx, int32_t flags, int32_t warmup, int32_t reps, double *ms);
 
 /* Device milliseconds of the last dmfted_ed_solve, split into phases:
