@@ -121,18 +121,22 @@ static void upload_model(dmfted_ctx *c) {
 // Kept states of the eigenspace: a device pool of FP64 vectors.
 static void states_reset(dmfted_ctx *c) { c->states.clear(); }
 
+static int64_t state_dim(const dmfted_ctx *c, int isector) {
+    return c->binom[c->getnup[isector - 1]] * c->binom[c->getndw[isector - 1]];
+}
+
 static int64_t states_used(const dmfted_ctx *c) {
     int64_t u = 0;
-    for (auto &s : c->states) u = std::max<int64_t>(u, s.off + c->binom[c->getnup[s.isector - 1]] *
-                                                                 c->binom[c->getndw[s.isector - 1]]);
+    for (auto &s : c->states)
+        if (!s.src) u = std::max<int64_t>(u, s.off + state_dim(c, s.isector));
     return u;
 }
 
-static void states_add(dmfted_ctx *c, double e, int isector, const double *psi, int64_t dim) {
-    const int64_t used = states_used(c);        // elements in use (<= states64.n)
-    const int64_t off = (used + 31) / 32 * 32;  // 256-byte aligned start of the new vector
-    if ((size_t)(off + dim) > c->states64.n) {
-        const size_t cap = std::max<size_t>((size_t)(off + dim), c->states64.n * 2);
+// Grows the eigenspace store to hold `need` elements, keeping the first
+// `used` ones.
+static void states_reserve(dmfted_ctx *c, int64_t used, int64_t need) {
+    if ((size_t)need > c->states64.n) {
+        const size_t cap = std::max<size_t>((size_t)need, c->states64.n * 2);
         double *np = nullptr;
         cudaError_t err = cudaMalloc((void **)&np, cap * sizeof(double));
         DM_REQUIRE(err == cudaSuccess, DMFTED_ERR_NOMEM, "cudaMalloc for the eigenspace failed");
@@ -144,14 +148,43 @@ static void states_add(dmfted_ctx *c, double e, int isector, const double *psi, 
         c->states64.p = np;
         c->states64.n = cap;
     }
+}
+
+// Energy-ordered insertion after equal energies (es_insert_state_c,
+// ED_EIGENSPACE.f90:157-213: traverse until e <= next).
+static void states_insert(dmfted_ctx *c, const dmfted_ctx::State &st) {
+    auto it = c->states.begin();
+    while (it != c->states.end() && !(st.e <= it->e)) ++it;
+    c->states.insert(it, st);
+}
+
+static void states_add(dmfted_ctx *c, double e, int isector, const double *psi, int64_t dim) {
+    const int64_t used = states_used(c);        // elements in use (<= states64.n)
+    const int64_t off = (used + 31) / 32 * 32;  // 256-byte aligned start of the new vector
+    states_reserve(c, used, off + dim);
     DM_CUDA(cudaMemcpyAsync(c->states64.p + off, psi, dim * sizeof(double), cudaMemcpyDeviceToDevice,
                             c->stream));
     DM_CUDA(cudaStreamSynchronize(c->stream));  // psi is a scratch buffer the next sector reuses
-    // energy-ordered insertion after equal energies (es_insert_state_c,
-    // ED_EIGENSPACE.f90:157-213: traverse until e <= next)
-    auto it = c->states.begin();
-    while (it != c->states.end() && !(e <= it->e)) ++it;
-    c->states.insert(it, dmfted_ctx::State{e, isector, off});
+    states_insert(c, dmfted_ctx::State{e, isector, off, nullptr});
+}
+
+// Copies every state still held by the batch pool into the store.
+static void states_materialize(dmfted_ctx *c) {
+    int64_t used = states_used(c), need = (used + 31) / 32 * 32;
+    for (auto &s : c->states)
+        if (s.src) need = (need + state_dim(c, s.isector) + 31) / 32 * 32;
+    states_reserve(c, used, need);
+    int64_t off = (used + 31) / 32 * 32;
+    for (auto &s : c->states) {
+        if (!s.src) continue;
+        const int64_t dim = state_dim(c, s.isector);
+        DM_CUDA(cudaMemcpyAsync(c->states64.p + off, s.src, dim * sizeof(double),
+                                cudaMemcpyDeviceToDevice, c->stream));
+        s.off = off;
+        s.src = nullptr;
+        off = (off + dim + 31) / 32 * 32;
+    }
+    DM_CUDA(cudaStreamSynchronize(c->stream));
 }
 
 __global__ void k_interleave_split(const double *z, double *re, double *im, int64_t n) {
@@ -188,13 +221,12 @@ static void real_to_host_c128(dmfted_ctx *c, const double *d, int64_t n, double 
 // limit insert; at the limit insert only below the highest energy, which is
 // popped first (es_pop_state, :219-299).
 static void states_add_capped(dmfted_ctx *c, double e, int isector, const double *psi, int64_t dim,
-                              int size) {
-    if ((int)c->states.size() < size) {
-        states_add(c, e, isector, psi, dim);
-    } else if (!c->states.empty() && e < c->states.back().e) {
-        c->states.pop_back();
-        states_add(c, e, isector, psi, dim);
-    }
+                              int size, bool deferred = false) {
+    const bool take = (int)c->states.size() < size;
+    if (!take && !(!c->states.empty() && e < c->states.back().e)) return;
+    if (!take) c->states.pop_back();
+    if (deferred) states_insert(c, dmfted_ctx::State{e, isector, -1, psi});
+    else states_add(c, e, isector, psi, dim);
 }
 
 // ed_diag_c, finite-temperature branch (ED_DIAG.f90:93-228): for every sector
@@ -204,21 +236,41 @@ static int64_t ed_diag_finite_t(dmfted_ctx *c, const std::vector<int> &list) {
     const dmfted_params &p = c->p;
     states_reset(c);
     int64_t hv = 0;
+    // sectors small enough for one CTA run together first; every sector then
+    // enters the list in the reference's order
+    // Eigenpairs are FP64 in both precision modes: a Krylov basis kept in
+    // FP32 is orthogonal only to ~1e-7, and the recurrence then returns
+    // spurious copies of converged eigenvalues, which change the kept list.
+    // (DMFTED_FT_EIGS_FP32=1 selects FP32 vectors here for measurement.)
+    const int eprec = c->ft_eigs_fp32 ? p.precision : DMFTED_FP64;
+    std::vector<BatchEig> batched;
+    batch_eigs(c, list, eprec, batched);
     std::vector<double> ev(kLzMax + 8);
-    for (int isector : list) {
+    for (size_t li = 0; li < list.size(); li++) {
+        const int isector = list[li];
         SectorView s = sector_view(c, isector);
+        if (batched[li].m >= 0) {
+            hv += batched[li].steps;
+            // the batch pool keeps these vectors: only the survivors are copied
+            for (int i = 0; i < batched[li].m; i++)
+                states_add_capped(c, batched[li].evals[i], isector,
+                                  batched[li].vecs + (size_t)i * s.dim, s.dim, c->nstates_total,
+                                  true);
+            continue;
+        }
         const int neigen = (int)std::min<int64_t>(s.dim, c->neigen_sector[isector - 1]);
         if (neigen <= 0) continue;
         const int nit = (int)std::min<int64_t>(s.dim, p.lanc_niter);
         c->eigvecs.alloc((size_t)neigen * s.dim);
         int steps = 0;
-        const int m = lanczos_eigs(c, s, neigen, p.precision, p.lanc_tolerance, nit, ev.data(),
+        const int m = lanczos_eigs(c, s, neigen, eprec, p.lanc_tolerance, nit, ev.data(),
                                    c->eigvecs.p, &steps);
         hv += steps;
         for (int i = 0; i < m; i++)
             states_add_capped(c, ev[i], isector, c->eigvecs.p + (size_t)i * s.dim, s.dim,
                               c->nstates_total);
     }
+    states_materialize(c);
     return hv;
 }
 
@@ -338,7 +390,6 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     c->hf_terms.assign(acc.begin() + 3 * no, acc.end());
     DM_CUDA(cudaEventRecord(ev[2], c->stream));
     // ---- Green's functions ---------------------------------------------------
-    const int L = p.lmats + p.lreal;
     const size_t gsz = (size_t)c->nspin * no;
     c->gm.alloc(std::max<size_t>(2 * gsz * p.lmats, 2));
     c->gr.alloc(std::max<size_t>(2 * gsz * p.lreal, 2));
@@ -348,10 +399,8 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     DM_CUDA(cudaMemsetAsync(c->gm.p, 0, c->gm.n * sizeof(double), c->stream));
     DM_CUDA(cudaMemsetAsync(c->gr.p, 0, c->gr.n * sizeof(double), c->stream));
     int64_t hv_gf = 0;
-    const int gf_prec = p.precision;
+    std::vector<ChainRec> recs;
     for (auto &st : c->states) {
-        SectorView si = sector_view(c, st.isector);
-        const double *psi = c->states64.p + st.off;
         double weight;
         if (c->finite_t && p.beta * (st.e - c->egs) < 200.0)
             weight = std::exp(-p.beta * (st.e - c->egs)) / c->zeta;
@@ -361,27 +410,27 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
             weight = 0.0;
         if (weight == 0.0) continue;  // pesoBZ = 0: the chains add nothing
         for (int ispin = 0; ispin < c->nspin; ispin++)
-            for (int iorb = 0; iorb < no; iorb++) {
-                double *gmo = c->gm.p + 2 * (size_t)(ispin * no + iorb) * p.lmats;
-                double *gro = c->gr.p + 2 * (size_t)(ispin * no + iorb) * p.lreal;
+            for (int iorb = 0; iorb < no; iorb++)
                 for (int ph = 0; ph < 2; ph++) {
                     const bool particle = ph == 0;
                     const int js = particle ? c->getcdgsector[2 * (st.isector - 1) + ispin]
                                             : c->getcsector[2 * (st.isector - 1) + ispin];
                     if (js == 0) continue;
-                    SectorView sj = chain_view(c, js);
-                    c->s64b.alloc(sj.dim);
-                    gf_apply_op(c, si, sj, iorb, ispin, particle, psi, c->s64b.p, c->red_out.p + 2);
-                    const int nl = (int)std::min<int64_t>(sj.dim, p.lanc_ngfiter);
-                    LanczosScalars lz = lz_slot(c, 1, nl);
-                    lanczos_chain(c, sj, c->s64b.p, gf_prec, lz);
-                    if (L > 0)
-                        gf_add_chain(c, lz.alpha, lz.beta, lz.status + 1, c->red_out.p + 2, weight,
-                                     st.e, particle ? 1 : -1, gmo, gro);
-                    hv_gf += nl;
+                    ChainRec r;
+                    r.psi_off = st.off;
+                    r.isector = st.isector;
+                    r.jsector = js;
+                    r.ispin = ispin;
+                    r.iorb = iorb;
+                    r.particle = particle ? 1 : 0;
+                    r.nlanc = (int)std::min<int64_t>(sector_view(c, js).dim, p.lanc_ngfiter);
+                    r.weight = weight;
+                    r.e = st.e;
+                    recs.push_back(r);
+                    hv_gf += r.nlanc;
                 }
-            }
     }
+    batch_chains_gf(c, recs, p.precision);
     gf_sigma(c);
     DM_CUDA(cudaEventRecord(ev[3], c->stream));
     DM_CUDA(cudaStreamSynchronize(c->stream));
@@ -517,6 +566,11 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         c->device = p->device;
         if (const char *e = getenv("DMFTED_HXV_NC")) c->tune_nc = atoi(e);
         if (const char *e = getenv("DMFTED_MIXED_TOL32")) c->mixed_tol32 = atof(e);
+        if (const char *e = getenv("DMFTED_BATCH_MAX_DIM")) c->batch_max_dim = atoll(e);
+        if (const char *e = getenv("DMFTED_BATCH_BUDGET_MB")) c->batch_budget = atoll(e) << 20;
+        if (const char *e = getenv("DMFTED_FT_EIGS_FP32")) c->ft_eigs_fp32 = atoi(e) != 0;
+        if (const char *e = getenv("DMFTED_BATCH_CLUSTER_MIN"))
+            c->batch_cluster_min = std::max<int64_t>(1, atoll(e));
         DM_CUDA(cudaSetDevice(c->device));
         DM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         const size_t nh = 2 * (size_t)c->nspin * c->nspin * c->norb * c->norb;

@@ -10,12 +10,8 @@
 // |up>|dw> (ED_SETUP.f90:1055-1081); for a down site that includes all nup
 // up electrons.
 //
-// K7 (k_gf_cf): adds pref * sum_j Z(1,j)^2 / (z - isign (E_j - E_i)) for every
-// frequency.  The reference diagonalises the chain's tridiagonal with tql2 and
-// sums the poles (add_to_lanczos_gf_normal, build_gf_normal.f90:442-488); the
-// same sum is the continued fraction 1/(zeta - a_0 - b_1^2/(zeta - a_1 - ...))
-// at zeta = z + E_i (particle) or -(...) at zeta = E_i - z (hole), evaluated
-// bottom-up in FP64 by one thread per frequency.
+// The chains' contributions to G (the pole sums of add_to_lanczos_gf_normal)
+// are evaluated as continued fractions in batch.cu.
 #include <algorithm>
 
 #include "internal.cuh"
@@ -77,41 +73,6 @@ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
     }
 }
 
-__global__ void k_gf_cf(const double *alpha, const double *beta, const int *nsteps,
-                        const double *norm2, double weight, double ei, int isign, const double *wm,
-                        int lmats, const double *wr, int lreal, double eps, double2 *gm,
-                        double2 *gr) {
-    __shared__ double sa[1024], sb2[1024];
-    const int n = *nsteps;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        sa[i] = alpha[i];
-        sb2[i] = i > 0 ? beta[i] * beta[i] : 0.0;
-    }
-    __syncthreads();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= lmats + lreal || n <= 0) return;
-    const double2 z = t < lmats ? make_double2(0.0, wm[t]) : make_double2(wr[t - lmats], eps);
-    const double2 zeta = isign > 0 ? make_double2(z.x + ei, z.y) : make_double2(ei - z.x, -z.y);
-    double2 den = make_double2(zeta.x - sa[n - 1], zeta.y);
-    for (int k = n - 2; k >= 0; k--) {
-        const double2 q = cdiv(make_double2(sb2[k + 1], 0.0), den);
-        den = make_double2(zeta.x - sa[k] - q.x, zeta.y - q.y);
-    }
-    const double2 cf = cdiv(make_double2(1.0, 0.0), den);
-    const double pref = (isign > 0 ? 1.0 : -1.0) * weight * (*norm2);
-    if (t < lmats) {
-        double2 g = gm[t];
-        g.x += pref * cf.x;
-        g.y += pref * cf.y;
-        gm[t] = g;
-    } else {
-        double2 g = gr[t - lmats];
-        g.x += pref * cf.x;
-        g.y += pref * cf.y;
-        gr[t - lmats] = g;
-    }
-}
-
 // Sigma = G0^-1 - G^-1 with G0^-1 = z + xmu - Hloc_aa - Delta(z),
 // Delta(z) = sum_k V_k^2/(z - e_k) (get_sigma_normal.f90:17-39,
 // ED_BATH_FUNCTIONS.f90:247-257,1800-1806), and G0and = 1/G0^-1
@@ -154,18 +115,6 @@ void gf_apply_op(dmfted_ctx *c, const SectorView &si, const SectorView &sj, int 
         ispin, iorb, particle ? 1 : 0, si.nup, si.dimup, sj.dimup, sj.dim, sj.swapped ? 1 : 0,
         c->words.p + sj.offup,
         c->words.p + sj.offdw, c->rank.p, psi, vv, d_norm2, c->red_partials.p, c->red_counter.p);
-    DM_CHECK_LAUNCH();
-    c->launches++;
-}
-
-void gf_add_chain(dmfted_ctx *c, const double *d_alpha, const double *d_beta, const int *d_n,
-                  const double *d_norm2, double weight, double ei, int isign, double *gm,
-                  double *gr) {
-    const int L = c->p.lmats + c->p.lreal;
-    if (L <= 0) return;
-    k_gf_cf<<<div_up(L, 256), 256, 0, c->stream>>>(d_alpha, d_beta, d_n, d_norm2, weight, ei, isign,
-                                                   c->d_wm.p, c->p.lmats, c->d_wr.p, c->p.lreal,
-                                                   c->p.eps, (double2 *)gm, (double2 *)gr);
     DM_CHECK_LAUNCH();
     c->launches++;
 }

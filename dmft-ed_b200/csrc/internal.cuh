@@ -213,12 +213,26 @@ struct dmfted_ctx {
     dmfted::DBuf<double> obs_d;           // observable accumulators of one state
     dmfted::DBuf<double> eig_aux;         // Ritz values, vectors of T, coefficients, dots
     dmfted::DBuf<double> eigvecs;         // eigenvectors of one sector (Neigen x dim)
+    // persistent work-queue path (batch.cu): sectors up to batch_max_dim
+    // states run one job per CTA
+    int64_t batch_max_dim = 1 << 17;
+    int64_t batch_budget = 0;             // bytes of Krylov bases per launch (0: a third of free)
+    int64_t batch_cluster_min = 1024;     // states per CTA for a job shared by a cluster
+    bool ft_eigs_fp32 = false;            // finite-T eigenpairs with FP32 vectors (measurement only)
+    dmfted::DBuf<uint8_t> bwork;          // Krylov bases / chain vectors of the jobs
+    dmfted::DBuf<double> bvec;            // eigenvectors of the batched sectors
+    dmfted::DBuf<double> baux;            // Ritz vectors and coefficients
+    dmfted::DBuf<uint8_t> bjobs;          // job tables
+    dmfted::DBuf<double> bscal;           // chain alpha / beta, norm2; eigenvalues
+    dmfted::DBuf<int> bint;               // queue counter, step counts
+    dmfted::DBuf<double> bcf;             // continued-fraction terms (chain x frequency)
     int64_t launches = 0;
     // results of the last solve (device and host)
     struct State {
         double e;
         int isector;
-        int64_t off;  // offset (elements) of the vector in states64
+        int64_t off;                  // offset (elements) of the vector in states64
+        const double *src = nullptr;  // not yet copied: the vector is still here
     };
     std::vector<State> states;  // energy-ordered eigenspace
     dmfted::DBuf<double> states64;
@@ -239,6 +253,28 @@ void fock_init(dmfted_ctx *c);              // words, rank, class offsets
 void fock_set_couplings(dmfted_ctx *c);     // cnt/ell/diag/par for both spins, dint
 SectorView sector_view(const dmfted_ctx *c, int isector);
 SectorView chain_view(const dmfted_ctx *c, int isector);
+
+// ---- batch.cu ------------------------------------------------------------
+// Lowest eigenpairs of many sectors, one CTA per sector.  For every entry of
+// `list`: results[i].m >= 0 when the sector ran here (m eigenpairs, values in
+// evals, FP64 vectors at vecs, dim apart), -1 when it must take the grid path
+// (too large, or neigen == 0 gives m = 0).
+struct BatchEig {
+    int m = -1, steps = 0;
+    std::vector<double> evals;
+    const double *vecs = nullptr;
+};
+void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, int precision,
+                std::vector<BatchEig> &results);
+// Green's-function chains: one record per chain, in accumulation order.
+struct ChainRec {
+    int64_t psi_off;  // state vector in states64
+    int isector, jsector, ispin, iorb, particle, nlanc;
+    double weight, e;
+};
+// Runs every chain (one CTA per chain up to batch_max_dim states, the grid
+// path above it) and adds all of them to the Matsubara / real-axis G.
+void batch_chains_gf(dmfted_ctx *c, const std::vector<ChainRec> &recs, int precision);
 void fock_build_map(dmfted_ctx *c, int isector, int32_t *d_map);  // combined map
 
 // ---- hxv.cu --------------------------------------------------------------
@@ -288,10 +324,6 @@ int lanczos_eigs(dmfted_ctx *c, const SectorView &s, int neigen, int precision, 
 // |vv|^2 -> *d_norm2 (device).  Asynchronous.
 void gf_apply_op(dmfted_ctx *c, const SectorView &si, const SectorView &sj, int iorb, int ispin,
                  bool particle, const double *psi, double *vv, double *d_norm2);
-// G(z) += weight * norm2 * CF(z) on the Lmats and Lreal grids.
-void gf_add_chain(dmfted_ctx *c, const double *d_alpha, const double *d_beta, const int *d_n,
-                  const double *d_norm2, double weight, double ei, int isign, double *gm,
-                  double *gr);
 void gf_sigma(dmfted_ctx *c);  // impSmats/impSreal/impG0mats from impG*
 
 // ---- observables.cu --------------------------------------------------------

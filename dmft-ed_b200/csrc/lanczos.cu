@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "hxv.cuh"
+#include "tridiag.cuh"
 
 namespace dmfted {
 
@@ -105,116 +106,6 @@ __global__ void __launch_bounds__(kRedThreads) k_lz_init(const T *s0, int64_t n,
     }
 }
 
-// Sturm count: number of eigenvalues of the n x n tridiagonal (a, b[1..n-1])
-// below x.
-__device__ int sturm_count(const double *a, const double *b, int n, double x, double pivmin) {
-    int cnt = 0;
-    double q = a[0] - x;
-    if (fabs(q) < pivmin) q = -pivmin;
-    if (q < 0.0) cnt++;
-    for (int i = 1; i < n; i++) {
-        q = (a[i] - x) - b[i] * b[i] / q;
-        if (fabs(q) < pivmin) q = -pivmin;
-        if (q < 0.0) cnt++;
-    }
-    return cnt;
-}
-
-// j-th lowest eigenvalue (0-based) of T_n by multisection with all threads of
-// the block; a, b in shared memory.  Returns the value in every thread.
-__device__ double tridiag_eig(const double *a, const double *b, int n, int j) {
-    __shared__ int cnts[kRedThreads];
-    __shared__ double lohi[2];
-    if (threadIdx.x == 0) {
-        double lo = a[0], hi = a[0], amax = 0.0;
-        for (int i = 0; i < n; i++) {
-            const double r = (i > 0 ? fabs(b[i]) : 0.0) + (i + 1 < n ? fabs(b[i + 1]) : 0.0);
-            lo = fmin(lo, a[i] - r);
-            hi = fmax(hi, a[i] + r);
-            amax = fmax(amax, fabs(a[i]) + r);
-        }
-        const double pad = 2.2e-16 * fmax(amax, 1e-300) * 4.0 + 1e-300;
-        lohi[0] = lo - pad;
-        lohi[1] = hi + pad;
-    }
-    __syncthreads();
-    double amax = fmax(fabs(lohi[0]), fabs(lohi[1]));
-    const double pivmin = 1e-300 + 2.2e-16 * 2.2e-16 * fmax(amax * amax, 1e-300);
-    for (int round = 0; round < 40; round++) {
-        const double lo = lohi[0], hi = lohi[1];
-        if (hi - lo <= 2.0 * 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300) break;
-        const int nt = blockDim.x;
-        const double x = lo + (hi - lo) * (double)(threadIdx.x + 1) / (double)(nt + 1);
-        cnts[threadIdx.x] = sturm_count(a, b, n, x, pivmin);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int t = 0;
-            while (t < nt && cnts[t] <= j) t++;
-            const double nlo = t == 0 ? lo : lo + (hi - lo) * (double)t / (double)(nt + 1);
-            const double nhi = t == nt ? hi : lo + (hi - lo) * (double)(t + 1) / (double)(nt + 1);
-            lohi[0] = nlo;
-            lohi[1] = nhi;
-        }
-        __syncthreads();
-    }
-    const double r = 0.5 * (lohi[0] + lohi[1]);
-    __syncthreads();
-    return r;
-}
-
-// Eigenvector y of T_n (diag a[0..n), off-diagonal b[1..n)) for eigenvalue
-// lam: three steps of inverse iteration, Gaussian elimination with partial
-// pivoting on the tridiagonal.  Single thread.  ws: 5n doubles, sw: n bytes.
-__device__ void tridiag_evec(const double *a, const double *b, int n, double lam, double *yv,
-                             double *ws, unsigned char *sw) {
-    double *D = ws, *U1 = ws + n, *U2 = ws + 2 * n, *M = ws + 3 * n;
-    double nrm = 0.0;
-    for (int i = 0; i < n; i++) nrm = fmax(nrm, fabs(a[i] - lam) + (i > 0 ? fabs(b[i]) : 0.0));
-    const double tiny = fmax(nrm, 1e-300) * 1e-15;
-    double d = a[0] - lam, u1 = n > 1 ? b[1] : 0.0, u2 = 0.0;
-    for (int i = 0; i < n - 1; i++) {
-        const double l = b[i + 1], dn = a[i + 1] - lam, un = (i + 2 < n) ? b[i + 2] : 0.0;
-        if (fabs(d) >= fabs(l)) {
-            if (d == 0.0) d = tiny;
-            const double m = l / d;
-            D[i] = d; U1[i] = u1; U2[i] = u2; M[i] = m; sw[i] = 0;
-            d = dn - m * u1;
-            u1 = un - m * u2;
-            u2 = 0.0;
-        } else {
-            const double m = d / l;
-            D[i] = l; U1[i] = dn; U2[i] = un; M[i] = m; sw[i] = 1;
-            d = u1 - m * dn;
-            u1 = u2 - m * un;
-            u2 = 0.0;
-        }
-    }
-    if (d == 0.0) d = tiny;
-    D[n - 1] = d;
-    for (int i = 0; i < n; i++) yv[i] = 1.0 / sqrt((double)n);
-    for (int it = 0; it < 3; it++) {
-        for (int i = 0; i < n - 1; i++) {
-            if (sw[i]) {
-                const double t = yv[i];
-                yv[i] = yv[i + 1];
-                yv[i + 1] = t;
-            }
-            yv[i + 1] -= M[i] * yv[i];
-        }
-        yv[n - 1] /= D[n - 1];
-        if (n > 1) yv[n - 2] = (yv[n - 2] - U1[n - 2] * yv[n - 1]) / D[n - 2];
-        for (int i = n - 3; i >= 0; i--) yv[i] = (yv[i] - U1[i] * yv[i + 1] - U2[i] * yv[i + 2]) / D[i];
-        double ss = 0.0;
-        for (int i = 0; i < n; i++) ss += yv[i] * yv[i];
-        ss = 1.0 / sqrt(ss);
-        for (int i = 0; i < n; i++) yv[i] *= ss;
-    }
-    const double sg = yv[0] < 0.0 ? -1.0 : 1.0;  // deterministic sign
-    for (int i = 0; i < n; i++) yv[i] *= sg;
-}
-
-// Dynamic shared memory of the two Ritz kernels for n steps.
-__host__ __device__ inline size_t ritz_smem(int n) { return (size_t)8 * n * sizeof(double) + n + 16; }
 
 // Every ncheck steps: lowest Ritz value theta of T_n and the ARPACK stopping
 // test on its Ritz estimate, b_n |y_n| <= tol * max(eps^(2/3), |theta|)
@@ -352,13 +243,8 @@ __global__ void k_convert(const TI *in, TO *out, int64_t n) {
 // hands ARPACK (.repo/ARPACK_LANCZOS.f90:394-403).
 __global__ void k_random_start(double *x, int64_t n, uint64_t seed) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(i + 1);
-        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-        z = z ^ (z >> 31);
-        x[i] = ((double)(z >> 11) + 1.0) * (1.0 / 9007199254740992.0);
-    }
+         i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = random_start_value(i, seed);
 }
 
 // ---------------------------------------------------------------------------
@@ -675,38 +561,15 @@ __global__ void k_ritz_multi(LanczosScalars lz, double tol, int mwant, double *e
     extern __shared__ double rs[];
     const int n = lz.status[ST_STEPS];
     if (n <= 0) return;
-    double *sa = rs, *sb = rs + n, *yv = rs + 2 * n, *ws = rs + 3 * n;
-    unsigned char *sw = reinterpret_cast<unsigned char *>(rs + 8 * n);
+    double *sa = rs, *sb = rs + n;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         sa[i] = lz.alpha[i];
         sb[i] = i > 0 ? lz.beta[i] : 0.0;
     }
     __syncthreads();
-    const int m = min(mwant, n);
-    bool ok = true;
-    for (int j = 0; j < m; j++) {
-        const double e = tridiag_eig(sa, sb, n, j);
-        if (threadIdx.x == 0) {
-            tridiag_evec(sa, sb, n, e, yv, ws, sw);
-            // orthogonalise against the lower eigenvectors (close eigenvalues)
-            for (int q = 0; q < j; q++) {
-                double d = 0.0;
-                for (int i = 0; i < n; i++) d += Y[(int64_t)q * n + i] * yv[i];
-                for (int i = 0; i < n; i++) yv[i] -= d * Y[(int64_t)q * n + i];
-            }
-            double nr = 0.0;
-            for (int i = 0; i < n; i++) nr += yv[i] * yv[i];
-            nr = 1.0 / sqrt(nr);
-            const double sg = yv[0] < 0.0 ? -nr : nr;
-            for (int i = 0; i < n; i++) Y[(int64_t)j * n + i] = yv[i] * sg;
-            evals[j] = e;
-            est[j] = fabs(lz.beta[n]) * fabs(Y[(int64_t)j * n + n - 1]);
-            const double eps23 = 3.666852862501036e-11;
-            if (!(est[j] <= tol * fmax(eps23, fabs(e)))) ok = false;
-        }
-        __syncthreads();
-    }
+    const bool ok = ritz_multi_dev(sa, sb, n, mwant, tol, lz.beta[n], evals, Y, est, rs + 2 * n);
     if (threadIdx.x == 0 && !final_pass) {
+        const int m = min(mwant, n);
         if (lz.status[ST_BREAK] || (ok && n >= m && m == mwant) || (ok && n == lz.kmax)) {
             lz.status[ST_CONV] = 1;
             lz.status[ST_DONE] = 1;
