@@ -119,6 +119,49 @@ static void upload_model(dmfted_ctx *c) {
 }
 
 // Kept states of the eigenspace: a device pool of FP64 vectors.
+static cudaEvent_t hv_event(dmfted_ctx *c) {
+    if (!c->hv_ev_free.empty()) {
+        cudaEvent_t e = c->hv_ev_free.back();
+        c->hv_ev_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    DM_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void hv_timer_begin(dmfted_ctx *c) {
+    if (!c->hv_timing) return;
+    cudaEvent_t a = hv_event(c), b = hv_event(c);
+    DM_CUDA(cudaEventRecord(a, c->stream));
+    c->hv_ev.emplace_back(a, b);
+}
+
+void hv_timer_end(dmfted_ctx *c, double bytes) {
+    if (!c->hv_timing || c->hv_ev.size() == c->hv_ev_bytes.size()) return;
+    DM_CUDA(cudaEventRecord(c->hv_ev.back().second, c->stream));
+    c->hv_ev_bytes.push_back(bytes);
+}
+
+// Folds the recorded pairs into the totals (waits for the stream).
+static void hv_timer_collect(dmfted_ctx *c) {
+    if (c->hv_ev.empty()) return;
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < c->hv_ev_bytes.size(); i++) {
+        float ms = 0.f;
+        DM_CUDA(cudaEventElapsedTime(&ms, c->hv_ev[i].first, c->hv_ev[i].second));
+        c->hv_ms += ms;
+        c->hv_bytes += c->hv_ev_bytes[i];
+        c->hv_count++;
+    }
+    for (auto &pr : c->hv_ev) {
+        c->hv_ev_free.push_back(pr.first);
+        c->hv_ev_free.push_back(pr.second);
+    }
+    c->hv_ev.clear();
+    c->hv_ev_bytes.clear();
+}
+
 static void states_reset(dmfted_ctx *c) { c->states.clear(); }
 
 static int64_t state_dim(const dmfted_ctx *c, int isector) {
@@ -630,6 +673,11 @@ int dmfted_free(dmfted_ctx *c) {
     // here rather than left for the next context to trip over
     cudaError_t pending = c->stream ? cudaStreamSynchronize(c->stream) : cudaSuccess;
     cudaStream_t st = c->stream;
+    for (cudaEvent_t e : c->hv_ev_free) cudaEventDestroy(e);
+    for (auto &pr : c->hv_ev) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
     delete c;
     if (st) cudaStreamDestroy(st);
     DM_REQUIRE(pending == cudaSuccess, DMFTED_ERR_CUDA,
@@ -1000,6 +1048,30 @@ int dmfted_time_hxv(dmfted_ctx *c, int32_t flags, int32_t warmup, int32_t reps, 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *ms = t / reps;
+    API_END
+}
+
+int dmfted_hxv_timing(dmfted_ctx *c, int32_t on) {
+    API_BEGIN
+    DM_REQUIRE(c, DMFTED_ERR_ARG, "null argument");
+    DM_CUDA(cudaSetDevice(c->device));
+    hv_timer_collect(c);
+    c->hv_timing = on != 0;
+    c->hv_ms = c->hv_bytes = 0.0;
+    c->hv_count = 0;
+    API_END
+}
+
+int dmfted_get_hxv_timing(dmfted_ctx *c, double *ms, int64_t *launches, double *bytes) {
+    API_BEGIN
+    DM_REQUIRE(c && ms && launches && bytes, DMFTED_ERR_ARG, "null argument");
+    DM_CUDA(cudaSetDevice(c->device));
+    hv_timer_collect(c);
+    *ms = c->hv_ms;
+    *launches = c->hv_count;
+    *bytes = c->hv_bytes;
+    c->hv_ms = c->hv_bytes = 0.0;
+    c->hv_count = 0;
     API_END
 }
 

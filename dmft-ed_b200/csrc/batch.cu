@@ -53,6 +53,7 @@ struct BatchTables {
     const T *dint;
     int64_t poff[kMaxNs + 1];   // padded class offsets
     int64_t binom[kMaxNs + 1];  // class sizes
+    int64_t nrank;              // entries of the rank table (2^Ns)
     int norb, P, W;
 };
 
@@ -79,6 +80,7 @@ static BatchTables<T> batch_tables(const dmfted_ctx *c) {
         b.poff[n] = c->class_poff[n];
         b.binom[n] = c->binom[n];
     }
+    b.nrank = (int64_t)1 << c->ns;
     b.norb = c->norb;
     b.P = c->P;
     b.W = std::max(c->W, 1);
@@ -140,20 +142,24 @@ __device__ void stage_tables(const BatchTables<T> &tb, BatchSmem<T> &sm) {
 // up hops (rows of the same column) and the down hops (same row of the
 // neighbouring columns), as the grid-wide kernel.
 template <typename T>
-__device__ __forceinline__ T hx_elem(const Sec<T> &s, const BatchSmem<T> &sm, int ni,
+__device__ __forceinline__ T hx_elem(const Sec<T> &s, const BatchSmem<T> &sm, int ni, int W, int P,
                                      const T *x, uint32_t r, uint32_t q) {
     const uint32_t imask = (uint32_t)ni - 1u;
     const uint32_t base = s.dimup * q;
     T h = (s.du[r] + s.dd[q] + sm.dint[(s.wu[r] & imask) * ni + (s.wd[q] & imask)]) * x[base + r];
     const int cu = s.cu[r];
     for (int e = 0; e < cu; e++) {
+        if (!DM_IN(e, W)) break;
         const uint32_t en = s.eu[(int64_t)e * s.dimup + r];
+        if (!DM_IN(ell_par(en), P) || !DM_IN(ell_col(en), s.dimup)) continue;
         const T v = sm.pu[ell_par(en)];
         h += (ell_neg(en) ? -v : v) * x[base + ell_col(en)];
     }
     const int cd = s.cd[q];
     for (int e = 0; e < cd; e++) {
+        if (!DM_IN(e, W)) break;
         const uint32_t en = s.ed[(int64_t)e * s.dimdw + q];
+        if (!DM_IN(ell_par(en), P) || !DM_IN(ell_col(en), s.dimdw)) continue;
         const T v = sm.pd[ell_par(en)];
         h += (ell_neg(en) ? -v : v) * x[s.dimup * ell_col(en) + r];
     }
@@ -246,10 +252,17 @@ struct ChainJob {
 constexpr int kChainStride = kLzMax + 2;
 
 // One chain, run by CL CTAs (a cluster) or by one CTA.
+// Extents of the buffers a batched launch writes or gathers from, checked
+// against every job in a checked build (the checks are uniform over the CTAs
+// of a cluster, so a skipped job is skipped by all of them).
+struct BatchCaps {
+    int64_t work, vec, aux, states, slots;
+};
+
 template <typename T, int CL>
 __device__ void chain_job(const BatchTables<T> &tb, BatchSmem<T> &sm, const ChainJob &J,
                           const double *states64, T *work, double *alpha, double *beta,
-                          int *nsteps, double *norm2, double thr) {
+                          int *nsteps, double *norm2, double thr, const BatchCaps &cap) {
     const int ni = 1 << tb.norb;
     const int tid = threadIdx.x, bd = blockDim.x;
     const int rank = cta_rank<CL>();
@@ -258,6 +271,9 @@ __device__ void chain_job(const BatchTables<T> &tb, BatchSmem<T> &sm, const Chai
     const Sec<T> s = make_sec(tb, J.tnup, J.tndw);
     const uint32_t dim = s.dim;
     const uint32_t ld = (dim + 31u) & ~31u;
+    if (!DM_IN(J.work_off + 2 * (int64_t)ld - 1, cap.work) || !DM_IN(J.slot, cap.slots) ||
+        !DM_IN(J.kmax, kChainStride - 1))
+        return;
     T *P = work + J.work_off, *Q = P + ld;
     double *al = alpha + (int64_t)J.slot * kChainStride;
     double *be = beta + (int64_t)J.slot * kChainStride;
@@ -275,7 +291,7 @@ __device__ void chain_job(const BatchTables<T> &tb, BatchSmem<T> &sm, const Chai
         const bool has = (wj & bit) != 0u;
         if (J.particle ? has : !has) {
             const uint32_t w = J.particle ? (wj ^ bit) : (wj | bit);
-            const int64_t rs = tb.rank[w];
+            const int64_t rs = DM_IN(w, tb.nrank) ? tb.rank[w] : 0;
             uint32_t par = __popc(w & (bit - 1u)) & 1u;
             int64_t src;
             if (J.ispin == 0) {
@@ -284,7 +300,7 @@ __device__ void chain_job(const BatchTables<T> &tb, BatchSmem<T> &sm, const Chai
                 par ^= (uint32_t)J.snup & 1u;
                 src = r + sdimup * rs;
             }
-            val = par ? -psi[src] : psi[src];
+            if (DM_IN(J.psi_off + src, cap.states)) val = par ? -psi[src] : psi[src];
         }
         n2[0].add(val * val);
         const T vt = (T)val;
@@ -308,7 +324,7 @@ __device__ void chain_job(const BatchTables<T> &tb, BatchSmem<T> &sm, const Chai
         a[0].zero();
         for (uint32_t i = i0; i < dim; i += st) {
             const uint32_t r = i % s.dimup, q = i / s.dimup;
-            const T h = hx_elem(s, sm, ni, Q, r, q);
+            const T h = hx_elem(s, sm, ni, tb.W, tb.P, Q, r, q);
             const T u = (T)(sc * (double)h - cprev * (double)P[i]);
             P[i] = u;
             a[0].add((double)Q[i] * (double)u);
@@ -353,20 +369,20 @@ template <typename T, int CL>
 __global__ void __launch_bounds__(kBatchThreads, 1)
     k_batch_chains(const BatchTables<T> tb, const ChainJob *jobs, int nbig, int njobs,
                    unsigned *queue, const double *states64, T *work, double *alpha, double *beta,
-                   int *nsteps, double *norm2, double thr) {
+                   int *nsteps, double *norm2, double thr, const BatchCaps cap) {
     __shared__ BatchSmem<T> sm;
     stage_tables(tb, sm);
     if constexpr (CL > 1) {
         for (;;) {
             const int jid = next_job<CL>(queue, sm);
             if (jid >= nbig) break;
-            chain_job<T, CL>(tb, sm, jobs[jid], states64, work, alpha, beta, nsteps, norm2, thr);
+            chain_job<T, CL>(tb, sm, jobs[jid], states64, work, alpha, beta, nsteps, norm2, thr, cap);
         }
     }
     for (;;) {
         const int jid = nbig + next_job<1>(queue + 1, sm);
         if (jid >= njobs) break;
-        chain_job<T, 1>(tb, sm, jobs[jid], states64, work, alpha, beta, nsteps, norm2, thr);
+        chain_job<T, 1>(tb, sm, jobs[jid], states64, work, alpha, beta, nsteps, norm2, thr, cap);
     }
 }
 
@@ -450,7 +466,7 @@ __device__ void reorth_dots(const T *B, uint32_t ld, int nv, const T *y, uint32_
 #pragma unroll
         for (int t = 0; t < kEigsChunk; t++) {
             warp_reduce(d[t]);
-            if (lane == 0 && j0 + t < nv) {
+            if (lane == 0 && j0 + t < nv && DM_IN(2 * ((j0 + t) * nsl + sl) + 1, kDpart)) {
                 dpart[2 * ((j0 + t) * nsl + sl)] = d[t].hi;
                 dpart[2 * ((j0 + t) * nsl + sl) + 1] = d[t].lo;
             }
@@ -505,7 +521,7 @@ __device__ __forceinline__ CSum reorth_update(const T *B, uint32_t ld, int nv, T
 template <typename T, int CL>
 __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn, const EigsJob &J,
                          T *basis_pool, double *vec_pool, double *aux_pool, double *evals,
-                         int *steps_out, double tol, int ncheck) {
+                         int *steps_out, double tol, int ncheck, const BatchCaps &cap) {
     double *sal = dyn, *sbe = sal + (kEigsMaxSteps + 2), *ssc = sbe + (kEigsMaxSteps + 2);
     double *scf = ssc + (kEigsMaxSteps + 2), *dpart = scf + (kEigsMaxSteps + 2);
     double *rwork = dpart + kDpart;
@@ -517,6 +533,12 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
     const Sec<T> s = make_sec(tb, J.nup, J.ndw);
     const uint32_t dim = s.dim;
     const uint32_t ld = (dim + 31u) & ~31u;
+    if (!DM_IN(J.basis_off + (int64_t)(J.kmax + 1) * ld - 1, cap.work) ||
+        !DM_IN(J.vec_off + (int64_t)J.neigen * dim - 1, cap.vec) ||
+        !DM_IN(J.aux_off + (rank + 1) * eigs_aux_per_cta(J.neigen, J.kmax) - 1, cap.aux) ||
+        !DM_IN(J.slot, cap.slots) || !DM_IN(J.kmax, kEigsMaxSteps + 1) ||
+        !DM_IN(J.neigen, kEigsMaxEigen + 1))
+        return;
     T *B = basis_pool + J.basis_off;
     // private Ritz scratch of this CTA: Y, coefficients, eigenvalues
     const int64_t nk = (int64_t)J.neigen * J.kmax;
@@ -548,7 +570,7 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
         a1[0].zero();
         for (uint32_t i = i0; i < dim; i += st) {
             const uint32_t r = i % s.dimup, q = i / s.dimup;
-            const T h = hx_elem(s, sm, ni, x, r, q);
+            const T h = hx_elem(s, sm, ni, tb.W, tb.P, x, r, q);
             const T u = (T)(sc * (double)h - cprev * (double)xp[i]);
             y[i] = u;
             a1[0].add((double)x[i] * (double)u);
@@ -646,7 +668,7 @@ template <typename T, int CL>
 __global__ void __launch_bounds__(kBatchThreads, 1)
     k_batch_eigs(const BatchTables<T> tb, const EigsJob *jobs, int nbig, int njobs,
                  unsigned *queue, T *basis_pool, double *vec_pool, double *aux_pool,
-                 double *evals, int *steps_out, double tol, int ncheck) {
+                 double *evals, int *steps_out, double tol, int ncheck, const BatchCaps cap) {
     __shared__ BatchSmem<T> sm;
     extern __shared__ double dyn[];
     stage_tables(tb, sm);
@@ -655,14 +677,14 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
             const int jid = next_job<CL>(queue, sm);
             if (jid >= nbig) break;
             eigs_job<T, CL>(tb, sm, dyn, jobs[jid], basis_pool, vec_pool, aux_pool, evals,
-                            steps_out, tol, ncheck);
+                            steps_out, tol, ncheck, cap);
         }
     }
     for (;;) {
         const int jid = nbig + next_job<1>(queue + 1, sm);
         if (jid >= njobs) break;
         eigs_job<T, 1>(tb, sm, dyn, jobs[jid], basis_pool, vec_pool, aux_pool, evals, steps_out,
-                       tol, ncheck);
+                       tol, ncheck, cap);
     }
 }
 
@@ -812,7 +834,10 @@ static void run_batch_eigs(dmfted_ctx *c, int j0, int nbig, int j1, int wave, do
                       batch_tables<T>(c), reinterpret_cast<const EigsJob *>(c->bjobs.p) + j0, nbig,
                       j1 - j0, reinterpret_cast<unsigned *>(c->bint.p) + 2 * wave,
                       reinterpret_cast<T *>(c->bwork.p), c->bvec.p, c->baux.p, c->bscal.p,
-                      c->bint.p + 2 * kMaxWaves, tol, std::max(1, c->p.lanc_ncheck));
+                      c->bint.p + 2 * kMaxWaves, tol, std::max(1, c->p.lanc_ncheck),
+                      BatchCaps{(int64_t)(c->bwork.n / sizeof(T)), (int64_t)c->bvec.n,
+                                (int64_t)c->baux.n, 0,
+                                (int64_t)(c->bscal.n / kEigsMaxEigen)});
 }
 
 template <typename T>
@@ -940,17 +965,20 @@ void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, int precision,
 
 template <typename T, int CL>
 static void run_batch_chains(dmfted_ctx *c, int nbig, int nj, double *alpha, double *beta,
-                             int *nsteps, double *norm2) {
+                             int *nsteps, double *norm2, int64_t nslots) {
     launch_persistent(c, k_batch_chains<T, CL>, CL, nbig + div_up(nj - nbig, CL), 0,
                       batch_tables<T>(c), reinterpret_cast<const ChainJob *>(c->bjobs.p), nbig, nj,
                       reinterpret_cast<unsigned *>(c->bint.p), (const double *)c->states64.p,
                       reinterpret_cast<T *>(c->bwork.p), alpha, beta, nsteps, norm2,
-                      c->p.lanc_gf_threshold);
+                      c->p.lanc_gf_threshold,
+                      BatchCaps{(int64_t)(c->bwork.n / sizeof(T)), 0, 0, (int64_t)c->states64.n,
+                                nslots});
 }
 
 template <typename T>
 static void run_batch_chains_cl(dmfted_ctx *c, int CL, const std::vector<ChainJob> &jobs,
-                                double *alpha, double *beta, int *nsteps, double *norm2) {
+                                double *alpha, double *beta, int *nsteps, double *norm2,
+                                int64_t nslots) {
     const int nj = (int)jobs.size();
     DM_CUDA(cudaMemcpyAsync(c->bjobs.p, jobs.data(), nj * sizeof(ChainJob), cudaMemcpyHostToDevice,
                             c->stream));
@@ -960,10 +988,10 @@ static void run_batch_chains_cl(dmfted_ctx *c, int CL, const std::vector<ChainJo
            c->binom[jobs[nbig].tnup] * c->binom[jobs[nbig].tndw] >= c->batch_cluster_min * CL)
         nbig++;
     switch (CL) {
-        case 8: run_batch_chains<T, 8>(c, nbig, nj, alpha, beta, nsteps, norm2); break;
-        case 4: run_batch_chains<T, 4>(c, nbig, nj, alpha, beta, nsteps, norm2); break;
-        case 2: run_batch_chains<T, 2>(c, nbig, nj, alpha, beta, nsteps, norm2); break;
-        default: run_batch_chains<T, 1>(c, 0, nj, alpha, beta, nsteps, norm2); break;
+        case 8: run_batch_chains<T, 8>(c, nbig, nj, alpha, beta, nsteps, norm2, nslots); break;
+        case 4: run_batch_chains<T, 4>(c, nbig, nj, alpha, beta, nsteps, norm2, nslots); break;
+        case 2: run_batch_chains<T, 2>(c, nbig, nj, alpha, beta, nsteps, norm2, nslots); break;
+        default: run_batch_chains<T, 1>(c, 0, nj, alpha, beta, nsteps, norm2, nslots); break;
     }
 }
 
@@ -1014,8 +1042,8 @@ void batch_chains_gf(dmfted_ctx *c, const std::vector<ChainRec> &recs, int preci
         for (const ChainJob &J : jobs)
             dmax = std::max<int64_t>(dmax, c->binom[J.tnup] * c->binom[J.tndw]);
         const int CL = chain_cluster(c, (int)jobs.size(), dmax);
-        if (fp64) run_batch_chains_cl<double>(c, CL, jobs, alpha, beta, nsteps, norm2);
-        else run_batch_chains_cl<float>(c, CL, jobs, alpha, beta, nsteps, norm2);
+        if (fp64) run_batch_chains_cl<double>(c, CL, jobs, alpha, beta, nsteps, norm2, nrec);
+        else run_batch_chains_cl<float>(c, CL, jobs, alpha, beta, nsteps, norm2, nrec);
     }
     // chains too large for one CTA: the grid-wide recurrence, in order
     for (int i = 0; i < nrec; i++) {

@@ -12,26 +12,42 @@
 // is sum_i C(c_i, i) over the set-bit positions c_1 < ... < c_n.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "internal.cuh"
 
 namespace dmfted {
 
-__constant__ int64_t c_binom[(kMaxNs + 1) * (kMaxNs + 1)];  // C(b, i) at b*(kMaxNs+1)+i
-__constant__ int64_t c_class_off[kMaxNs + 2];   // compact offsets (enumeration)
-__constant__ int64_t c_class_poff[kMaxNs + 2];  // padded storage offsets (32-element aligned)
+// C(b, i) at b*(kMaxNs+1)+i for every b <= kMaxNs.  Constant memory is shared
+// by every context of the process; this table is the same for all of them.
+__constant__ int64_t c_binom[(kMaxNs + 1) * (kMaxNs + 1)];
+
+// Class offsets of one context (they depend on Ns), passed by value.
+struct ClassTab {
+    int64_t off[kMaxNs + 2];   // compact offsets (enumeration)
+    int64_t poff[kMaxNs + 2];  // padded storage offsets (32-element aligned)
+};
+
+static ClassTab class_tab(const dmfted_ctx *c) {
+    ClassTab t{};
+    for (int n = 0; n < kMaxNs + 2; n++) {
+        t.off[n] = c->class_off[n];
+        t.poff[n] = c->class_poff[n];
+    }
+    return t;
+}
 
 __device__ __forceinline__ int64_t binom_d(int b, int i) {
     return (i < 0 || b < 0 || i > b) ? 0 : c_binom[b * (kMaxNs + 1) + i];
 }
 
 // K1a: words[g] for every g in [0, 2^Ns) and the rank table.
-__global__ void k_words(int ns, uint32_t *words, int32_t *rank) {
+__global__ void k_words(int ns, const ClassTab ct, uint32_t *words, int32_t *rank) {
     int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (g >= ((int64_t)1 << ns)) return;
     int n = 0;
-    while (c_class_off[n + 1] <= g) n++;
-    int64_t r = g - c_class_off[n];
+    while (ct.off[n + 1] <= g) n++;
+    int64_t r = g - ct.off[n];
     int64_t rr = r;
     uint32_t w = 0;
     int b = ns - 1;
@@ -41,7 +57,7 @@ __global__ void k_words(int ns, uint32_t *words, int32_t *rank) {
         rr -= binom_d(b, i);
         b--;
     }
-    words[c_class_poff[n] + r] = w;
+    words[ct.poff[n] + r] = w;
     rank[w] = (int32_t)r;
 }
 
@@ -63,15 +79,16 @@ __device__ __forceinline__ uint32_t between_parity(uint32_t w, int p, int q) {
 // ED_SETUP.f90:1055-1081 (levels below the lower position cancel).
 // Also writes the bath-energy part of the diagonal, sum_k e_k n_k
 // (HxVbath.f90:1-13).
-__global__ void k_ell_build(int ns, int norb, int nbath, int W, const uint32_t *words,
-                            const int32_t *rank, const double *par, const double *ebath,
-                            uint8_t *cnt, uint32_t *ell, double *diag, float *diag_f) {
+__global__ void k_ell_build(int ns, const ClassTab ct, int norb, int nbath, int W,
+                            const uint32_t *words, const int32_t *rank, const double *par,
+                            const double *ebath, uint8_t *cnt, uint32_t *ell, double *diag,
+                            float *diag_f) {
     int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (g >= ((int64_t)1 << ns)) return;
     int n = 0;
-    while (c_class_off[n + 1] <= g) n++;
-    const int64_t r = g - c_class_off[n];
-    const int64_t off = c_class_poff[n];
+    while (ct.off[n + 1] <= g) n++;
+    const int64_t r = g - ct.off[n];
+    const int64_t off = ct.poff[n];
     const int64_t rows = binom_d(ns, n);
     uint32_t *erow = ell + (int64_t)W * off + r;
     const int64_t gs = off + r;  // storage index
@@ -121,14 +138,14 @@ __global__ void k_ell_build(int ns, int norb, int nbath, int W, const uint32_t *
 // slot, putting on every row the hop whose target quad is least used so far in
 // that slot.  Balanced quads mean fewer shared-memory wavefronts per gather;
 // the set of hops of a row is unchanged.  One thread per group.
-__global__ void k_ell_balance(int ns, int n, int W, int vw, const uint8_t *cnt, uint32_t *ell) {
+__global__ void k_ell_balance(int ns, int n, int64_t off, int W, int vw, const uint8_t *cnt,
+                              uint32_t *ell) {
     const int64_t rows = binom_d(ns, n);
     const int64_t span = vw == 2 ? 64 : 32;
     const int64_t ngroups = ((rows + span - 1) / span) * vw;
     const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (g >= ngroups) return;
     const int64_t blk = g / vw, par = g % vw;
-    const int64_t off = c_class_poff[n];
     uint32_t *e = ell + (int64_t)W * off;
     int load[kMaxW][8];
     const int wmax = W < kMaxW ? W : kMaxW;
@@ -190,20 +207,24 @@ void fock_init(dmfted_ctx *c) {
         c->class_poff[n + 1] = c->class_poff[n] + (cn + 31) / 32 * 32;
     }
     // classes beyond ns are empty; keep offsets monotone so the class search stops
-    DM_CUDA(cudaMemcpyToSymbolAsync(c_binom, bt.data(), bt.size() * sizeof(int64_t), 0,
-                                    cudaMemcpyHostToDevice, c->stream));
-    DM_CUDA(cudaMemcpyToSymbolAsync(c_class_off, c->class_off.data(),
-                                    c->class_off.size() * sizeof(int64_t), 0,
-                                    cudaMemcpyHostToDevice, c->stream));
-    DM_CUDA(cudaMemcpyToSymbolAsync(c_class_poff, c->class_poff.data(),
-                                    c->class_poff.size() * sizeof(int64_t), 0,
-                                    cudaMemcpyHostToDevice, c->stream));
+    {
+        // once per device: the table is the same for every context, and other
+        // contexts' kernels may be reading it
+        static std::mutex mu;
+        static bool loaded[64] = {false};
+        std::lock_guard<std::mutex> lk(mu);
+        if (!loaded[c->device & 63]) {
+            DM_CUDA(cudaMemcpyToSymbol(c_binom, bt.data(), bt.size() * sizeof(int64_t)));
+            loaded[c->device & 63] = true;
+        }
+    }
     c->nwords = (int64_t)1 << ns;
     c->nstore = c->class_poff[kMaxNs + 1];
     c->words.alloc(c->nstore);
     DM_CUDA(cudaMemsetAsync(c->words.p, 0, c->nstore * sizeof(uint32_t), c->stream));
     c->rank.alloc(c->nwords);
-    k_words<<<div_up(c->nwords, 256), 256, 0, c->stream>>>(ns, c->words.p, c->rank.p);
+    k_words<<<div_up(c->nwords, 256), 256, 0, c->stream>>>(ns, class_tab(c), c->words.p,
+                                                            c->rank.p);
     DM_CHECK_LAUNCH();
     c->launches++;
     c->W = c->norb * c->nbath + c->norb * (c->norb - 1);
@@ -299,16 +320,16 @@ void fock_set_couplings(dmfted_ctx *c) {
         DM_CUDA(cudaMemcpyAsync(d_eb.p, eb.data(), eb.size() * sizeof(double), cudaMemcpyHostToDevice,
                                 c->stream));
         k_ell_build<<<div_up(c->nwords, 256), 256, 0, c->stream>>>(
-            c->ns, norb, nbath, std::max(c->W, 1), c->words.p, c->rank.p, t.par.p, d_eb.p, t.cnt.p,
-            t.ell.p, t.diag.p, t.diag_f.p);
+            c->ns, class_tab(c), norb, nbath, std::max(c->W, 1), c->words.p, c->rank.p, t.par.p,
+            d_eb.p, t.cnt.p, t.ell.p, t.diag.p, t.diag_f.p);
         DM_CHECK_LAUNCH();
         c->launches++;
         // gather grouping of the H*v: two rows per thread for even class sizes
         for (int n = 0; n <= c->ns; n++) {
             const int vw = (c->binom[n] % 2 == 0) ? 2 : 1;
             const int64_t ng = ((c->binom[n] + (vw == 2 ? 63 : 31)) / (vw == 2 ? 64 : 32)) * vw;
-            k_ell_balance<<<div_up(ng, 64), 64, 0, c->stream>>>(c->ns, n, std::max(c->W, 1), vw,
-                                                                t.cnt.p, t.ell.p);
+            k_ell_balance<<<div_up(ng, 64), 64, 0, c->stream>>>(
+                c->ns, n, c->class_poff[n], std::max(c->W, 1), vw, t.cnt.p, t.ell.p);
             DM_CHECK_LAUNCH();
             c->launches++;
         }

@@ -387,8 +387,12 @@ static void launch_nc(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int n
 template <typename T, bool LZ>
 static void launch_hxv(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
     constexpr int NCT = 16 / sizeof(T);
+    // algorithmic bytes: read x (and v_prev for the Lanczos step), write y
+    const double bytes = (LZ ? 3.0 : 2.0) * (double)a.dimup * a.dimdw * a.nstack * nvec * sizeof(T);
+    hv_timer_begin(c);
     if (g.vw == 2) launch_nc<T, NCT, 2, LZ>(c, a, g, nvec);
     else launch_nc<T, NCT, 1, LZ>(c, a, g, nvec);
+    hv_timer_end(c, bytes);
 }
 
 template <typename T>

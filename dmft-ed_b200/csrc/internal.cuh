@@ -69,13 +69,13 @@ const char *last_error();
 // bad launch shows where it went wrong instead of faulting.  Compiles to
 // `true` in the normal build.
 #ifdef DMFTED_DEVICE_CHECKS
-__device__ __forceinline__ bool dm_in(int64_t i, int64_t n, int line) {
+__device__ __forceinline__ bool dm_in(int64_t i, int64_t n, const char *file, int line) {
     if (i >= 0 && i < n) return true;
-    printf("dmfted device check failed: line %d block %d thread %d index %lld extent %lld\n", line,
-           (int)blockIdx.x, (int)threadIdx.x, (long long)i, (long long)n);
+    printf("dmfted device check failed: %s:%d block %d thread %d index %lld extent %lld\n", file,
+           line, (int)blockIdx.x, (int)threadIdx.x, (long long)i, (long long)n);
     return false;
 }
-#define DM_IN(i, n) ::dmfted::dm_in((int64_t)(i), (int64_t)(n), __LINE__)
+#define DM_IN(i, n) ::dmfted::dm_in((int64_t)(i), (int64_t)(n), __FILE__, __LINE__)
 #else
 #define DM_IN(i, n) true
 #endif
@@ -227,6 +227,13 @@ struct dmfted_ctx {
     dmfted::DBuf<int> bint;               // queue counter, step counts
     dmfted::DBuf<double> bcf;             // continued-fraction terms (chain x frequency)
     int64_t launches = 0;
+    // live timing of the H*v launches (dmfted_hxv_timing)
+    bool hv_timing = false;
+    std::vector<cudaEvent_t> hv_ev_free;              // recycled events
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> hv_ev;  // pairs not yet read
+    std::vector<double> hv_ev_bytes;
+    double hv_ms = 0.0, hv_bytes = 0.0;
+    int64_t hv_count = 0;
     // results of the last solve (device and host)
     struct State {
         double e;
@@ -247,6 +254,11 @@ struct dmfted_ctx {
 };
 
 namespace dmfted {
+
+// ---- api.cu --------------------------------------------------------------
+// Event pair around one H*v launch when live timing is on.
+void hv_timer_begin(dmfted_ctx *c);
+void hv_timer_end(dmfted_ctx *c, double bytes);
 
 // ---- fock.cu -------------------------------------------------------------
 void fock_init(dmfted_ctx *c);              // words, rank, class offsets

@@ -95,6 +95,8 @@ EXPORTS = {
     "dmfted_chi2_delta_batch_device": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, _vp,
                                                  _vp, _vp, _vp, _vp]),
     "dmfted_time_hxv": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp]),
+    "dmfted_hxv_timing": (C.c_int, [_vp, C.c_int32]),
+    "dmfted_get_hxv_timing": (C.c_int, [_vp, _dp, _lp, _dp]),
     "dmfted_get_timings": (C.c_int, [_vp, _dp, _lp]),
     "dmfted_launch_count": (C.c_int, [_vp, _lp, C.c_int32]),
 }
@@ -355,6 +357,15 @@ class EDSolver:
         _ck(lib().dmfted_get_timings(self.ctx, _p(t), _p(n, C.c_int64)))
         return dict(diag_ms=t[0], obs_ms=t[1], gf_ms=t[2], total_ms=t[3], hv_diag=int(n[0]),
                     hv_obs=int(n[1]), hv_gf=int(n[2]))
+
+    def hxv_timing(self, on=True):
+        """Record device time and algorithmic bytes of every H*v launch."""
+        _ck(lib().dmfted_hxv_timing(self.ctx, int(on)))
+
+    def hxv_timing_totals(self):
+        ms, n, b = C.c_double(), C.c_int64(), C.c_double()
+        _ck(lib().dmfted_get_hxv_timing(self.ctx, C.byref(ms), C.byref(n), C.byref(b)))
+        return dict(ms=ms.value, launches=n.value, bytes=b.value)
 
     def launch_count(self, reset=False):
         n = C.c_int64()

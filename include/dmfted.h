@@ -241,6 +241,17 @@ int dmfted_chi2_delta_batch_device(dmfted_ctx *ctx, int32_t nbatch, int32_t nbat
  * DimDw even).  The vectors are the context's own work buffers. */
 int dmfted_time_hxv(dmfted_ctx *ctx, int32_t flags, int32_t warmup, int32_t reps, double *ms);
 
+/* Live timing of the H*v launches (plain products and fused Lanczos steps)
+ * of everything that runs on the context from now on: on != 0 records a CUDA
+ * event pair on the context's stream around each launch.  Resets the totals.
+ * No counterpart in the reference (measurement support). */
+int dmfted_hxv_timing(dmfted_ctx *ctx, int32_t on);
+
+/* Totals of the timed H*v launches since the last call (then reset): device
+ * milliseconds, launch count and algorithmic bytes (read x, read v_prev for
+ * the fused step, write y, at the vector precision).  Waits for the stream. */
+int dmfted_get_hxv_timing(dmfted_ctx *ctx, double *ms, int64_t *launches, double *bytes);
+
 /* Device milliseconds of the last dmfted_ed_solve, split into phases:
  * t[0]=diagonalisation, t[1]=observables, t[2]=Green's functions,
  * t[3]=total; and the H*v products each phase used in n[0..2]. */
