@@ -295,7 +295,7 @@ def run_ours(args, rank, world, local_rank):
     hv32 = s.time_hxv(fp32=True, warmup=5, reps=50)
     hv64 = s.time_hxv(fp32=False, warmup=5, reps=50)
     extra = {}
-    if world == 1:
+    if world == 1 and args.only == "all":
         extra["finite_t_batched"] = finite_t_workload(dmfted, local_rank, args.steps, args.warmup)
         extra["differentiation"] = differentiation_workload(
             dmfted, local_rank, args.steps, args.warmup, solvers[dmfted.FP64], isec, bath)
@@ -366,6 +366,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", default="all",
+                    choices=["all", "headline", "finite_t", "differentiation"],
+                    help="run one workload (profiling); the default prints the full line")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -409,6 +412,21 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     import dmfted
+    if args.only in ("finite_t", "differentiation"):
+        # one secondary workload alone, for profiling; rank 0 prints it
+        import torch
+        torch.cuda.set_device(local_rank)
+        if args.only == "finite_t":
+            out = finite_t_workload(dmfted, local_rank, args.steps, args.warmup)
+        else:
+            s64 = make_solver(dmfted, dmfted.FP64, local_rank)
+            out = differentiation_workload(dmfted, local_rank, args.steps, args.warmup, s64,
+                                           s64.sector_index(NUP, NDW), seeded_bath())
+            out.pop("chi2_host")
+            s64.close()
+        if rank == 0:
+            print(json.dumps({args.only: out}))
+        return
     res, dim, hv32, hv64, extra = run_ours(args, rank, world, local_rank)
     mixed, fp64 = res[dmfted.MIXED], res[dmfted.FP64]
     t_mixed = max_over_ranks(sum(mixed["ms"]) / 1e3, world)

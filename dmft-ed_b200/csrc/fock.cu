@@ -78,11 +78,12 @@ __device__ __forceinline__ uint32_t between_parity(uint32_t w, int p, int q) {
 // levels strictly between p and q), the product of the two c/cdg signs of
 // ED_SETUP.f90:1055-1081 (levels below the lower position cancel).
 // Also writes the bath-energy part of the diagonal, sum_k e_k n_k
-// (HxVbath.f90:1-13).
+// (HxVbath.f90:1-13); with write_ell == 0 only the diagonal (the table depends
+// on which couplings are non-zero, not on their values).
 __global__ void k_ell_build(int ns, const ClassTab ct, int norb, int nbath, int W,
                             const uint32_t *words, const int32_t *rank, const double *par,
                             const double *ebath, uint8_t *cnt, uint32_t *ell, double *diag,
-                            float *diag_f) {
+                            float *diag_f, int write_ell) {
     int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (g >= ((int64_t)1 << ns)) return;
     int n = 0;
@@ -95,6 +96,7 @@ __global__ void k_ell_build(int ns, const ClassTab ct, int norb, int nbath, int 
     const uint32_t w = words[gs];
     int e = 0;
     const int pv = norb * nbath;
+    if (write_ell) {
     for (int a = 0; a < norb; a++)
         for (int b = 0; b < norb; b++) {
             if (a == b) continue;
@@ -119,6 +121,7 @@ __global__ void k_ell_build(int ns, const ClassTab ct, int norb, int nbath, int 
             }
         }
     cnt[gs] = (uint8_t)e;
+    }
     double d = 0.0;
     for (int a = 0; a < norb; a++)
         for (int k = 0; k < nbath; k++) {
@@ -297,12 +300,11 @@ void fock_set_couplings(dmfted_ctx *c) {
     for (int s = 0; s < nsp_tab; s++) {
         // spin s of the tables uses bath spin index s (0 -> ispin=1, 1 -> ispin=Nspin)
         const int bs = (s == 0) ? 0 : nsp - 1;
-        std::vector<double> par(c->P, 0.0), eb((size_t)norb * nbath, 0.0);
+        std::vector<double> par(c->P, 0.0);
         std::vector<float> parf(c->P, 0.f);
         for (int a = 0; a < norb; a++)
             for (int k = 0; k < nbath; k++) {
                 par[a * nbath + k] = c->bath_v[((size_t)bs * norb + a) * nbath + k];
-                eb[a * nbath + k] = c->bath_e[((size_t)bs * norb + a) * nbath + k];
             }
         for (int a = 0; a < norb; a++)
             for (int b = 0; b < norb; b++) {
@@ -315,17 +317,19 @@ void fock_set_couplings(dmfted_ctx *c) {
                                 c->stream));
         DM_CUDA(cudaMemcpyAsync(t.par_f.p, parf.data(), c->P * sizeof(float), cudaMemcpyHostToDevice,
                                 c->stream));
-        DBuf<double> d_eb;
-        d_eb.alloc(std::max<size_t>(eb.size(), 1));
-        DM_CUDA(cudaMemcpyAsync(d_eb.p, eb.data(), eb.size() * sizeof(double), cudaMemcpyHostToDevice,
-                                c->stream));
+        // the table holds targets, signs and coupling indices; it changes only
+        // when the set of non-zero couplings does
+        std::vector<uint8_t> pattern(par.size());
+        for (size_t q = 0; q < par.size(); q++) pattern[q] = par[q] != 0.0;
+        const bool rebuild = pattern != c->ell_pattern[s];
+        const double *d_eb = c->d_bath_e.p + (size_t)bs * norb * nbath;  // [norb][nbath] of spin bs
         k_ell_build<<<div_up(c->nwords, 256), 256, 0, c->stream>>>(
             c->ns, class_tab(c), norb, nbath, std::max(c->W, 1), c->words.p, c->rank.p, t.par.p,
-            d_eb.p, t.cnt.p, t.ell.p, t.diag.p, t.diag_f.p);
+            d_eb, t.cnt.p, t.ell.p, t.diag.p, t.diag_f.p, rebuild ? 1 : 0);
         DM_CHECK_LAUNCH();
         c->launches++;
         // gather grouping of the H*v: two rows per thread for even class sizes
-        for (int n = 0; n <= c->ns; n++) {
+        for (int n = 0; rebuild && n <= c->ns; n++) {
             const int vw = (c->binom[n] % 2 == 0) ? 2 : 1;
             const int64_t ng = ((c->binom[n] + (vw == 2 ? 63 : 31)) / (vw == 2 ? 64 : 32)) * vw;
             k_ell_balance<<<div_up(ng, 64), 64, 0, c->stream>>>(
@@ -333,8 +337,7 @@ void fock_set_couplings(dmfted_ctx *c) {
             DM_CHECK_LAUNCH();
             c->launches++;
         }
-        DM_CUDA(cudaStreamSynchronize(c->stream));
-        d_eb.release();
+        c->ell_pattern[s] = pattern;
     }
     const int ni = 1 << norb;
     std::vector<double> di(ni * ni);

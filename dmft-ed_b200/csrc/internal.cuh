@@ -189,6 +189,7 @@ struct dmfted_ctx {
     dmfted::DBuf<int32_t> rank;
     dmfted::DBuf<int64_t> d_class_off;
     dmfted::SpinTables spin[2];
+    std::vector<uint8_t> ell_pattern[2];  // non-zero couplings the tables were built for
     bool spin_shared = true;  // Nspin == 1: down tables alias the up tables
     dmfted::DBuf<double> dint;  // [(1<<norb)^2] impurity-only diagonal
     dmfted::DBuf<float> dint_f;

@@ -42,3 +42,20 @@ def test_interleaved_contexts_of_different_ns():
     assert abs(b2.egs() - e_b) <= 1e-12 * abs(e_b)
     b2.close()
     a.close()
+
+
+def test_bath_updates_with_and_without_zero_couplings():
+    # the hopping tables depend on which couplings are non-zero: a bath with a
+    # zero V_k removes those hops, the next bath without one restores them
+    m = O.seeded_model(33, nbath=7, u=2.0)
+    s = dmfted.EDSolver(params_for(m))
+    isec = s.sector_index(4, 4)
+    hm = O.build_sector(m.ns, 4, 4)
+    for zero in (None, 2, None, 5, 5, None):
+        mk = O.seeded_model(33, nbath=7, u=2.0)
+        if zero is not None:
+            mk.v[:, :, zero] = 0.0
+        s.ed_solve(mk.bath_array(), sectors=[isec])
+        e0, _, _ = O.lanczos_gs(mk, hm)
+        assert abs(s.egs() - e0) <= 1e-10 * abs(e0), zero
+    s.close()
