@@ -608,6 +608,8 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         c->ns = ns;
         c->device = p->device;
         if (const char *e = getenv("DMFTED_HXV_NC")) c->tune_nc = atoi(e);
+        if (const char *e = getenv("DMFTED_HXV_KERNEL")) c->tune_hxv = atoi(e);
+        if (const char *e = getenv("DMFTED_ELL_GROUP")) c->tune_ell_group = std::max(1, std::min(32, atoi(e)));
         if (const char *e = getenv("DMFTED_MIXED_TOL32")) c->mixed_tol32 = atof(e);
         if (const char *e = getenv("DMFTED_BATCH_MAX_DIM")) c->batch_max_dim = atoll(e);
         if (const char *e = getenv("DMFTED_BATCH_BUDGET_MB")) c->batch_budget = atoll(e) << 20;

@@ -136,13 +136,16 @@ __global__ void k_ell_build(int ns, const ClassTab ct, int norb, int nbath, int 
 // hops are gathers of 16-byte rows of the staged tile; row t sits in shared-
 // memory bank quad t % 8, and one warp-wide gather serves the rows of one
 // group: 64 consecutive rows split by parity when a thread owns two rows
-// (vw == 2), 32 consecutive rows otherwise.  Which slot of a row's list holds
-// which hop is free, so each group reorders its rows' entries greedily, slot by
-// slot, putting on every row the hop whose target quad is least used so far in
-// that slot.  Balanced quads mean fewer shared-memory wavefronts per gather;
-// the set of hops of a row is unchanged.  One thread per group.
-__global__ void k_ell_balance(int ns, int n, int64_t off, int W, int vw, const uint8_t *cnt,
-                              uint32_t *ell) {
+// (vw == 2), 32 consecutive rows otherwise.  A 16-byte shared-memory access is
+// served a quarter warp (8 lanes, 128 bytes) per wavefront, so the balance is
+// kept within each run of `gsize` lanes (8: a quarter warp).  Which slot of a
+// row's list holds which hop is free, so each group reorders its rows' entries
+// greedily, slot by slot, putting on every row the hop whose target quad is
+// least used so far in that slot.  Balanced quads mean fewer shared-memory
+// wavefronts per gather; the set of hops of a row is unchanged.  One thread
+// per group of 32 lanes.
+__global__ void k_ell_balance(int ns, int n, int64_t off, int W, int vw, int gsize,
+                              const uint8_t *cnt, uint32_t *ell) {
     const int64_t rows = binom_d(ns, n);
     const int64_t span = vw == 2 ? 64 : 32;
     const int64_t ngroups = ((rows + span - 1) / span) * vw;
@@ -157,6 +160,9 @@ __global__ void k_ell_balance(int ns, int n, int64_t off, int W, int vw, const u
     for (int l = 0; l < 32; l++) {
         const int64_t r = blk * span + (int64_t)l * vw + par;
         if (r >= rows) break;
+        if (l % gsize == 0)
+            for (int q = 0; q < wmax; q++)
+                for (int b = 0; b < 8; b++) load[q][b] = 0;
         const int c = cnt[off + r];
         // selection sort of this row's entries by current quad load, slot by slot
         for (int q = 0; q < c; q++) {
@@ -175,6 +181,29 @@ __global__ void k_ell_balance(int ns, int n, int64_t off, int W, int vw, const u
             }
             load[q][ell_col(e[(int64_t)q * rows + r]) & 7u]++;
         }
+    }
+}
+
+// Lean gather table of one class from its balanced ELL table (same slot
+// order): hop e of row r becomes (target row * 16) | (2 * coupling + sign) << 24;
+// slots at or beyond the row's hop count become zero-coupling entries that
+// point at the row itself (conflict-free: the rows of a quarter warp sit in
+// distinct bank quads).
+__global__ void k_ellx_build(int64_t rows, int64_t off, int W, int WX, const uint8_t *cnt,
+                             const uint32_t *ell, uint32_t *ellx) {
+    const int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    const int c = cnt[off + r];
+    const uint32_t *src = ell + (int64_t)W * off + r;
+    uint32_t *dst = ellx + (int64_t)WX * off + r;
+    for (int e = 0; e < WX; e++) {
+        uint32_t v = ((uint32_t)r << 4) | (255u << 24);
+        if (e < c && e < W) {
+            const uint32_t h = src[(int64_t)e * rows];
+            const uint32_t sidx = ell_par(h) * 2u + (ell_neg(h) ? 1u : 0u);
+            v = (ell_col(h) << 4) | ((sidx < 255u ? sidx : 255u) << 24);
+        }
+        dst[(int64_t)e * rows] = v;
     }
 }
 
@@ -234,12 +263,14 @@ void fock_init(dmfted_ctx *c) {
     c->P = c->norb * c->nbath + c->norb * c->norb;
     DM_REQUIRE(c->W <= kMaxW && c->P <= kMaxParams, DMFTED_ERR_UNSUPPORTED,
                "too many couplings per level for the packed hopping table");
+    c->WX = std::max(c->W, 8);
     c->spin_shared = (c->nspin == 1);
     const int nsp = c->spin_shared ? 1 : 2;
     for (int s = 0; s < nsp; s++) {
         SpinTables &t = c->spin[s];
         t.cnt.alloc(c->nstore);
         t.ell.alloc((size_t)std::max(c->W, 1) * c->nstore);
+        t.ellx.alloc((size_t)c->WX * c->nstore);
         t.diag.alloc(c->nstore);
         t.diag_f.alloc(c->nstore);
         DM_CUDA(cudaMemsetAsync(t.cnt.p, 0, c->nstore, c->stream));
@@ -333,9 +364,28 @@ void fock_set_couplings(dmfted_ctx *c) {
             const int vw = (c->binom[n] % 2 == 0) ? 2 : 1;
             const int64_t ng = ((c->binom[n] + (vw == 2 ? 63 : 31)) / (vw == 2 ? 64 : 32)) * vw;
             k_ell_balance<<<div_up(ng, 64), 64, 0, c->stream>>>(
-                c->ns, n, c->class_poff[n], std::max(c->W, 1), vw, t.cnt.p, t.ell.p);
+                c->ns, n, c->class_poff[n], std::max(c->W, 1), vw,
+                c->tune_ell_group > 0 ? c->tune_ell_group : 8, t.cnt.p, t.ell.p);
             DM_CHECK_LAUNCH();
             c->launches++;
+        }
+        if (rebuild) {
+            for (int n = 0; n <= c->ns; n++) {
+                k_ellx_build<<<div_up(c->binom[n], 256), 256, 0, c->stream>>>(
+                    c->binom[n], c->class_poff[n], std::max(c->W, 1), c->WX, t.cnt.p, t.ell.p,
+                    t.ellx.p);
+                DM_CHECK_LAUNCH();
+                c->launches++;
+            }
+            // most hops per word of each class (picks the lean H*v's hop counts)
+            std::vector<uint8_t> hc(c->nstore);
+            DM_CUDA(cudaMemcpyAsync(hc.data(), t.cnt.p, c->nstore, cudaMemcpyDeviceToHost,
+                                    c->stream));
+            DM_CUDA(cudaStreamSynchronize(c->stream));
+            t.cls_max.assign(c->ns + 1, 0);
+            for (int n = 0; n <= c->ns; n++)
+                for (int64_t r = 0; r < c->binom[n]; r++)
+                    t.cls_max[n] = std::max<int>(t.cls_max[n], hc[c->class_poff[n] + r]);
         }
         c->ell_pattern[s] = pattern;
     }

@@ -85,6 +85,32 @@ __device__ __forceinline__ void vst_cs(E *p, const E (&v)[VW]) {
     }
 }
 
+// Streaming load (last use: evict first) and an L2-resident store.
+template <typename E, int VW>
+__device__ __forceinline__ void vld_cs(const E *p, E (&v)[VW]) {
+    static_assert(sizeof(E) * VW == 8 || sizeof(E) * VW == 16, "8- or 16-byte vectors");
+    if constexpr (sizeof(E) * VW == 16) {
+        const uint4 q = __ldcs(reinterpret_cast<const uint4 *>(p));
+        memcpy(v, &q, 16);
+    } else {
+        const uint2 q = __ldcs(reinterpret_cast<const uint2 *>(p));
+        memcpy(v, &q, 8);
+    }
+}
+template <typename E, int VW>
+__device__ __forceinline__ void vst_cg(E *p, const E (&v)[VW]) {
+    static_assert(sizeof(E) * VW == 8 || sizeof(E) * VW == 16, "8- or 16-byte vectors");
+    if constexpr (sizeof(E) * VW == 16) {
+        uint4 q;
+        memcpy(&q, v, 16);
+        __stcg(reinterpret_cast<uint4 *>(p), q);
+    } else {
+        uint2 q;
+        memcpy(&q, v, 8);
+        __stcg(reinterpret_cast<uint2 *>(p), q);
+    }
+}
+
 // Factored H*v.  A CTA owns a tile of NC consecutive columns, staged in
 // shared memory row-interleaved (xs[row*NC + j]) so that one up-hop gather is
 // a single NC-wide load serving all NC columns.  Each thread owns VW
@@ -291,6 +317,664 @@ __global__ void __launch_bounds__(256, kHxvMinBlocks) k_hxv(const HxvArgs<T> a) 
     }
 }
 
+// ---------------------------------------------------------------------------
+// k_hxv_rv: the same product with the global loads of a row vector issued
+// together.  Each thread owns two consecutive rows (r, r+1) of the NC-column
+// tile per pass.  Before any shared-memory work it issues, at once, the
+// down-hop neighbour loads of all NC columns (up to kRvDw per column, held in
+// registers), the v_{k-1} rows and the hopping-table entries of its rows; the
+// diagonal and the up-hop gathers from shared memory then run while those
+// loads are in flight, and the neighbour values are consumed last.  One L2
+// round trip per row vector instead of one per column (the v_{k-1} rows are
+// issued after the up hops, where the hop-table registers are free).
+//
+// Shared-memory traffic per row vector is cut to what the gathers need:
+//  * the down-hop offsets and couplings of the tile are read as 16-byte
+//    broadcasts (uint4 / T4), four or two hops per read;
+//  * the column part of the diagonal (bath energies of the down word plus
+//    the impurity term for each impurity up-state) is one table per column,
+//    cdg[j][iu];
+//  * the two rows' 16-byte accesses to the staged tile are ordered per lane
+//    (lanes 4..7 of each quarter warp take row r+1 first), so each quarter
+//    warp touches eight distinct bank quads.
+constexpr int kRvDw = 8;      // down-hop neighbour loads per column held in registers
+constexpr int kRvUp = 8;      // hopping-table entries per row loaded ahead
+constexpr int kRvBlocks = 2;  // CTAs of 256 threads per SM (register budget 128)
+
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+    using type = float2;
+};
+template <>
+struct Pair<double> {
+    using type = double2;
+};
+
+template <typename T, bool LZ>
+__global__ void __launch_bounds__(256, kRvBlocks) k_hxv_rv(const HxvArgs<T> a) {
+    constexpr int NC = 16 / sizeof(T);
+    constexpr int KD = kRvDw, KU = kRvUp;
+    using T2 = typename Pair<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T spu[kMaxParams];
+    __shared__ __align__(16) T cdg[NC][1 << kMaxNorb];
+    __shared__ __align__(16) uint32_t noff[NC][kMaxW];
+    __shared__ __align__(16) T nval[NC][kMaxW];
+    __shared__ int scnt[NC];
+
+    if (LZ) {
+        if (a.status[0]) return;  // chain finished: every later step is a no-op
+    }
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int sw = (tid >> 2) & 1;  // this lane's row order for 16-byte tile accesses
+    const int64_t dimup = a.dimup, dimdw = a.dimdw, ncols = dimdw * a.nstack;
+    const int64_t total = ncols * dimup;
+    for (int i = tid; i < a.P; i += bd) spu[i] = a.pu[i];
+    const int ni = 1 << a.norb;
+    const unsigned imask = (unsigned)ni - 1u;
+    const int W = a.W, WW = W > KD ? W : KD;
+
+    double sc = 1.0, cprev = 0.0;
+    if (LZ) {
+        sc = a.scale[a.k];
+        cprev = a.k > 0 ? a.beta[a.k] * a.scale[a.k - 1] : 0.0;
+    }
+    const T sch = (T)sc, scl = (T)(sc - (double)sch);
+    const T cph = (T)cprev, cpl = (T)(cprev - (double)cph);
+    const T *x = a.x + (int64_t)blockIdx.y * a.vstride;
+    T *y = a.y + (int64_t)blockIdx.y * a.vstride;
+    const T *xprev = LZ ? a.xprev + (int64_t)blockIdx.y * a.vstride : nullptr;
+    T *xs = reinterpret_cast<T *>(smem_raw);  // [dimup][NC]
+    CSum dot;
+    dot.zero();
+
+    for (int64_t c0 = (int64_t)blockIdx.x * NC; c0 < ncols; c0 += (int64_t)gridDim.x * NC) {
+        const int nc = (int)min((int64_t)NC, ncols - c0);
+        __syncthreads();
+        // stage the tile (rows r and r+1 of NC columns), transposed in registers
+        for (int64_t r = (int64_t)tid * 2; r < dimup; r += (int64_t)bd * 2) {
+            T2 v[NC];
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                const int64_t idx = (c0 + j) * dimup + r;
+                if (j < nc && DM_IN(idx + 1, total))
+                    v[j] = *reinterpret_cast<const T2 *>(x + idx);
+                else
+                    v[j].x = v[j].y = T(0);
+            }
+            T ra[NC], rb[NC];
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                ra[j] = sw ? v[j].y : v[j].x;
+                rb[j] = sw ? v[j].x : v[j].y;
+            }
+            if (DM_IN((r + 1) * NC + NC - 1, dimup * NC)) {
+                vst<T, NC>(xs + (r + sw) * NC, ra);
+                vst<T, NC>(xs + (r + 1 - sw) * NC, rb);
+            }
+        }
+        // column tables: diagonal per impurity up-state, down-hop offsets and
+        // couplings (zero for the unused slots and the columns of a partial tile)
+        if (tid < NC) {
+            int cnt = 0;
+            if (tid < nc) {
+                const int64_t cg = c0 + tid, q = cg / dimdw;
+                const int64_t cc = DM_IN(cg - q * dimdw, dimdw) ? cg - q * dimdw : 0;
+                cnt = a.cd[cc];
+                const unsigned id = a.wd[cc] & imask;
+                const T dd = a.dd[cc];
+                for (int iu = 0; iu < ni; iu++)
+                    cdg[tid][iu] = dd + a.dint[a.dswap ? id * ni + iu : iu * ni + id];
+            } else {
+                for (int iu = 0; iu < ni; iu++) cdg[tid][iu] = T(0);
+            }
+            scnt[tid] = cnt;
+        }
+        for (int t = tid; t < NC * WW; t += bd) {
+            const int j = t / WW, e = t % WW;
+            uint32_t off = 0;
+            T v = T(0);
+            if (j < nc && e < W) {
+                const int64_t cg = c0 + j, q = cg / dimdw, cc = cg - q * dimdw;
+                if (e < (int)a.cd[cc] && DM_IN(e, kMaxW)) {
+                    const uint32_t en = a.ed[(int64_t)e * dimdw + cc];
+                    const bool ok = DM_IN(ell_par(en), a.P) && DM_IN(ell_col(en), dimdw);
+                    v = ok ? a.pd[ell_par(en)] : T(0);
+                    if (ell_neg(en)) v = -v;
+                    off = ok ? (uint32_t)((q * dimdw + (int64_t)ell_col(en)) * dimup) : 0u;
+                }
+            }
+            if (DM_IN(e, kMaxW)) {
+                noff[j][e] = off;
+                nval[j][e] = v;
+            }
+        }
+        __syncthreads();
+        for (int64_t r = (int64_t)tid * 2; r < dimup; r += (int64_t)bd * 2) {
+            // 1. global loads: neighbour rows of every column, v_{k-1}, hop tables
+            int cnts[NC];
+            T2 nb[NC][KD];
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                cnts[j] = scnt[j];
+                uint32_t o[KD];
+#pragma unroll
+                for (int e = 0; e < KD; e += 4) {
+                    const uint4 q4 = *reinterpret_cast<const uint4 *>(&noff[j][e]);
+                    o[e] = q4.x;
+                    o[e + 1] = q4.y;
+                    o[e + 2] = q4.z;
+                    o[e + 3] = q4.w;
+                }
+#pragma unroll
+                for (int e = 0; e < KD; e++) {
+                    if (e < cnts[j] && DM_IN(o[e] + r + 1, total)) {
+                        T t2[2];
+                        vld_cg<T, 2>(x + o[e] + r, t2);
+                        nb[j][e].x = t2[0];
+                        nb[j][e].y = t2[1];
+                    } else {
+                        nb[j][e].x = nb[j][e].y = T(0);
+                    }
+                }
+            }
+            const unsigned short cu2 = *reinterpret_cast<const unsigned short *>(a.cu + r);
+            const int cu0 = cu2 & 0xff, cu1 = cu2 >> 8;
+            const int cmax = max(cu0, cu1);
+            uint2 en[KU];
+#pragma unroll
+            for (int q = 0; q < KU; q++) {
+                if (q < cmax && DM_IN(q, W))
+                    en[q] = *reinterpret_cast<const uint2 *>(a.eu + (int64_t)q * dimup + r);
+                else
+                    en[q] = make_uint2(0u, 0u);
+            }
+            const uint2 wu2 = *reinterpret_cast<const uint2 *>(a.wu + r);
+            const T2 du2 = *reinterpret_cast<const T2 *>(a.du + r);
+
+            // 2. diagonal from the staged tile
+            T acc[NC][2];
+            {
+                T x0[NC], x1[NC];
+                T xa[NC], xb[NC];
+                vld<T, NC>(xs + (r + sw) * NC, xa);
+                vld<T, NC>(xs + (r + 1 - sw) * NC, xb);
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    x0[j] = sw ? xb[j] : xa[j];
+                    x1[j] = sw ? xa[j] : xb[j];
+                }
+                const unsigned iu0 = wu2.x & imask, iu1 = wu2.y & imask;
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    acc[j][0] = (du2.x + cdg[j][iu0]) * x0[j];
+                    acc[j][1] = (du2.y + cdg[j][iu1]) * x1[j];
+                }
+            }
+            // 3. up hops: NC-wide gathers from the tile
+#pragma unroll
+            for (int q = 0; q < KU; q++) {
+#pragma unroll
+                for (int i = 0; i < 2; i++) {
+                    const uint32_t e = i ? en[q].y : en[q].x;
+                    if (q < (i ? cu1 : cu0) && DM_IN(ell_col(e), dimup) && DM_IN(ell_par(e), a.P)) {
+                        T v = spu[ell_par(e)];
+                        if (ell_neg(e)) v = -v;
+                        T xg[NC];
+                        vld<T, NC>(xs + (int64_t)ell_col(e) * NC, xg);
+#pragma unroll
+                        for (int j = 0; j < NC; j++) acc[j][i] += v * xg[j];
+                    }
+                }
+            }
+            for (int q = KU; q < cmax && q < W; q++) {
+                const uint2 e2 = *reinterpret_cast<const uint2 *>(a.eu + (int64_t)q * dimup + r);
+#pragma unroll
+                for (int i = 0; i < 2; i++) {
+                    const uint32_t e = i ? e2.y : e2.x;
+                    if (q < (i ? cu1 : cu0) && DM_IN(ell_col(e), dimup) && DM_IN(ell_par(e), a.P)) {
+                        T v = spu[ell_par(e)];
+                        if (ell_neg(e)) v = -v;
+                        T xg[NC];
+                        vld<T, NC>(xs + (int64_t)ell_col(e) * NC, xg);
+#pragma unroll
+                        for (int j = 0; j < NC; j++) acc[j][i] += v * xg[j];
+                    }
+                }
+            }
+            // v_{k-1} rows: issued here, where the hop-table registers are free
+            T2 xp[NC];
+            if (LZ) {
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    const int64_t idx = (c0 + j) * dimup + r;
+                    if (j < nc && DM_IN(idx + 1, total))
+                        xp[j] = *reinterpret_cast<const T2 *>(xprev + idx);
+                    else
+                        xp[j].x = xp[j].y = T(0);
+                }
+            }
+            // 4. down hops: consume the neighbour rows, stream any beyond KD
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                constexpr int NV = 16 / sizeof(T);
+                T vv[KD];
+#pragma unroll
+                for (int e = 0; e < KD; e += NV) {
+                    T t4[NV];
+                    vld<T, NV>(&nval[j][e], t4);
+#pragma unroll
+                    for (int i = 0; i < NV; i++) vv[e + i] = t4[i];
+                }
+#pragma unroll
+                for (int e = 0; e < KD; e++) {
+                    acc[j][0] += vv[e] * nb[j][e].x;
+                    acc[j][1] += vv[e] * nb[j][e].y;
+                }
+                for (int e = KD; e < cnts[j] && e < W; e++) {
+                    const uint32_t o = noff[j][e];
+                    if (!DM_IN(o + r + 1, total)) continue;
+                    T xv[2];
+                    vld_cg<T, 2>(x + o + r, xv);
+                    const T v = nval[j][e];
+                    acc[j][0] += v * xv[0];
+                    acc[j][1] += v * xv[1];
+                }
+            }
+            // 5. Lanczos combination, store, alpha partial (the rows' own
+            // values re-read from the tile)
+            double part = 0.0;
+            T x0[NC], x1[NC];
+            if (LZ) {
+                T xa[NC], xb[NC];
+                vld<T, NC>(xs + (r + sw) * NC, xa);
+                vld<T, NC>(xs + (r + 1 - sw) * NC, xb);
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    x0[j] = sw ? xb[j] : xa[j];
+                    x1[j] = sw ? xa[j] : xb[j];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                if (j >= nc) continue;
+                const int64_t idx = (c0 + j) * dimup + r;
+                if (!DM_IN(idx + 1, total)) continue;
+                if (LZ) {
+                    const T xpv[2] = {xp[j].x, xp[j].y};
+#pragma unroll
+                    for (int i = 0; i < 2; i++) {
+                        if constexpr (sizeof(T) == 8) {
+                            acc[j][i] = sc * acc[j][i] - cprev * xpv[i];
+                        } else {
+                            T t = -cpl * xpv[i];
+                            t = fmaf(-cph, xpv[i], t);
+                            t = fmaf(scl, acc[j][i], t);
+                            acc[j][i] = fmaf(sch, acc[j][i], t);
+                        }
+                    }
+                    part = fma((double)x0[j], (double)acc[j][0], part);
+                    part = fma((double)x1[j], (double)acc[j][1], part);
+                }
+                vst_cs<T, 2>(y + idx, acc[j]);
+            }
+            if (LZ) dot.add(part);
+        }
+    }
+    if (LZ) {
+        CSum arr[1] = {dot};
+        double tot[1];
+        if (grid_reduce<1>(arr, a.partials, a.counter, tot)) {
+            if (tid == 0) a.alpha[a.k] = sc * tot[0];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_hxv_lean: k_hxv_rv with the per-element instruction count cut down, for
+// sectors whose words have at most 8 hops per spin (every sector of the
+// single-orbital baths up to Nbath = 15 at and near half filling).
+//  * Row hops come from the gather table `ellx` (built from the balanced ELL
+//    table): each entry is the shared-memory byte offset of the target row
+//    (bits 0..23) and an index into a signed-coupling table (bits 24..31,
+//    2p for +V_p, 2p+1 for -V_p, kLeanZero for 0).  A row with fewer than KU
+//    hops is padded with zero-coupling entries that point at the row itself,
+//    so the hop loop has a fixed length and no predicates.
+//  * Column hops are padded the same way to KD per column (padding points at
+//    the column's own data with a zero coupling).
+//  * Row and element indices are 32-bit (the stacked vector has fewer than
+//    2^32 elements).
+// KU, KD: hops per row / per column after padding (7 or 8).
+constexpr uint32_t kLeanZero = 255u;
+
+// MODE 0: plain product; 1: fused Lanczos step (u and its alpha); 2: the
+// whole Lanczos step in one cooperative launch: after the alpha partials a
+// grid barrier, every block folds them (same order, same alpha everywhere),
+// then rewrites its own tiles as w = u - alpha v_k and reduces |w| to
+// b_{k+1}, replacing k_lz_update.  In mode 2 u is stored with the default L2
+// policy so that the second pass finds u and v_k in L2.
+template <typename T, int KU, int KD, int MODE>
+__global__ void __launch_bounds__(256, kRvBlocks) k_hxv_lean(const HxvArgs<T> a,
+                                                           const uint32_t *__restrict__ eux) {
+    constexpr bool LZ = MODE >= 1, FUSE = MODE == 2;
+    constexpr int NC = 16 / sizeof(T);
+    constexpr int NV = 16 / sizeof(T);
+    using T2 = typename Pair<T>::type;
+    static_assert(KU <= 8 && KD <= 8, "hop counts above 8 use k_hxv_rv");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ T spv[256];
+    __shared__ __align__(16) T cdg[NC][1 << kMaxNorb];
+    __shared__ __align__(16) uint32_t noff[NC][8];
+    __shared__ __align__(16) T nval[NC][8];
+
+    if (LZ) {
+        if (a.status[0]) return;  // chain finished: every later step is a no-op
+    }
+    const int tid = threadIdx.x, bd = blockDim.x;
+    const int sw = (tid >> 2) & 1;  // this lane's row order for 16-byte tile accesses
+    const uint32_t dimup = (uint32_t)a.dimup, dimdw = (uint32_t)a.dimdw;
+    const uint32_t ncols = dimdw * (uint32_t)a.nstack;
+    const uint32_t total = ncols * dimup;
+    for (int i = tid; i < 256; i += bd) {
+        T v = T(0);
+        if (i < 2 * a.P && i != (int)kLeanZero) {
+            v = a.pu[i >> 1];
+            if (i & 1) v = -v;
+        }
+        spv[i] = v;
+    }
+    const int ni = 1 << a.norb;
+    const unsigned imask = (unsigned)ni - 1u;
+
+    double sc = 1.0, cprev = 0.0;
+    if (LZ) {
+        sc = a.scale[a.k];
+        cprev = a.k > 0 ? a.beta[a.k] * a.scale[a.k - 1] : 0.0;
+    }
+    const T sch = (T)sc, scl = (T)(sc - (double)sch);
+    const T cph = (T)cprev, cpl = (T)(cprev - (double)cph);
+    const T *x = a.x + (int64_t)blockIdx.y * a.vstride;
+    T *y = a.y + (int64_t)blockIdx.y * a.vstride;
+    const T *xprev = LZ ? a.xprev + (int64_t)blockIdx.y * a.vstride : nullptr;
+    T *xs = reinterpret_cast<T *>(smem_raw);  // [dimup][NC]
+    const unsigned char *xsb = smem_raw;
+    CSum dot;
+    dot.zero();
+
+    for (uint32_t c0 = blockIdx.x * NC; c0 < ncols; c0 += gridDim.x * NC) {
+        const int nc = (int)min((uint32_t)NC, ncols - c0);
+        __syncthreads();
+        // stage the tile (rows r and r+1 of NC columns), transposed in registers
+        for (uint32_t r = tid * 2; r < dimup; r += bd * 2) {
+            T2 v[NC];
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                const uint32_t idx = (c0 + j) * dimup + r;
+                if (j < nc && DM_IN(idx + 1, total))
+                    v[j] = *reinterpret_cast<const T2 *>(x + idx);
+                else
+                    v[j].x = v[j].y = T(0);
+            }
+            T ra[NC], rb[NC];
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                ra[j] = sw ? v[j].y : v[j].x;
+                rb[j] = sw ? v[j].x : v[j].y;
+            }
+            if (DM_IN((r + 1) * NC + NC - 1, dimup * NC)) {
+                vst<T, NC>(xs + (r + sw) * NC, ra);
+                vst<T, NC>(xs + (r + 1 - sw) * NC, rb);
+            }
+        }
+        // column tables; padding and the columns of a partial tile read the
+        // last real column of the tile with a zero coupling
+        if (tid < NC) {
+            if (tid < nc) {
+                const uint32_t cg = c0 + tid, q = cg / dimdw;
+                const uint32_t cc = DM_IN(cg - q * dimdw, dimdw) ? cg - q * dimdw : 0u;
+                const unsigned id = a.wd[cc] & imask;
+                const T dd = a.dd[cc];
+                for (int iu = 0; iu < ni; iu++)
+                    cdg[tid][iu] = dd + a.dint[a.dswap ? id * ni + iu : iu * ni + id];
+            } else {
+                for (int iu = 0; iu < ni; iu++) cdg[tid][iu] = T(0);
+            }
+        }
+        for (int t = tid; t < NC * 8; t += bd) {
+            const int j = t >> 3, e = t & 7;
+            const uint32_t jl = (uint32_t)min(j, nc - 1);
+            uint32_t off = (c0 + jl) * dimup;
+            T v = T(0);
+            if (j < nc && e < KD) {
+                const uint32_t cg = c0 + j, q = cg / dimdw, cc = cg - q * dimdw;
+                if (e < (int)a.cd[cc] && DM_IN(e, a.W)) {
+                    const uint32_t en = a.ed[(int64_t)e * dimdw + cc];
+                    const bool ok = DM_IN(ell_par(en), a.P) && DM_IN(ell_col(en), dimdw);
+                    if (ok) {
+                        v = a.pd[ell_par(en)];
+                        if (ell_neg(en)) v = -v;
+                        off = (q * dimdw + ell_col(en)) * dimup;
+                    }
+                }
+            }
+            noff[j][e] = off;
+            nval[j][e] = v;
+        }
+        __syncthreads();
+        for (uint32_t r = tid * 2; r < dimup; r += bd * 2) {
+            // 1. global loads: neighbour rows of every column, hop tables
+            T2 nb[NC][KD];
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                uint32_t o[8];
+                const uint4 q0 = *reinterpret_cast<const uint4 *>(&noff[j][0]);
+                const uint4 q1 = *reinterpret_cast<const uint4 *>(&noff[j][4]);
+                o[0] = q0.x; o[1] = q0.y; o[2] = q0.z; o[3] = q0.w;
+                o[4] = q1.x; o[5] = q1.y; o[6] = q1.z; o[7] = q1.w;
+#pragma unroll
+                for (int e = 0; e < KD; e++) {
+                    T t2[2];
+                    if (DM_IN(o[e] + r + 1, total)) {
+                        vld_cg<T, 2>(x + (o[e] + r), t2);
+                    } else {
+                        t2[0] = t2[1] = T(0);
+                    }
+                    nb[j][e].x = t2[0];
+                    nb[j][e].y = t2[1];
+                }
+            }
+            uint2 en[KU];
+#pragma unroll
+            for (int q = 0; q < KU; q++)
+                en[q] = *reinterpret_cast<const uint2 *>(eux + (q * dimup + r));
+            const uint2 wu2 = *reinterpret_cast<const uint2 *>(a.wu + r);
+            const T2 du2 = *reinterpret_cast<const T2 *>(a.du + r);
+
+            // 2. diagonal from the staged tile
+            T acc[NC][2];
+            {
+                T xa[NC], xb[NC];
+                vld<T, NC>(xs + (r + sw) * NC, xa);
+                vld<T, NC>(xs + (r + 1 - sw) * NC, xb);
+                const unsigned iu0 = wu2.x & imask, iu1 = wu2.y & imask;
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    acc[j][0] = (du2.x + cdg[j][iu0]) * (sw ? xb[j] : xa[j]);
+                    acc[j][1] = (du2.y + cdg[j][iu1]) * (sw ? xa[j] : xb[j]);
+                }
+            }
+            // 3. row hops: NC-wide gathers from the tile, fixed count
+#pragma unroll
+            for (int q = 0; q < KU; q++) {
+#pragma unroll
+                for (int i = 0; i < 2; i++) {
+                    const uint32_t e = i ? en[q].y : en[q].x;
+                    const T v = spv[e >> 24];
+                    const uint32_t bo = e & 0xFFFFFFu;
+                    T xg[NC];
+                    if (DM_IN(bo / 16, dimup)) {
+                        vld<T, NC>(reinterpret_cast<const T *>(xsb + bo), xg);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < NC; j++) xg[j] = T(0);
+                    }
+#pragma unroll
+                    for (int j = 0; j < NC; j++) acc[j][i] += v * xg[j];
+                }
+            }
+            // v_{k-1} rows: issued here, where the hop-table registers are free
+            T2 xp[NC];
+            if (LZ) {
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    const uint32_t idx = (c0 + (uint32_t)min(j, nc - 1)) * dimup + r;
+                    if (DM_IN(idx + 1, total)) {
+                        T t2[2];
+                        vld_cs<T, 2>(xprev + idx, t2);  // last use of v_{k-1} in the step
+                        xp[j].x = t2[0];
+                        xp[j].y = t2[1];
+                    } else {
+                        xp[j].x = xp[j].y = T(0);
+                    }
+                }
+            }
+            // 4. column hops: consume the neighbour rows
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                T vv[8];
+#pragma unroll
+                for (int e = 0; e < 8; e += NV) {
+                    T t4[NV];
+                    vld<T, NV>(&nval[j][e], t4);
+#pragma unroll
+                    for (int i = 0; i < NV; i++) vv[e + i] = t4[i];
+                }
+#pragma unroll
+                for (int e = 0; e < KD; e++) {
+                    acc[j][0] += vv[e] * nb[j][e].x;
+                    acc[j][1] += vv[e] * nb[j][e].y;
+                }
+            }
+            // 5. Lanczos combination, store, alpha partial (the rows' own
+            // values re-read from the tile)
+            double part = 0.0;
+            T x0[NC], x1[NC];
+            if (LZ) {
+                T xa[NC], xb[NC];
+                vld<T, NC>(xs + (r + sw) * NC, xa);
+                vld<T, NC>(xs + (r + 1 - sw) * NC, xb);
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    x0[j] = sw ? xb[j] : xa[j];
+                    x1[j] = sw ? xa[j] : xb[j];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NC; j++) {
+                if (j >= nc) continue;
+                const uint32_t idx = (c0 + j) * dimup + r;
+                if (!DM_IN(idx + 1, total)) continue;
+                if (LZ) {
+                    const T xpv[2] = {xp[j].x, xp[j].y};
+#pragma unroll
+                    for (int i = 0; i < 2; i++) {
+                        if constexpr (sizeof(T) == 8) {
+                            acc[j][i] = sc * acc[j][i] - cprev * xpv[i];
+                        } else {
+                            T t = -cpl * xpv[i];
+                            t = fmaf(-cph, xpv[i], t);
+                            t = fmaf(scl, acc[j][i], t);
+                            acc[j][i] = fmaf(sch, acc[j][i], t);
+                        }
+                    }
+                    part = fma((double)x0[j], (double)acc[j][0], part);
+                    part = fma((double)x1[j], (double)acc[j][1], part);
+                }
+                if (FUSE)
+                    vst_cg<T, 2>(y + idx, acc[j]);
+                else
+                    vst_cs<T, 2>(y + idx, acc[j]);
+            }
+            if (LZ) dot.add(part);
+        }
+    }
+    if (MODE == 1) {
+        CSum arr[1] = {dot};
+        double tot[1];
+        if (grid_reduce<1>(arr, a.partials, a.counter, tot)) {
+            if (tid == 0) a.alpha[a.k] = sc * tot[0];
+        }
+    }
+    if (FUSE) {
+        // alpha: block partials, barrier, the same ordered fold in every block
+        __shared__ double sred[64];
+        __shared__ double s_alpha;
+        const unsigned nb = gridDim.x;
+        {
+            CSum arr[1] = {dot};
+            block_reduce<1>(arr, sred);
+            if (tid == 0) {
+                a.partials[2 * blockIdx.x + 0] = arr[0].hi;
+                a.partials[2 * blockIdx.x + 1] = arr[0].lo;
+            }
+        }
+        if (!grid_barrier(a.counter + 1, a.counter + 2, a.status + kStBarrierErr, nb)) return;
+        {
+            CSum b;
+            b.zero();
+            for (unsigned j = tid; j < nb; j += bd)
+                b.merge(__ldcg(&a.partials[2 * j + 0]), __ldcg(&a.partials[2 * j + 1]));
+            CSum arr[1] = {b};
+            block_reduce<1>(arr, sred);
+            if (tid == 0) s_alpha = arr[0].value();
+            __syncthreads();
+        }
+        const double alpha = sc * s_alpha;
+        if (blockIdx.x == 0 && tid == 0) a.alpha[a.k] = alpha;
+        const double coef = alpha * sc;
+        // w = u - alpha v_k over the elements this thread wrote, |w|^2
+        CSum nrm;
+        nrm.zero();
+        for (uint32_t c0 = blockIdx.x * NC; c0 < ncols; c0 += gridDim.x * NC) {
+            const int nc = (int)min((uint32_t)NC, ncols - c0);
+            for (uint32_t r = tid * 2; r < dimup; r += bd * 2) {
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    if (j >= nc) continue;
+                    const uint32_t idx = (c0 + j) * dimup + r;
+                    if (!DM_IN(idx + 1, total)) continue;
+                    T u2[2], x2[2];
+                    vld_cg<T, 2>(y + idx, u2);
+                    vld_cg<T, 2>(x + idx, x2);
+#pragma unroll
+                    for (int i = 0; i < 2; i++) {
+                        u2[i] = (T)((double)u2[i] - coef * (double)x2[i]);
+                        nrm.add((double)u2[i] * (double)u2[i]);
+                    }
+                    vst_cg<T, 2>(y + idx, u2);
+                }
+            }
+        }
+        CSum arr[1] = {nrm};
+        double tot[1];
+        if (grid_reduce<1>(arr, a.partials + 2 * nb, a.counter, tot)) {
+            if (tid == 0) {
+                const double b = sqrt(tot[0]);
+                a.beta[a.k + 1] = b;
+                a.scale[a.k + 1] = b > 0.0 ? 1.0 / b : 0.0;
+                a.status[1] = a.k + 1;
+                if (b < a.thr) {
+                    a.status[0] = 1;
+                    a.status[4] = 1;
+                }
+                if (a.k + 1 >= a.kmax) a.status[0] = 1;
+            }
+        }
+    }
+}
+
 template <typename T>
 HxvArgs<T> make_hxv_args(const dmfted_ctx *c, const SectorView &s) {
     HxvArgs<T> a{};
@@ -313,6 +997,10 @@ HxvArgs<T> make_hxv_args(const dmfted_ctx *c, const SectorView &s) {
     a.cd = tq.cnt.p + offq;
     a.eu = tr.ell.p + (int64_t)a.W * offr;
     a.ed = tq.ell.p + (int64_t)a.W * offq;
+    a.eux = tr.ellx.p ? tr.ellx.p + (int64_t)c->WX * offr : nullptr;
+    const int nr = sw ? s.ndw : s.nup, nq = sw ? s.nup : s.ndw;
+    a.ku_max = (int)tr.cls_max.size() > nr ? tr.cls_max[nr] : kMaxW;
+    a.kd_max = (int)tq.cls_max.size() > nq ? tq.cls_max[nq] : kMaxW;
     a.dswap = sw ? 1 : 0;
     if constexpr (sizeof(T) == 8) {
         a.du = (const T *)tr.diag.p + offr;
@@ -385,12 +1073,83 @@ static void launch_nc(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int n
 }
 
 template <typename T, bool LZ>
+static void launch_rv(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
+    auto kern = k_hxv_rv<T, LZ>;
+    static bool attr_set[64] = {false};
+    if (!attr_set[c->device & 63]) {
+        DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
+        attr_set[c->device & 63] = true;
+    }
+    dim3 grid(g.grid, nvec);
+    kern<<<grid, g.threads, g.smem, c->stream>>>(a);
+    DM_CHECK_LAUNCH();
+    c->launches++;
+}
+
+template <typename T, int KU, int KD, int MODE>
+static void launch_lean_k(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
+    auto kern = k_hxv_lean<T, KU, KD, MODE>;
+    static bool attr_set[64] = {false};
+    static int resident[64] = {0};  // blocks per SM at the full shared-memory size
+    if (!attr_set[c->device & 63]) {
+        DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
+        attr_set[c->device & 63] = true;
+    }
+    if (MODE == 2) {
+        // cooperative: every block resident (the grid barrier needs it)
+        int per_sm = 0;
+        DM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, g.threads, g.smem));
+        DM_REQUIRE(per_sm > 0 && nvec == 1, DMFTED_ERR_UNSUPPORTED,
+                   "fused Lanczos step: no resident block for this sector");
+        (void)resident;
+        const int grid = std::min(g.grid, per_sm * num_sms(c));
+        void *args[] = {(void *)&a, (void *)&a.eux};
+        DM_CUDA(cudaLaunchCooperativeKernel((const void *)kern, dim3(grid), dim3(g.threads), args,
+                                            g.smem, c->stream));
+    } else {
+        dim3 grid(g.grid, nvec);
+        kern<<<grid, g.threads, g.smem, c->stream>>>(a, a.eux);
+    }
+    DM_CHECK_LAUNCH();
+    c->launches++;
+}
+
+// Hop counts padded to 7 or 8 (rows and columns independently).
+template <typename T, int MODE>
+static void launch_lean(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
+    const bool u8 = a.ku_max > 7, d8 = a.kd_max > 7;
+    if (u8 && d8) launch_lean_k<T, 8, 8, MODE>(c, a, g, nvec);
+    else if (u8) launch_lean_k<T, 8, 7, MODE>(c, a, g, nvec);
+    else if (d8) launch_lean_k<T, 7, 8, MODE>(c, a, g, nvec);
+    else launch_lean_k<T, 7, 7, MODE>(c, a, g, nvec);
+}
+
+// Whether the lean kernel serves this sector view: at most 8 hops per word
+// on either side, signed coupling indices within 8 bits, row offsets within
+// 24 bits, two-row vectors, fewer than 2^32 stacked elements.
+template <typename T>
+static bool lean_ok(const dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g) {
+    return g.vw == 2 && c->tune_hxv != 1 && c->tune_hxv != 2 && a.eux && a.ku_max <= 8 &&
+           a.kd_max <= 8 && 2 * a.P <= (int)kLeanZero && a.dimup * 16 < (1 << 24) &&
+           (double)a.dimup * a.dimdw * a.nstack < 4.0e9;
+}
+
+template <typename T, bool LZ>
 static void launch_hxv(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
     constexpr int NCT = 16 / sizeof(T);
     // algorithmic bytes: read x (and v_prev for the Lanczos step), write y
     const double bytes = (LZ ? 3.0 : 2.0) * (double)a.dimup * a.dimdw * a.nstack * nvec * sizeof(T);
+    // the register-batched kernel needs two-row vectors and 32-bit element
+    // offsets within the stacked vector
+    const bool rv = g.vw == 2 && c->tune_hxv != 1 &&
+                    (double)a.dimup * a.dimdw * a.nstack < 4.0e9;
+    const bool lean = lean_ok<T>(c, a, g);
     hv_timer_begin(c);
-    if (g.vw == 2) launch_nc<T, NCT, 2, LZ>(c, a, g, nvec);
+    if (lean) launch_lean<T, LZ ? 1 : 0>(c, a, g, nvec);
+    else if (rv) launch_rv<T, LZ>(c, a, g, nvec);
+    else if (g.vw == 2) launch_nc<T, NCT, 2, LZ>(c, a, g, nvec);
     else launch_nc<T, NCT, 1, LZ>(c, a, g, nvec);
     hv_timer_end(c, bytes);
 }

@@ -27,6 +27,9 @@
 
 namespace dmfted {
 
+// Lanczos status word set when a grid barrier of the fused step timed out.
+constexpr int kStBarrierErr = 5;
+
 template <typename T>
 struct HxvArgs {
     int64_t dimup, dimdw;
@@ -37,6 +40,8 @@ struct HxvArgs {
     const uint32_t *eu, *ed;   // ELL (row stride dimup / dimdw)
     const T *pu, *pd;          // coupling values
     const T *dint;             // (1<<norb)^2 impurity diagonal
+    const uint32_t *eux;       // lean gather table of the row class (stride dimup)
+    int ku_max, kd_max;        // most hops of a row word / of a column word
     int dswap;                 // rows are down words: dint is indexed [dw][up]
     const T *x;
     T *y;
@@ -48,6 +53,10 @@ struct HxvArgs {
     double *alpha, *beta, *scale;
     int *status;
     int k;
+    // fused step (H*v, then w = u - alpha v_k and b_{k+1} = |w| after a grid
+    // barrier): breakdown threshold and step limit of k_lz_update
+    double thr;
+    int kmax;
     double *partials;
     unsigned *counter;
 };

@@ -126,6 +126,11 @@ struct DBuf {
 struct SpinTables {
     DBuf<uint8_t> cnt;
     DBuf<uint32_t> ell;
+    // gather table of k_hxv_lean, width WX = max(W, 8): per hop the byte offset
+    // of the target row in a 16-byte-per-row tile (bits 0..23) and the signed
+    // coupling index 2p + sign (bits 24..31; 255 = zero coupling, padding)
+    DBuf<uint32_t> ellx;
+    std::vector<int> cls_max;  // most hops of a word, per popcount class
     DBuf<double> diag;
     DBuf<float> diag_f;
     DBuf<double> par;  // [P] coupling values (V_{a,k}, then Re Hloc_{ab})
@@ -167,6 +172,7 @@ struct dmfted_ctx {
     int ns = 0, norb = 0, nbath = 0, nspin = 0;
     int nsectors = 0;
     int W = 0;  // ELL width
+    int WX = 0; // width of the lean gather table (max(W, 8))
     int P = 0;  // couplings per spin
     int64_t nwords = 0;
     std::vector<int64_t> class_off;   // compact class offsets (size kMaxNs+2)
@@ -209,6 +215,8 @@ struct dmfted_ctx {
     dmfted::DBuf<double> s64a, s64b, s64c;  // sector-sized FP64 scratch
     double mixed_tol32 = 1e-6;            // FP32-phase stopping tolerance of the mixed form
     int tune_nc = 0;                      // H*v columns per CTA override (0 = automatic)
+    int tune_hxv = 0;                     // H*v kernel: 0 automatic, 1 k_hxv, 2 k_hxv_rv
+    int tune_ell_group = 0;               // lanes per hop-table balance group (0: 8)
     dmfted::DBuf<double> d_wm, d_wr;      // Matsubara / real-axis grids
     dmfted::DBuf<double> d_bath_e, d_bath_v, d_hloc_aa;  // [nspin][norb][nbath], [nspin][norb]
     dmfted::DBuf<double> obs_d;           // observable accumulators of one state
