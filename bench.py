@@ -460,7 +460,7 @@ def main():
         config={"workload": "impurity solve Ns=14 (Nbath=13, U=3, beta=100) sector 7/7 "
                             "dim 11778624: Lanczos GS (residual tol 1e-12) + observables + "
                             "particle/hole chains (200 steps) + G, Sigma on Lmats=4096",
-                "precision": "mixed (FP32 vectors, compensated FP64 alpha/beta, FP64 refinement)",
+                "precision": "mixed (FP32 vectors, compensated FP64 alpha/beta, FP64 refinement, GF chains with 20 leading FP64 steps)",
                 "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between steps",
                 "seed": SEED},
         fp64_dropin=dict(ms_per_step=t_fp64 / args.steps * 1e3,

@@ -611,9 +611,11 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         if (const char *e = getenv("DMFTED_HXV_KERNEL")) c->tune_hxv = atoi(e);
         if (const char *e = getenv("DMFTED_ELL_GROUP")) c->tune_ell_group = std::max(1, std::min(32, atoi(e)));
         if (const char *e = getenv("DMFTED_MIXED_TOL32")) c->mixed_tol32 = atof(e);
+        if (const char *e = getenv("DMFTED_GF_HEAD64")) c->gf_head64 = std::max(0, atoi(e));
         if (const char *e = getenv("DMFTED_BATCH_MAX_DIM")) c->batch_max_dim = atoll(e);
         if (const char *e = getenv("DMFTED_BATCH_BUDGET_MB")) c->batch_budget = atoll(e) << 20;
         if (const char *e = getenv("DMFTED_FT_EIGS_FP32")) c->ft_eigs_fp32 = atoi(e) != 0;
+        if (const char *e = getenv("DMFTED_BATCH_CHAINS_FP32")) c->batch_chains_fp32 = atoi(e) != 0;
         if (const char *e = getenv("DMFTED_BATCH_CLUSTER_MIN"))
             c->batch_cluster_min = std::max<int64_t>(1, atoll(e));
         DM_CUDA(cudaSetDevice(c->device));
@@ -1011,7 +1013,7 @@ int dmfted_time_hxv(dmfted_ctx *c, int32_t flags, int32_t warmup, int32_t reps, 
     DM_REQUIRE(c->cur_sector != 0, DMFTED_ERR_STATE, "time_hxv: Hsector NOT set");
     DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "time_hxv: bath not set");
     DM_CUDA(cudaSetDevice(c->device));
-    const bool fp32 = (flags & 1) != 0, fused = (flags & 2) != 0;
+    const bool fp32 = (flags & 1) != 0, fused = (flags & 2) != 0, whole = (flags & 8) != 0;
     SectorView s = (flags & 4) ? chain_view(c, c->cur_sector) : sector_view(c, c->cur_sector);
     const size_t es = fp32 ? 4 : 8;
     const size_t ld = (size_t)((s.dim + 31) / 32 * 32);
@@ -1019,7 +1021,8 @@ int dmfted_time_hxv(dmfted_ctx *c, int32_t flags, int32_t warmup, int32_t reps, 
     DM_CUDA(cudaMemsetAsync(c->chainbuf.p, 0, 3 * ld * es, c->stream));
     void *x = c->chainbuf.p, *y = c->chainbuf.p + ld * es, *xp = c->chainbuf.p + 2 * ld * es;
     LanczosScalars lz = lz_slot(c, 3, kLzMax);
-    if (fused) {
+    if (whole) lz.kmax = kLzMax - 2;  // step 1 never reaches the step limit
+    if (fused || whole) {
         // step k = 1 of a recurrence with unit scales and b_1 = 0.5
         std::vector<double> init(kLzStride, 0.0);
         for (int i = 0; i < kLzMax + 2; i++) init[2 * (kLzMax + 2) + i] = 1.0;  // scale
@@ -1029,7 +1032,12 @@ int dmfted_time_hxv(dmfted_ctx *c, int32_t flags, int32_t warmup, int32_t reps, 
         DM_CUDA(cudaMemsetAsync(lz.status, 0, 8 * sizeof(int), c->stream));
     }
     auto run = [&]() {
-        if (fused) {
+        if (whole) {
+            // the whole step (update and |w| included); a negative breakdown
+            // threshold keeps the zero test vectors from ending the recurrence
+            if (fp32) lanczos_step<float>(c, s, (const float *)x, (const float *)xp, (float *)y, s.dim, lz, 1, -1.0, 1);
+            else lanczos_step<double>(c, s, (const double *)x, (const double *)xp, (double *)y, s.dim, lz, 1, -1.0, 1);
+        } else if (fused) {
             if (fp32) hxv_lanczos_step<float>(c, s, (const float *)x, (const float *)xp, (float *)y, lz, 1);
             else hxv_lanczos_step<double>(c, s, (const double *)x, (const double *)xp, (double *)y, lz, 1);
         } else {

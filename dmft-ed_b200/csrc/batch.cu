@@ -1000,7 +1000,10 @@ void batch_chains_gf(dmfted_ctx *c, const std::vector<ChainRec> &recs, int preci
     const int L = p.lmats + p.lreal;
     const int nrec = (int)recs.size();
     if (nrec == 0) return;
-    const bool fp64 = precision == DMFTED_FP64;
+    // Batched chains (one CTA or cluster per chain) are FP64 in both forms: an
+    // FP32 chain perturbs G(iwn) at the 1e-6 level and, being latency-bound
+    // rather than bandwidth-bound, saves under 10 % of the chain time.
+    const bool fp64 = precision == DMFTED_FP64 || !c->batch_chains_fp32;
     const size_t es = fp64 ? sizeof(double) : sizeof(float);
     c->bscal.alloc((size_t)2 * nrec * kChainStride + nrec);
     double *alpha = c->bscal.p, *beta = alpha + (size_t)nrec * kChainStride;

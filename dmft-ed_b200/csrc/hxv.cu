@@ -371,6 +371,7 @@ __global__ void __launch_bounds__(256, kRvBlocks) k_hxv_rv(const HxvArgs<T> a) {
     const int sw = (tid >> 2) & 1;  // this lane's row order for 16-byte tile accesses
     const int64_t dimup = a.dimup, dimdw = a.dimdw, ncols = dimdw * a.nstack;
     const int64_t total = ncols * dimup;
+    (void)total;  // bounds of the checked build
     for (int i = tid; i < a.P; i += bd) spu[i] = a.pu[i];
     const int ni = 1 << a.norb;
     const unsigned imask = (unsigned)ni - 1u;
@@ -649,16 +650,11 @@ __global__ void __launch_bounds__(256, kRvBlocks) k_hxv_rv(const HxvArgs<T> a) {
 // KU, KD: hops per row / per column after padding (7 or 8).
 constexpr uint32_t kLeanZero = 255u;
 
-// MODE 0: plain product; 1: fused Lanczos step (u and its alpha); 2: the
-// whole Lanczos step in one cooperative launch: after the alpha partials a
-// grid barrier, every block folds them (same order, same alpha everywhere),
-// then rewrites its own tiles as w = u - alpha v_k and reduces |w| to
-// b_{k+1}, replacing k_lz_update.  In mode 2 u is stored with the default L2
-// policy so that the second pass finds u and v_k in L2.
+// MODE 0: plain product; 1: fused Lanczos step (u and its alpha).
 template <typename T, int KU, int KD, int MODE>
 __global__ void __launch_bounds__(256, kRvBlocks) k_hxv_lean(const HxvArgs<T> a,
                                                            const uint32_t *__restrict__ eux) {
-    constexpr bool LZ = MODE >= 1, FUSE = MODE == 2;
+    constexpr bool LZ = MODE >= 1;
     constexpr int NC = 16 / sizeof(T);
     constexpr int NV = 16 / sizeof(T);
     using T2 = typename Pair<T>::type;
@@ -677,6 +673,7 @@ __global__ void __launch_bounds__(256, kRvBlocks) k_hxv_lean(const HxvArgs<T> a,
     const uint32_t dimup = (uint32_t)a.dimup, dimdw = (uint32_t)a.dimdw;
     const uint32_t ncols = dimdw * (uint32_t)a.nstack;
     const uint32_t total = ncols * dimup;
+    (void)total;  // bounds of the checked build
     for (int i = tid; i < 256; i += bd) {
         T v = T(0);
         if (i < 2 * a.P && i != (int)kLeanZero) {
@@ -892,10 +889,7 @@ __global__ void __launch_bounds__(256, kRvBlocks) k_hxv_lean(const HxvArgs<T> a,
                     part = fma((double)x0[j], (double)acc[j][0], part);
                     part = fma((double)x1[j], (double)acc[j][1], part);
                 }
-                if (FUSE)
-                    vst_cg<T, 2>(y + idx, acc[j]);
-                else
-                    vst_cs<T, 2>(y + idx, acc[j]);
+                vst_cs<T, 2>(y + idx, acc[j]);
             }
             if (LZ) dot.add(part);
         }
@@ -905,72 +899,6 @@ __global__ void __launch_bounds__(256, kRvBlocks) k_hxv_lean(const HxvArgs<T> a,
         double tot[1];
         if (grid_reduce<1>(arr, a.partials, a.counter, tot)) {
             if (tid == 0) a.alpha[a.k] = sc * tot[0];
-        }
-    }
-    if (FUSE) {
-        // alpha: block partials, barrier, the same ordered fold in every block
-        __shared__ double sred[64];
-        __shared__ double s_alpha;
-        const unsigned nb = gridDim.x;
-        {
-            CSum arr[1] = {dot};
-            block_reduce<1>(arr, sred);
-            if (tid == 0) {
-                a.partials[2 * blockIdx.x + 0] = arr[0].hi;
-                a.partials[2 * blockIdx.x + 1] = arr[0].lo;
-            }
-        }
-        if (!grid_barrier(a.counter + 1, a.counter + 2, a.status + kStBarrierErr, nb)) return;
-        {
-            CSum b;
-            b.zero();
-            for (unsigned j = tid; j < nb; j += bd)
-                b.merge(__ldcg(&a.partials[2 * j + 0]), __ldcg(&a.partials[2 * j + 1]));
-            CSum arr[1] = {b};
-            block_reduce<1>(arr, sred);
-            if (tid == 0) s_alpha = arr[0].value();
-            __syncthreads();
-        }
-        const double alpha = sc * s_alpha;
-        if (blockIdx.x == 0 && tid == 0) a.alpha[a.k] = alpha;
-        const double coef = alpha * sc;
-        // w = u - alpha v_k over the elements this thread wrote, |w|^2
-        CSum nrm;
-        nrm.zero();
-        for (uint32_t c0 = blockIdx.x * NC; c0 < ncols; c0 += gridDim.x * NC) {
-            const int nc = (int)min((uint32_t)NC, ncols - c0);
-            for (uint32_t r = tid * 2; r < dimup; r += bd * 2) {
-#pragma unroll
-                for (int j = 0; j < NC; j++) {
-                    if (j >= nc) continue;
-                    const uint32_t idx = (c0 + j) * dimup + r;
-                    if (!DM_IN(idx + 1, total)) continue;
-                    T u2[2], x2[2];
-                    vld_cg<T, 2>(y + idx, u2);
-                    vld_cg<T, 2>(x + idx, x2);
-#pragma unroll
-                    for (int i = 0; i < 2; i++) {
-                        u2[i] = (T)((double)u2[i] - coef * (double)x2[i]);
-                        nrm.add((double)u2[i] * (double)u2[i]);
-                    }
-                    vst_cg<T, 2>(y + idx, u2);
-                }
-            }
-        }
-        CSum arr[1] = {nrm};
-        double tot[1];
-        if (grid_reduce<1>(arr, a.partials + 2 * nb, a.counter, tot)) {
-            if (tid == 0) {
-                const double b = sqrt(tot[0]);
-                a.beta[a.k + 1] = b;
-                a.scale[a.k + 1] = b > 0.0 ? 1.0 / b : 0.0;
-                a.status[1] = a.k + 1;
-                if (b < a.thr) {
-                    a.status[0] = 1;
-                    a.status[4] = 1;
-                }
-                if (a.k + 1 >= a.kmax) a.status[0] = 1;
-            }
         }
     }
 }
@@ -1091,27 +1019,13 @@ template <typename T, int KU, int KD, int MODE>
 static void launch_lean_k(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
     auto kern = k_hxv_lean<T, KU, KD, MODE>;
     static bool attr_set[64] = {false};
-    static int resident[64] = {0};  // blocks per SM at the full shared-memory size
     if (!attr_set[c->device & 63]) {
         DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      200 * 1024));
         attr_set[c->device & 63] = true;
     }
-    if (MODE == 2) {
-        // cooperative: every block resident (the grid barrier needs it)
-        int per_sm = 0;
-        DM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, g.threads, g.smem));
-        DM_REQUIRE(per_sm > 0 && nvec == 1, DMFTED_ERR_UNSUPPORTED,
-                   "fused Lanczos step: no resident block for this sector");
-        (void)resident;
-        const int grid = std::min(g.grid, per_sm * num_sms(c));
-        void *args[] = {(void *)&a, (void *)&a.eux};
-        DM_CUDA(cudaLaunchCooperativeKernel((const void *)kern, dim3(grid), dim3(g.threads), args,
-                                            g.smem, c->stream));
-    } else {
-        dim3 grid(g.grid, nvec);
-        kern<<<grid, g.threads, g.smem, c->stream>>>(a, a.eux);
-    }
+    dim3 grid(g.grid, nvec);
+    kern<<<grid, g.threads, g.smem, c->stream>>>(a, a.eux);
     DM_CHECK_LAUNCH();
     c->launches++;
 }

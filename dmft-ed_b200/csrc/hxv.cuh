@@ -27,9 +27,6 @@
 
 namespace dmfted {
 
-// Lanczos status word set when a grid barrier of the fused step timed out.
-constexpr int kStBarrierErr = 5;
-
 template <typename T>
 struct HxvArgs {
     int64_t dimup, dimdw;
@@ -53,10 +50,6 @@ struct HxvArgs {
     double *alpha, *beta, *scale;
     int *status;
     int k;
-    // fused step (H*v, then w = u - alpha v_k and b_{k+1} = |w| after a grid
-    // barrier): breakdown threshold and step limit of k_lz_update
-    double thr;
-    int kmax;
     double *partials;
     unsigned *counter;
 };

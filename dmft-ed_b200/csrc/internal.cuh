@@ -214,6 +214,7 @@ struct dmfted_ctx {
     dmfted::DBuf<uint8_t> chainbuf;       // rotating vectors of a GF chain
     dmfted::DBuf<double> s64a, s64b, s64c;  // sector-sized FP64 scratch
     double mixed_tol32 = 1e-6;            // FP32-phase stopping tolerance of the mixed form
+    int gf_head64 = 20;                   // leading FP64 steps of a mixed-form GF chain
     int tune_nc = 0;                      // H*v columns per CTA override (0 = automatic)
     int tune_hxv = 0;                     // H*v kernel: 0 automatic, 1 k_hxv, 2 k_hxv_rv
     int tune_ell_group = 0;               // lanes per hop-table balance group (0: 8)
@@ -228,6 +229,7 @@ struct dmfted_ctx {
     int64_t batch_budget = 0;             // bytes of Krylov bases per launch (0: a third of free)
     int64_t batch_cluster_min = 1024;     // states per CTA for a job shared by a cluster
     bool ft_eigs_fp32 = false;            // finite-T eigenpairs with FP32 vectors (measurement only)
+    bool batch_chains_fp32 = false;       // batched GF chains in FP32 in the mixed form (measurement only)
     dmfted::DBuf<uint8_t> bwork;          // Krylov bases / chain vectors of the jobs
     dmfted::DBuf<double> bvec;            // eigenvectors of the batched sectors
     dmfted::DBuf<double> baux;            // Ritz vectors and coefficients
@@ -311,6 +313,11 @@ LanczosScalars lz_slot(dmfted_ctx *c, int slot, int kmax);
 template <typename T>
 void hxv_lanczos_step(dmfted_ctx *c, const SectorView &s, const T *x, const T *xprev, T *y,
                       const LanczosScalars &lz, int k, int nstack = 1);
+// Lanczos step k on n = dim * nstack elements: y = w_{k+1} (unnormalised),
+// a_k, b_{k+1}.
+template <typename T>
+void lanczos_step(dmfted_ctx *c, const SectorView &s, const T *x, const T *xp, T *y, int64_t n,
+                  const LanczosScalars &lz, int k, double thr, int nstack);
 struct LanczosResult {
     double e0;
     int steps;

@@ -303,6 +303,19 @@ static void ritz_attr(dmfted_ctx *c) {
     done[c->device & 63] = true;
 }
 
+// One Lanczos step k: the fused H*v launch followed by the update kernel.
+template <typename T>
+void lanczos_step(dmfted_ctx *c, const SectorView &s, const T *x, const T *xp, T *y, int64_t n,
+                  const LanczosScalars &lz, int k, double thr, int nstack) {
+    hxv_lanczos_step<T>(c, s, x, xp, y, lz, k, nstack);
+    launch_lz_update<T>(c, y, x, n, lz, k, thr);
+}
+template void lanczos_step<double>(dmfted_ctx *, const SectorView &, const double *,
+                                   const double *, double *, int64_t, const LanczosScalars &, int,
+                                   double, int);
+template void lanczos_step<float>(dmfted_ctx *, const SectorView &, const float *, const float *,
+                                  float *, int64_t, const LanczosScalars &, int, double, int);
+
 // One Lanczos run on sector s storing the whole basis in T.
 //  start == nullptr : random start vector (deterministic seed)
 //  refine == false  : start (FP64) is rounded to T and used as s_0
@@ -360,8 +373,7 @@ static LanczosResult gs_run(dmfted_ctx *c, const SectorView &s, double *psi, con
             T *x = basis + (size_t)k * ld;
             const T *xp = basis + (size_t)(k > 0 ? k - 1 : k) * ld;
             T *y = basis + (size_t)(k + 1) * ld;
-            hxv_lanczos_step<T>(c, s, x, xp, y, lz, k);
-            launch_lz_update<T>(c, y, x, dim, lz, k, 1e-300);
+            lanczos_step<T>(c, s, x, xp, y, dim, lz, k, 1e-300, 1);
         }
         k_ritz_check<<<1, kRedThreads, ritz_smem(launched), c->stream>>>(lz, tol);
         DM_CHECK_LAUNCH();
@@ -431,15 +443,54 @@ static void chain_impl(dmfted_ctx *c, const SectorView &s, const double *v0,
     DM_CHECK_LAUNCH();
     c->launches += 2;
     for (int k = 0; k < lz.kmax; k++) {
-        hxv_lanczos_step<T>(c, s, Q, P, P, lz, k, nstack);
-        launch_lz_update<T>(c, P, Q, dim, lz, k, c->p.lanc_gf_threshold);
+        lanczos_step<T>(c, s, Q, P, P, dim, lz, k, c->p.lanc_gf_threshold, nstack);
         std::swap(P, Q);
+    }
+}
+
+// Mixed-precision chain: the first `head` steps in FP64, then FP32.  The
+// Matsubara G(iwn) of a chain depends on its coefficients a_k, b_k with a
+// weight that falls off quickly with k (the continued fraction converges
+// geometrically off the real axis), and FP32 vectors perturb every
+// coefficient at the 1e-7 level.  Computing the leading coefficients in FP64
+// and the tail in FP32 keeps G(iwn) at FP64 accuracy (1e-12 or better for 16+
+// FP64 steps on the single-orbital baths) while most H*v run in FP32.  At the
+// switch the two live vectors are rounded to FP32; their scales (device
+// scalars) carry over unchanged.
+static void chain_mixed(dmfted_ctx *c, const SectorView &s, const double *v0,
+                        const LanczosScalars &lz, int nstack, int head) {
+    const int64_t dim = s.dim * nstack;
+    const size_t ld = (size_t)((dim + 31) / 32 * 32);
+    c->chainbuf.alloc(2 * ld * (sizeof(double) + sizeof(float)));
+    double *P = reinterpret_cast<double *>(c->chainbuf.p), *Q = P + ld;
+    float *Pf = reinterpret_cast<float *>(Q + ld), *Qf = Pf + ld;
+    const int eg = ew_grid(c, dim);
+    DM_CUDA(cudaMemsetAsync(P, 0, ld * sizeof(double), c->stream));
+    k_convert<double, double><<<eg, 256, 0, c->stream>>>(v0, Q, dim);
+    k_lz_init<double><<<red_grid(c, dim), kRedThreads, 0, c->stream>>>(
+        Q, dim, lz, c->red_partials.p, c->red_counter.p);
+    DM_CHECK_LAUNCH();
+    c->launches += 2;
+    const int h = std::min(head, lz.kmax);
+    for (int k = 0; k < h; k++) {
+        lanczos_step<double>(c, s, Q, P, P, dim, lz, k, c->p.lanc_gf_threshold, nstack);
+        std::swap(P, Q);
+    }
+    if (h >= lz.kmax) return;
+    k_convert<float, double><<<eg, 256, 0, c->stream>>>(P, Pf, dim);
+    k_convert<float, double><<<eg, 256, 0, c->stream>>>(Q, Qf, dim);
+    DM_CHECK_LAUNCH();
+    c->launches += 2;
+    for (int k = h; k < lz.kmax; k++) {
+        lanczos_step<float>(c, s, Qf, Pf, Pf, dim, lz, k, c->p.lanc_gf_threshold, nstack);
+        std::swap(Pf, Qf);
     }
 }
 
 void lanczos_chain(dmfted_ctx *c, const SectorView &s, const double *v0, int precision,
                    const LanczosScalars &lz, int nstack) {
     if (precision == DMFTED_FP64) chain_impl<double>(c, s, v0, lz, nstack);
+    else if (c->gf_head64 > 0) chain_mixed(c, s, v0, lz, nstack, c->gf_head64);
     else chain_impl<float>(c, s, v0, lz, nstack);
 }
 

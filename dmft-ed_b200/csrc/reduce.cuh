@@ -123,43 +123,4 @@ __device__ __forceinline__ bool grid_reduce(CSum (&a)[NS], double *partials, uns
     return true;
 }
 
-// Grid-wide barrier of a cooperative launch (every block resident), with a
-// bounded wait.  arrive: counter that is 0 on entry and is left 0; gen: a
-// generation word that the last block to arrive increments.  A block whose
-// wait runs out (about two seconds) sets *err and returns false, and so does
-// every block that sees *err already set; the caller then skips the rest of
-// its work and the host reports the error word.
-constexpr unsigned kBarrierSpins = 1u << 24;
-
-__device__ __forceinline__ bool grid_barrier(unsigned *arrive, unsigned *gen, int *err,
-                                             unsigned nblocks) {
-    __shared__ int ok_s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned g = atomicAdd(gen, 0u);
-        __threadfence();
-        const unsigned t = atomicAdd(arrive, 1u);
-        if (t == nblocks - 1) {
-            atomicExch(arrive, 0u);
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
-            unsigned it = 0;
-            while (*reinterpret_cast<volatile unsigned *>(gen) == g) {
-                if (++it > kBarrierSpins || *reinterpret_cast<volatile int *>(err)) {
-                    atomicExch(err, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        ok_s = ok;
-    }
-    __syncthreads();
-    return ok_s != 0;
-}
-
 }  // namespace dmfted

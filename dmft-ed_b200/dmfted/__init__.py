@@ -246,9 +246,11 @@ class EDSolver:
         _ck(lib().dmfted_hxv_c128(self.ctx, v.size, _p(v.view(np.float64)), _p(hv.view(np.float64))))
         return hv
 
-    def time_hxv(self, fp32=False, warmup=3, reps=10, fused=False, chain_order=False):
+    def time_hxv(self, fp32=False, warmup=3, reps=10, fused=False, chain_order=False,
+                 whole_step=False):
         ms = C.c_double()
-        flags = int(fp32) | (2 if fused else 0) | (4 if chain_order else 0)
+        flags = (int(fp32) | (2 if fused else 0) | (4 if chain_order else 0)
+                 | (8 if whole_step else 0))
         _ck(lib().dmfted_time_hxv(self.ctx, flags, warmup, reps, C.byref(ms)))
         return ms.value
 

@@ -28,6 +28,8 @@ def main(argv=None):
     ap.add_argument("--sector", type=int, nargs=2, default=(7, 7), metavar=("NUP", "NDW"))
     ap.add_argument("--fp32", action="store_true", help="float32 vectors (default float64)")
     ap.add_argument("--fused", action="store_true", help="the fused Lanczos-step variant")
+    ap.add_argument("--step", action="store_true",
+                    help="the whole Lanczos step (fused product, w = u - a x, |w|)")
     ap.add_argument("--chain-order", action="store_true",
                     help="the vector order of Green's-function chains")
     ap.add_argument("--warmup", type=int, default=5)
@@ -46,11 +48,14 @@ def main(argv=None):
         s.setup_hv_sector(isec)
         dim = s.sector_dim(isec)
         ms = s.time_hxv(fp32=a.fp32, warmup=a.warmup, reps=a.reps, fused=a.fused,
-                        chain_order=a.chain_order)
+                        chain_order=a.chain_order, whole_step=a.step)
     es = 4 if a.fp32 else 8
-    nbytes = (3 if a.fused else 2) * dim * es
+    # algorithmic bytes: read x (and v_prev), write y; the whole step has the
+    # same three vectors (u is an intermediate)
+    nbytes = (3 if (a.fused or a.step) else 2) * dim * es
     print(f"sector {a.sector[0]}/{a.sector[1]} dim {dim} {'fp32' if a.fp32 else 'fp64'}"
-          f"{' fused' if a.fused else ''}{' chain-order' if a.chain_order else ''}: "
+          f"{' fused' if a.fused else ''}{' step' if a.step else ''}"
+          f"{' chain-order' if a.chain_order else ''}: "
           f"{ms * 1e3:.1f} us/launch, {nbytes / (ms * 1e-3) / 1e9:.0f} GB/s algorithmic")
 
 

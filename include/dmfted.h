@@ -46,7 +46,10 @@ extern "C" {
 /* ---- precision of the Lanczos vectors ------------------------------- */
 #define DMFTED_FP64 0  /* plain FP64: the drop-in path                       */
 #define DMFTED_MIXED 1 /* FP32 vectors and H*v, compensated FP64 alpha/beta,
-                          FP64 refinement of the ground state, FP64 G(iwn)   */
+                          FP64 refinement of the ground state, GF chains
+                          with their first 20 steps in FP64 and the rest in
+                          FP32 (chains of one-CTA batches: FP64), FP64
+                          continued fractions for G(iwn)                      */
 
 /* Input variables of ED_INPUT_VARS.f90 that define the hot path, with the
  * reference's names and defaults (dmfted_default_params fills those). */
@@ -238,7 +241,9 @@ int dmfted_chi2_delta_batch_device(dmfted_ctx *ctx, int32_t nbatch, int32_t nbat
  * float64), bit 1 = the fused Lanczos-step variant (H*v - b v_prev and the
  * alpha dot product) instead of the plain product, bit 2 = the vector order
  * used by Green's-function chains (down rank fastest when DimUp is odd and
- * DimDw even).  The vectors are the context's own work buffers. */
+ * DimDw even), bit 3 = the whole Lanczos step as the solver runs it (the
+ * fused product, then w = u - a x and |w|).
+ * The vectors are the context's own work buffers. */
 int dmfted_time_hxv(dmfted_ctx *ctx, int32_t flags, int32_t warmup, int32_t reps, double *ms);
 
 /* Live timing of the H*v launches (plain products and fused Lanczos steps)

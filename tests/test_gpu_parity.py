@@ -225,6 +225,23 @@ def test_ed_solve_cfg1_mixed_energy():
     s.close()
 
 
+@pytest.mark.parametrize("u,head", [(3.0, None), (1.0, None), (3.0, "8")])
+def test_ed_solve_mixed_meets_fp64_bars(monkeypatch, u, head):
+    # the mixed form on the grid-wide chain path (FP64 head, FP32 tail) against
+    # the FP64 oracle: |dE0|/|E0| <= 1e-10 and max|dG(iwn)| <= 1e-8
+    monkeypatch.setenv("DMFTED_BATCH_MAX_DIM", "0")
+    if head is not None:
+        monkeypatch.setenv("DMFTED_GF_HEAD64", head)
+    m = O.seeded_model(7, norb=1, nbath=9, u=u, beta=100.0)
+    s = solver_for(m, precision=dmfted.MIXED, lmats=1024, lreal=0)
+    s.ed_solve(m.bath_array(), sectors=[s.sector_index(5, 5)])
+    ref = O.solve_sector_t0(m, 5, 5, lmats=1024, lreal=0, nthreads=8)
+    assert abs(s.egs() - ref["e0"]) <= 1e-10 * abs(ref["e0"])
+    dg = np.abs(s.ed_get_gimp_matsubara()[0, 0, 0, 0] - ref["gmats"][0, 0]).max()
+    assert dg <= 1e-8, dg
+    s.close()
+
+
 def test_full_sector_scan_t0():
     # the reference scans every (nup, ndw) sector (ED_DIAG.f90:115)
     m = O.seeded_model(5, nbath=3, u=2.0)
