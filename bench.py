@@ -162,7 +162,8 @@ def finite_t_workload(dmfted, device, steps, warmup):
         out["fp64" if prec == dmfted.FP64 else "mixed"] = dict(
             ms_per_solve=statistics.median(ms), launches_per_solve=launches,
             states_kept=len(e), gf_chains=tm["hv_gf"] // NGF, diag_ms=tm["diag_ms"],
-            gf_ms=tm["gf_ms"], max_dG_vs_fp64=float(np.abs(g - ref_g).max()))
+            gf_ms=tm["gf_ms"], max_dG_vs_fp64=float(np.abs(g - ref_g).max()),
+            autotune=s.autotune_log())
         s.close()
     return out
 

@@ -611,6 +611,7 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         if (const char *e = getenv("DMFTED_HXV_KERNEL")) c->tune_hxv = atoi(e);
         if (const char *e = getenv("DMFTED_ELL_GROUP")) c->tune_ell_group = std::max(1, std::min(32, atoi(e)));
         if (const char *e = getenv("DMFTED_MIXED_TOL32")) c->mixed_tol32 = atof(e);
+        if (const char *e = getenv("DMFTED_AUTOTUNE")) c->autotune = atoi(e) != 0;
         if (const char *e = getenv("DMFTED_GF_HEAD64")) c->gf_head64 = std::max(0, atoi(e));
         if (const char *e = getenv("DMFTED_BATCH_MAX_DIM")) c->batch_max_dim = atoll(e);
         if (const char *e = getenv("DMFTED_BATCH_BUDGET_MB")) c->batch_budget = atoll(e) << 20;
@@ -1058,6 +1059,20 @@ int dmfted_time_hxv(dmfted_ctx *c, int32_t flags, int32_t warmup, int32_t reps, 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *ms = t / reps;
+    API_END
+}
+
+int dmfted_autotune_log(dmfted_ctx *c, char *buf, int32_t len, int32_t *needed) {
+    API_BEGIN
+    DM_REQUIRE(c && (buf || len == 0) && len >= 0, DMFTED_ERR_ARG, "bad argument");
+    std::string all;
+    for (const std::string &l : c->tune_log) all += l + "\n";
+    if (needed) *needed = (int32_t)all.size() + 1;
+    if (len > 0) {
+        const size_t n = std::min<size_t>(all.size(), (size_t)len - 1);
+        memcpy(buf, all.data(), n);
+        buf[n] = '\0';
+    }
     API_END
 }
 

@@ -23,6 +23,8 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <string>
 #include <vector>
 
 #include "internal.cuh"
@@ -776,6 +778,10 @@ static void launch_persistent(dmfted_ctx *c, void (*kern)(KArgs...), int CL, int
     at[0].val.clusterDim.z = 1;
     cfg.attrs = at;
     cfg.numAttrs = CL > 1 ? 1 : 0;
+    if (CL > 8) {
+        // 16 CTAs per cluster is beyond the portable size: opt in per kernel
+        DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
     int units = std::max(1, num_sms(c) / CL);
     if (CL > 1) {
         cfg.gridDim = dim3(units * CL);
@@ -799,7 +805,7 @@ static int eigs_cluster(const dmfted_ctx *c, int64_t dmax) {
     const int64_t per = c->batch_cluster_min;
     if (const char *e = getenv("DMFTED_BATCH_CLUSTER_EIGS")) {
         const int v = atoi(e);
-        if (v == 1 || v == 2 || v == 4 || v == 8) return v;
+        if (v == 1 || v == 2 || v == 4 || v == 8 || v == 16) return v;
     }
     return dmax >= 8 * per ? 8 : dmax >= 4 * per ? 4 : dmax >= 2 * per ? 2 : 1;
 }
@@ -810,13 +816,87 @@ static int chain_cluster(dmfted_ctx *c, int njobs, int64_t dmax) {
     const int64_t per = c->batch_cluster_min;
     if (const char *e = getenv("DMFTED_BATCH_CLUSTER_GF")) {
         const int v = atoi(e);
-        if (v == 1 || v == 2 || v == 4 || v == 8) return v;
+        if (v == 1 || v == 2 || v == 4 || v == 8 || v == 16) return v;
     }
     int cl = 1;
     while (cl < 8 && (int64_t)njobs * cl * 2 <= 2 * (int64_t)num_sms(c) &&
            dmax / (cl * 2) >= 2 * per)
         cl *= 2;
     return cl;
+}
+
+// Autotuner of the batched phases.  The cluster size of a phase (CTAs per
+// shared job) is picked per job-shape key -- precision, Fock space, hop-table
+// width (the nonzeros per row), largest job dimension and the job count's
+// power-of-two bucket (the state list grows over the first DMFT iterations)
+// -- by measurement.  The first phase with a new key runs once at the largest
+// candidate size untimed (pools reach their final size, caches warm), then
+// measures the candidates -- the fixed rule's size and its neighbours, half
+// and double, within 1..16 and giving every CTA of a shared job at least
+// batch_cluster_min states -- in two interleaved rounds, timed with CUDA
+// events on the context's stream; each candidate's faster run counts (the
+// rounds cancel clock drift).  The rule's size is kept unless a candidate is
+// more than 3 % faster; the choice then serves every later phase with that
+// key.  The phase is left with the results of a run at the chosen size
+// (re-run if another size ran last).  An environment override of the size,
+// or DMFTED_AUTOTUNE=0, keeps the fixed rule.
+template <typename Run>
+static int tuned_cluster(dmfted_ctx *c, const char *kind, const char *override_env, int rule,
+                         int64_t njobs, int64_t dmax, int precision, Run run) {
+    if (!c->autotune || getenv(override_env)) {
+        run(rule);
+        return rule;
+    }
+    int bucket = 0;
+    while ((int64_t(1) << bucket) <= njobs) bucket++;
+    char key[256];
+    snprintf(key, sizeof(key), "%s prec=%d ns=%d norb=%d W=%d jobs<2^%d dmax=%lld", kind,
+             precision, c->ns, c->norb, c->W, bucket, (long long)dmax);
+    auto it = c->tune_choice.find(key);
+    if (it != c->tune_choice.end()) {
+        run(it->second);
+        return it->second;
+    }
+    std::vector<int> cand;
+    for (int cl : {rule / 2, rule, rule * 2})
+        if (cl == rule || (cl >= 1 && cl <= 16 && (cl == 1 || dmax >= c->batch_cluster_min * cl)))
+            cand.push_back(cl);
+    run(cand.back());  // untimed: pools at their largest size, caches warm
+    cudaEvent_t e0, e1;
+    DM_CUDA(cudaEventCreate(&e0));
+    DM_CUDA(cudaEventCreate(&e1));
+    std::vector<float> t(cand.size(), 1e30f);
+    for (int round = 0; round < 2; round++)
+        for (size_t i = 0; i < cand.size(); i++) {
+            DM_CUDA(cudaEventRecord(e0, c->stream));
+            run(cand[i]);
+            DM_CUDA(cudaEventRecord(e1, c->stream));
+            DM_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            DM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            t[i] = std::min(t[i], ms);
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::string log = std::string(key) + " ->";
+    for (size_t i = 0; i < cand.size(); i++) {
+        char b[64];
+        snprintf(b, sizeof(b), " CL%d=%.3fms", cand[i], t[i]);
+        log += b;
+    }
+    int best = rule;
+    float tbest = 0.97f * t[std::find(cand.begin(), cand.end(), rule) - cand.begin()];
+    for (size_t i = 0; i < cand.size(); i++)
+        if (t[i] < tbest) {
+            tbest = t[i];
+            best = cand[i];
+        }
+    if (best != cand.back()) run(best);
+    char b[64];
+    snprintf(b, sizeof(b), " chosen CL%d (rule CL%d)", best, rule);
+    c->tune_log.push_back(log + b);
+    c->tune_choice[key] = best;
+    return best;
 }
 
 // One launch over the jobs [j0, j1) of the queue; the job table holds the
@@ -844,6 +924,7 @@ template <typename T>
 static void run_batch_eigs_cl(dmfted_ctx *c, int CL, int j0, int nbig, int j1, int wave,
                               double tol) {
     switch (CL) {
+        case 16: run_batch_eigs<T, 16>(c, j0, nbig, j1, wave, tol); break;
         case 8: run_batch_eigs<T, 8>(c, j0, nbig, j1, wave, tol); break;
         case 4: run_batch_eigs<T, 4>(c, j0, nbig, j1, wave, tol); break;
         case 2: run_batch_eigs<T, 2>(c, j0, nbig, j1, wave, tol); break;
@@ -852,16 +933,11 @@ static void run_batch_eigs_cl(dmfted_ctx *c, int CL, int j0, int nbig, int j1, i
 }
 
 
-void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, int precision,
-                std::vector<BatchEig> &res) {
+static void batch_eigs_cl(dmfted_ctx *c, const std::vector<int> &list, int precision,
+                          std::vector<BatchEig> &res, int CL) {
     const dmfted_params &p = c->p;
     res.assign(list.size(), BatchEig());
     const bool fp64 = precision == DMFTED_FP64;
-    int64_t dmax = 0;
-    for (int is : list)
-        if (c->neigen_sector[is - 1] > 0 && sector_view(c, is).dim <= c->batch_max_dim)
-            dmax = std::max(dmax, sector_view(c, is).dim);
-    const int CL = eigs_cluster(c, dmax);
     const size_t es = fp64 ? sizeof(double) : sizeof(float);
     std::vector<EigsJob> jobs;
     std::vector<int> where;  // list index of each job
@@ -963,6 +1039,18 @@ void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, int precision,
     }
 }
 
+void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, int precision,
+                std::vector<BatchEig> &res) {
+    int64_t dmax = 0, nj = 0;
+    for (int is : list)
+        if (c->neigen_sector[is - 1] > 0 && sector_view(c, is).dim <= c->batch_max_dim) {
+            dmax = std::max(dmax, sector_view(c, is).dim);
+            nj++;
+        }
+    tuned_cluster(c, "eigs", "DMFTED_BATCH_CLUSTER_EIGS", eigs_cluster(c, dmax), nj, dmax,
+                  precision, [&](int cl) { batch_eigs_cl(c, list, precision, res, cl); });
+}
+
 template <typename T, int CL>
 static void run_batch_chains(dmfted_ctx *c, int nbig, int nj, double *alpha, double *beta,
                              int *nsteps, double *norm2, int64_t nslots) {
@@ -988,6 +1076,7 @@ static void run_batch_chains_cl(dmfted_ctx *c, int CL, const std::vector<ChainJo
            c->binom[jobs[nbig].tnup] * c->binom[jobs[nbig].tndw] >= c->batch_cluster_min * CL)
         nbig++;
     switch (CL) {
+        case 16: run_batch_chains<T, 16>(c, nbig, nj, alpha, beta, nsteps, norm2, nslots); break;
         case 8: run_batch_chains<T, 8>(c, nbig, nj, alpha, beta, nsteps, norm2, nslots); break;
         case 4: run_batch_chains<T, 4>(c, nbig, nj, alpha, beta, nsteps, norm2, nslots); break;
         case 2: run_batch_chains<T, 2>(c, nbig, nj, alpha, beta, nsteps, norm2, nslots); break;
@@ -1044,9 +1133,12 @@ void batch_chains_gf(dmfted_ctx *c, const std::vector<ChainRec> &recs, int preci
         int64_t dmax = 0;
         for (const ChainJob &J : jobs)
             dmax = std::max<int64_t>(dmax, c->binom[J.tnup] * c->binom[J.tndw]);
-        const int CL = chain_cluster(c, (int)jobs.size(), dmax);
-        if (fp64) run_batch_chains_cl<double>(c, CL, jobs, alpha, beta, nsteps, norm2, nrec);
-        else run_batch_chains_cl<float>(c, CL, jobs, alpha, beta, nsteps, norm2, nrec);
+        tuned_cluster(c, "chains", "DMFTED_BATCH_CLUSTER_GF",
+                      chain_cluster(c, (int)jobs.size(), dmax), (int64_t)jobs.size(), dmax,
+                      fp64 ? DMFTED_FP64 : DMFTED_MIXED, [&](int cl) {
+                          if (fp64) run_batch_chains_cl<double>(c, cl, jobs, alpha, beta, nsteps, norm2, nrec);
+                          else run_batch_chains_cl<float>(c, cl, jobs, alpha, beta, nsteps, norm2, nrec);
+                      });
     }
     // chains too large for one CTA: the grid-wide recurrence, in order
     for (int i = 0; i < nrec; i++) {

@@ -23,6 +23,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -228,6 +229,11 @@ struct dmfted_ctx {
     int64_t batch_max_dim = 1 << 17;
     int64_t batch_budget = 0;             // bytes of Krylov bases per launch (0: a third of free)
     int64_t batch_cluster_min = 1024;     // states per CTA for a job shared by a cluster
+    // autotuner of the batched launches (batch.cu): cluster size per job-shape
+    // key, measured on first use; the log keeps every measurement
+    bool autotune = true;
+    std::map<std::string, int> tune_choice;
+    std::vector<std::string> tune_log;
     bool ft_eigs_fp32 = false;            // finite-T eigenpairs with FP32 vectors (measurement only)
     bool batch_chains_fp32 = false;       // batched GF chains in FP32 in the mixed form (measurement only)
     dmfted::DBuf<uint8_t> bwork;          // Krylov bases / chain vectors of the jobs

@@ -96,6 +96,7 @@ EXPORTS = {
                                                  _vp, _vp, _vp, _vp]),
     "dmfted_time_hxv": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp]),
     "dmfted_hxv_timing": (C.c_int, [_vp, C.c_int32]),
+    "dmfted_autotune_log": (C.c_int, [_vp, C.c_char_p, C.c_int32, C.POINTER(C.c_int32)]),
     "dmfted_get_hxv_timing": (C.c_int, [_vp, _dp, _lp, _dp]),
     "dmfted_get_timings": (C.c_int, [_vp, _dp, _lp]),
     "dmfted_launch_count": (C.c_int, [_vp, _lp, C.c_int32]),
@@ -368,6 +369,14 @@ class EDSolver:
         ms, n, b = C.c_double(), C.c_int64(), C.c_double()
         _ck(lib().dmfted_get_hxv_timing(self.ctx, C.byref(ms), C.byref(n), C.byref(b)))
         return dict(ms=ms.value, launches=n.value, bytes=b.value)
+
+    def autotune_log(self):
+        """Lines of the autotuner: job-shape key, time per cluster size, choice."""
+        need = C.c_int32()
+        _ck(lib().dmfted_autotune_log(self.ctx, None, 0, C.byref(need)))
+        buf = C.create_string_buffer(need.value)
+        _ck(lib().dmfted_autotune_log(self.ctx, buf, need.value, None))
+        return [l for l in buf.value.decode().split("\n") if l]
 
     def launch_count(self, reset=False):
         n = C.c_int64()

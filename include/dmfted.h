@@ -252,6 +252,13 @@ int dmfted_time_hxv(dmfted_ctx *ctx, int32_t flags, int32_t warmup, int32_t reps
  * No counterpart in the reference (measurement support). */
 int dmfted_hxv_timing(dmfted_ctx *ctx, int32_t on);
 
+/* The autotuner's measurements so far, one line per job-shape key of a
+ * batched phase: the key, the device time of each candidate cluster size and
+ * the size kept.  Written into buf (NUL-terminated, truncated to len bytes);
+ * *needed (may be NULL) receives the full length + 1.  No counterpart in the
+ * reference (measurement support). */
+int dmfted_autotune_log(dmfted_ctx *ctx, char *buf, int32_t len, int32_t *needed);
+
 /* Totals of the timed H*v launches since the last call (then reset): device
  * milliseconds, launch count and algorithmic bytes (read x, read v_prev for
  * the fused step, write y, at the vector precision).  Waits for the stream. */

@@ -92,7 +92,7 @@ def test_batch_mixed_precision_close_to_fp64():
     assert np.abs(f32["g"] - f64["g"]).max() <= 1e-4
 
 
-@pytest.mark.parametrize("cl_eigs,cl_gf", [("2", "2"), ("4", "8"), ("8", "4")])
+@pytest.mark.parametrize("cl_eigs,cl_gf", [("2", "2"), ("4", "8"), ("8", "4"), ("16", "16")])
 def test_batch_clusters_match_single_cta(cl_eigs, cl_gf):
     # one job shared by a cluster of CTAs (interleaved elements, sums folded
     # through distributed shared memory) gives the single-CTA result
@@ -102,3 +102,43 @@ def test_batch_clusters_match_single_cta(cl_eigs, cl_gf):
     one = solve(m, dict(base, DMFTED_BATCH_CLUSTER_EIGS="1", DMFTED_BATCH_CLUSTER_GF="1"))
     many = solve(m, dict(base, DMFTED_BATCH_CLUSTER_EIGS=cl_eigs, DMFTED_BATCH_CLUSTER_GF=cl_gf))
     agree(many, one, tol_e=1e-12, tol_g=1e-11)
+
+
+def test_batch_autotune_picks_measured_cluster_and_agrees():
+    # the autotuner times candidate cluster sizes of each batched phase on
+    # first use of a job shape, keeps the fastest, and its results agree
+    # with the fixed rule's; later solves of the same shapes re-use the
+    # choices (no job shape is measured twice)
+    m = split_model(25, 2, 2, beta=50.0, ust=2.0, jh=0.5)
+    env = {"DMFTED_BATCH_MAX_DIM": str(1 << 17), "DMFTED_BATCH_CLUSTER_MIN": "8"}
+    rule = solve(m, dict(env, DMFTED_AUTOTUNE="0"))
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        p = dmfted.default_params(norb=m.norb, nbath=m.nbath, nspin=m.nspin, uloc=list(m.uloc),
+                                  ust=m.ust, jh=m.jh, beta=m.beta, lmats=256, lreal=0,
+                                  lanc_nstates_total=16)
+        s = dmfted.EDSolver(p)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    s.ed_solve(m.bath_array())
+    log = s.autotune_log()
+    assert any(l.startswith("eigs ") and "chosen CL" in l for l in log), log
+    assert any(l.startswith("chains ") and "chosen CL" in l for l in log), log
+    for line in log:  # the fixed rule's size is always among the measured candidates
+        size = line.split("(rule ")[1].rstrip(")")
+        assert f" {size}=" in line, line
+    e, secs, z = s.eigenspace()
+    g = s.ed_get_gimp_matsubara()
+    assert np.array_equal(secs, rule["secs"])
+    assert np.allclose(e, rule["e"], rtol=0, atol=1e-10 * max(1.0, np.abs(rule["e"]).max()))
+    assert np.abs(g - rule["g"]).max() <= 1e-9
+    s.ed_solve(m.bath_array())
+    s.ed_solve(m.bath_array())
+    keys = [l.split(" ->")[0] for l in s.autotune_log()]
+    assert len(keys) == len(set(keys))  # each job shape measured once
+    s.close()
