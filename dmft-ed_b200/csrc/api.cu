@@ -354,6 +354,27 @@ static void ed_analysis_finite_t(dmfted_ctx *c) {
 //   observables_impurity (n, docc, ED_OBSERVABLES.f90:113-160)
 //   buildgf_impurity -> lanc_build_gf_normal_c per (iorb, ispin)
 //   (build_gf_normal.f90:4-16,71-180) -> get_sigma_normal.
+
+// Thermal average of the raw accumulators over the kept states, with the
+// Boltzmann weights of ED_OBSERVABLES.f90:128-129 (T=0: 1/Z over the ground
+// states); hops: include the hop terms of the Hellmann-Feynman gradient.
+static std::vector<double> thermal_observables(dmfted_ctx *c, bool hops) {
+    const int na = obs_count(c);
+    c->obs_d.alloc(na);
+    std::vector<double> acc(na, 0.0), one(na);
+    for (auto &st : c->states) {
+        SectorView s = sector_view(c, st.isector);
+        const double peso =
+            (c->finite_t ? std::exp(-c->p.beta * (st.e - c->egs)) : 1.0) / c->zeta;
+        observables_raw(c, s, c->states64.p + st.off, c->obs_d.p, hops);
+        DM_CUDA(cudaMemcpyAsync(one.data(), c->obs_d.p, na * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+        DM_CUDA(cudaStreamSynchronize(c->stream));
+        for (int q = 0; q < na; q++) acc[q] += peso * one[q];
+    }
+    return acc;
+}
+
 static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list) {
     DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "ed_solve: bath not set");
     const dmfted_params &p = c->p;
@@ -406,20 +427,7 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     }
     DM_CUDA(cudaEventRecord(ev[1], c->stream));
     // ---- observables -------------------------------------------------------
-    const int na = obs_count(c);
-    c->obs_d.alloc(na);
-    std::vector<double> acc(na, 0.0), one(na);
-    for (auto &st : c->states) {
-        SectorView s = sector_view(c, st.isector);
-        // ED_OBSERVABLES.f90:128-129
-        const double peso =
-            (c->finite_t ? std::exp(-p.beta * (st.e - c->egs)) : 1.0) / c->zeta;
-        observables_raw(c, s, c->states64.p + st.off, c->obs_d.p);
-        DM_CUDA(cudaMemcpyAsync(one.data(), c->obs_d.p, na * sizeof(double), cudaMemcpyDeviceToHost,
-                                c->stream));
-        DM_CUDA(cudaStreamSynchronize(c->stream));
-        for (int q = 0; q < na; q++) acc[q] += peso * one[q];
-    }
+    const std::vector<double> acc = thermal_observables(c, false);
     const int no = c->norb;
     c->obs.assign(5 * no, 0.0);
     for (int a = 0; a < no; a++) {
@@ -431,6 +439,7 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
         c->obs[4 * no + a] = nu - nd;  // magz
     }
     c->hf_terms.assign(acc.begin() + 3 * no, acc.end());
+    c->hf_hops = false;  // the hop terms are computed when the gradient is asked for
     DM_CUDA(cudaEventRecord(ev[2], c->stream));
     // ---- Green's functions ---------------------------------------------------
     const size_t gsz = (size_t)c->nspin * no;
@@ -954,6 +963,12 @@ int dmfted_hf_gradient(dmfted_ctx *c, double *grad, int32_t nb) {
     const int no = c->norb, nbth = c->nbath, ns = c->nspin;
     DM_REQUIRE(nb == 2 * ns * no * nbth, DMFTED_ERR_ARG, "hf_gradient: wrong bath dimensions");
     const int pv = no * nbth;
+    if (!c->hf_hops) {
+        DM_CUDA(cudaSetDevice(c->device));
+        const std::vector<double> acc = thermal_observables(c, true);
+        c->hf_terms.assign(acc.begin() + 3 * no, acc.end());
+        c->hf_hops = true;
+    }
     const double *nk = c->hf_terms.data();           // [2][norb][nbath]
     const double *hop = c->hf_terms.data() + 2 * pv;  // [2][norb][nbath]
     for (int is = 0; is < ns; is++)

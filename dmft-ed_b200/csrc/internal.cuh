@@ -222,6 +222,7 @@ struct dmfted_ctx {
     dmfted::DBuf<double> d_wm, d_wr;      // Matsubara / real-axis grids
     dmfted::DBuf<double> d_bath_e, d_bath_v, d_hloc_aa;  // [nspin][norb][nbath], [nspin][norb]
     dmfted::DBuf<double> obs_d;           // observable accumulators of one state
+    bool hf_hops = false;                 // hf_terms holds the hop expectations of the last solve
     dmfted::DBuf<double> eig_aux;         // Ritz values, vectors of T, coefficients, dots
     dmfted::DBuf<double> eigvecs;         // eigenvectors of one sector (Neigen x dim)
     // persistent work-queue path (batch.cu): sectors up to batch_max_dim
@@ -362,7 +363,8 @@ void gf_sigma(dmfted_ctx *c);  // impSmats/impSreal/impG0mats from impG*
 
 // ---- observables.cu --------------------------------------------------------
 int obs_count(const dmfted_ctx *c);
-void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, double *d_out);
+void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, double *d_out,
+                     bool hops);
 
 // ---- chi2.cu -------------------------------------------------------------
 void chi2_batch_device(dmfted_ctx *c, int nbatch, int nbath, int L, const double *a,

@@ -367,8 +367,16 @@ static LanczosResult gs_run(dmfted_ctx *c, const SectorView &s, double *psi, con
         c->launches++;
         launched = 1;
     }
+    // Checks fall on multiples of ncheck steps.  From the decay of the Ritz
+    // estimate between two checks the loop predicts the steps still needed
+    // (linear convergence) and skips checks for at most half of them, so the
+    // check that sees convergence is the one the fixed schedule would run,
+    // unless convergence more than doubles its pace.
+    int every = ncheck;
+    double est_prev = -1.0;
+    int at_prev = 0;
     while (launched < kmax) {
-        for (int j = 0; j < ncheck && launched < kmax; j++, launched++) {
+        for (int j = 0; j < every && launched < kmax; j++, launched++) {
             const int k = launched;
             T *x = basis + (size_t)k * ld;
             const T *xp = basis + (size_t)(k > 0 ? k - 1 : k) * ld;
@@ -378,9 +386,20 @@ static LanczosResult gs_run(dmfted_ctx *c, const SectorView &s, double *psi, con
         k_ritz_check<<<1, kRedThreads, ritz_smem(launched), c->stream>>>(lz, tol);
         DM_CHECK_LAUNCH();
         c->launches++;
+        double rz[2];
         DM_CUDA(cudaMemcpyAsync(hst, lz.status, sizeof(hst), cudaMemcpyDeviceToHost, c->stream));
+        DM_CUDA(cudaMemcpyAsync(rz, lz.ritz, sizeof(rz), cudaMemcpyDeviceToHost, c->stream));
         DM_CUDA(cudaStreamSynchronize(c->stream));
         if (hst[ST_DONE]) break;
+        every = ncheck;
+        const double target = tol * std::max(3.666852862501036e-11, std::fabs(rz[0]));
+        if (est_prev > 0.0 && rz[1] > 0.0 && rz[1] < est_prev && launched > at_prev) {
+            const double rate = std::log(est_prev / rz[1]) / (launched - at_prev);  // per step
+            const double left = std::log(rz[1] / target) / rate;                   // steps to go
+            if (left > 2.0 * ncheck) every = ncheck * std::max(1, (int)(0.5 * left / ncheck));
+        }
+        est_prev = rz[1];
+        at_prev = launched;
     }
     if (kmax <= launched && !hst[ST_DONE] && !refine) {
         // (kmax reached inside the loop: the last check above already ran)

@@ -6,13 +6,21 @@
 //                                       (HxVimp_bath.f90)
 // with the normal bath stride Norb+(iorb-1)*Nbath+k (ED_SETUP.f90:445-462).
 //
-// One pass over the state vector.  Accumulators (NA of them) live in
-// per-thread shared-memory slots (no atomics), are folded per CTA in a fixed
-// order, and a second kernel folds the CTA partials with compensated sums,
-// so the result is reproducible bit for bit.
-//
 // Accumulator layout: [0,norb) n_up, [norb,2norb) n_dw, [2norb,3norb) docc,
 // then nk[s][a][k] (2*norb*nbath), then hop[s][a][k] (2*norb*nbath).
+//
+// Occupations (k_obs_occ, every solve): the state is the DimUp x DimDw matrix
+// psi[r, c], and every occupation is diagonal in one spin, so with
+// w = |psi|^2 they factor into row sums R_r = sum_c w and column sums
+// C_c = sum_r w:  n_up = sum_r R_r n(r), n_dw = sum_c C_c n(c), and
+// docc = sum_c n_dw(c) sum_r w n_up(r).  Per element: one square, one
+// shared-memory add (the thread's own rows) and Norb FMAs; the bit weights
+// are applied per row and per column.  Hop expectations (k_obs_hop) gather
+// psi at the hop targets; only the Hellmann-Feynman gradient needs them, so
+// they are computed when it is asked for.
+//
+// CTA partials are folded by a second kernel with compensated sums, in a
+// fixed order: the result is reproducible bit for bit.
 #include <algorithm>
 
 #include "hxv.cuh"
@@ -20,54 +28,112 @@
 namespace dmfted {
 
 constexpr int kObsThreads = 64;
+constexpr int kOccThreads = 256;
 
-__global__ void __launch_bounds__(kObsThreads) k_obs(HxvArgs<double> a, int nbath, const double *psi,
-                                                     int na, double *partials) {
-    extern __shared__ double slot[];  // [na][kObsThreads]
-    const int tid = threadIdx.x;
+__device__ __forceinline__ double block_sum_occ(double v, double *red) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int i = 0; i < nw; i++) t += red[i];  // every thread, same order
+    return t;
+}
+
+// Occupation accumulators [0, 3*norb + 2*norb*nbath) of one state; CTAs own
+// columns, threads own rows.  Dynamic shared memory: R[dimup], then the
+// CTA's accumulators.
+__global__ void __launch_bounds__(kOccThreads) k_obs_occ(HxvArgs<double> a, int nbath,
+                                                         const double *psi, int nocc,
+                                                         double *partials) {
+    extern __shared__ double occ_sm[];
+    __shared__ double red[kOccThreads / 32];
+    const int tid = threadIdx.x, bd = blockDim.x;
     const int norb = a.norb, pv = norb * nbath;
-    for (int q = 0; q < na; q++) slot[q * kObsThreads + tid] = 0.0;
-    const int off_nk = 3 * norb, off_hop = 3 * norb + 2 * pv;
+    const int64_t dimup = a.dimup;
+    double *R = occ_sm, *ca = occ_sm + dimup;
+    for (int64_t r = tid; r < dimup; r += bd) R[r] = 0.0;
+    for (int q = tid; q < nocc; q += bd) ca[q] = 0.0;
+    __syncthreads();
+    for (int64_t c = blockIdx.x; c < a.dimdw; c += gridDim.x) {
+        double sw = 0.0, sd[kMaxNorb] = {0.0, 0.0, 0.0};
+        for (int64_t r = tid; r < dimup; r += bd) {
+            const double x = psi[r + dimup * c];
+            const double w = x * x;
+            R[r] += w;
+            sw += w;
+            const uint32_t wu = a.wu[r];
+#pragma unroll
+            for (int o = 0; o < kMaxNorb; o++)
+                if (o < norb) sd[o] += (wu >> o) & 1u ? w : 0.0;
+        }
+        const double csum = block_sum_occ(sw, red);
+        double dsum[kMaxNorb];
+#pragma unroll
+        for (int o = 0; o < kMaxNorb; o++) dsum[o] = o < norb ? block_sum_occ(sd[o], red) : 0.0;
+        if (tid == 0) {
+            const uint32_t wd = a.wd[c];
+            for (int o = 0; o < norb; o++) {
+                const bool nd = (wd >> o) & 1u;
+                if (nd) {
+                    ca[norb + o] += csum;
+                    ca[2 * norb + o] += dsum[o];
+                }
+                for (int k = 0; k < nbath; k++)
+                    if ((wd >> (norb + o * nbath + k)) & 1u) ca[3 * norb + pv + o * nbath + k] += csum;
+            }
+        }
+    }
+    __syncthreads();
+    // row-side occupations from the row sums
+    for (int q = 0; q < norb + pv; q++) {
+        const int bit = q < norb ? q : norb + (q - norb);
+        double v = 0.0;
+        for (int64_t r = tid; r < dimup; r += bd)
+            if ((a.wu[r] >> bit) & 1u) v += R[r];
+        v = block_sum_occ(v, red);
+        if (tid == 0) ca[q < norb ? q : 3 * norb + (q - norb)] += v;
+    }
+    __syncthreads();
+    for (int q = tid; q < nocc; q += bd) {
+        partials[((int64_t)q * gridDim.x + blockIdx.x) * 2 + 0] = ca[q];
+        partials[((int64_t)q * gridDim.x + blockIdx.x) * 2 + 1] = 0.0;
+    }
+}
+
+// Hop accumulators [0, 2*norb*nbath) (the hop part of the layout) of one
+// state: per-thread shared-memory slots, gathers at the hop targets.
+__global__ void __launch_bounds__(kObsThreads) k_obs_hop(HxvArgs<double> a, int nbath,
+                                                         const double *psi, double *partials) {
+    extern __shared__ double slot[];  // [2*pv][kObsThreads]
+    const int tid = threadIdx.x;
+    const int norb = a.norb, pv = norb * nbath, nh = 2 * pv;
+    for (int q = 0; q < nh; q++) slot[q * kObsThreads + tid] = 0.0;
     const int64_t dimup = a.dimup;
     for (int64_t cidx = blockIdx.x; cidx < a.dimdw; cidx += gridDim.x) {
-        const uint32_t wd = a.wd[cidx];
         const int cd = a.cd[cidx];
         for (int64_t r = tid; r < dimup; r += kObsThreads) {
             const double x = psi[r + dimup * cidx];
-            const double w = x * x;
-            const uint32_t wu = a.wu[r];
-            for (int o = 0; o < norb; o++) {
-                const double nu = (wu >> o) & 1u, nd = (wd >> o) & 1u;
-                slot[o * kObsThreads + tid] += w * nu;
-                slot[(norb + o) * kObsThreads + tid] += w * nd;
-                slot[(2 * norb + o) * kObsThreads + tid] += w * nu * nd;
-            }
-            for (int o = 0; o < norb; o++)
-                for (int k = 0; k < nbath; k++) {
-                    const int ms = norb + o * nbath + k;
-                    const int p = o * nbath + k;
-                    slot[(off_nk + p) * kObsThreads + tid] += w * (double)((wu >> ms) & 1u);
-                    slot[(off_nk + pv + p) * kObsThreads + tid] += w * (double)((wd >> ms) & 1u);
-                }
             const int cu = a.cu[r];
             for (int e = 0; e < cu; e++) {
                 const uint32_t en = a.eu[(int64_t)e * dimup + r];
                 const int p = ell_par(en);
                 if (p >= pv) continue;
                 const double y = psi[ell_col(en) + dimup * cidx];
-                slot[(off_hop + p) * kObsThreads + tid] += ell_neg(en) ? -x * y : x * y;
+                slot[p * kObsThreads + tid] += ell_neg(en) ? -x * y : x * y;
             }
             for (int e = 0; e < cd; e++) {
                 const uint32_t en = a.ed[(int64_t)e * a.dimdw + cidx];
                 const int p = ell_par(en);
                 if (p >= pv) continue;
                 const double y = psi[r + dimup * (int64_t)ell_col(en)];
-                slot[(off_hop + pv + p) * kObsThreads + tid] += ell_neg(en) ? -x * y : x * y;
+                slot[(pv + p) * kObsThreads + tid] += ell_neg(en) ? -x * y : x * y;
             }
         }
     }
     __syncthreads();
-    for (int q = tid; q < na; q += kObsThreads) {
+    for (int q = tid; q < nh; q += kObsThreads) {
         CSum s;
         s.zero();
         for (int t = 0; t < kObsThreads; t++) s.add(slot[q * kObsThreads + t]);
@@ -89,24 +155,45 @@ __global__ void k_obs_fold(const double *partials, int nblocks, int na, double *
 
 int obs_count(const dmfted_ctx *c) { return 3 * c->norb + 4 * c->norb * c->nbath; }
 
-// Raw accumulators of one state (weight 1) into d_out[obs_count] (device).
-void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, double *d_out) {
+// Raw accumulators of one state (weight 1) into d_out[obs_count] (device):
+// the occupations, and the hop terms when hops is set (else zero).
+void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, double *d_out,
+                     bool hops) {
     HxvArgs<double> a = make_hxv_args<double>(c, s);
     const int na = obs_count(c);
-    const size_t smem = (size_t)na * kObsThreads * sizeof(double);
-    DM_REQUIRE(smem <= 200 * 1024, DMFTED_ERR_UNSUPPORTED, "too many bath levels for k_obs");
-    static bool attr = false;
-    if (!attr) {
-        DM_CUDA(cudaFuncSetAttribute(k_obs, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr = true;
+    const int pv = c->norb * c->nbath, nocc = 3 * c->norb + 2 * pv;
+    const size_t smem = ((size_t)a.dimup + nocc) * sizeof(double);
+    DM_REQUIRE(smem <= 200 * 1024, DMFTED_ERR_UNSUPPORTED, "sector rows too long for k_obs_occ");
+    static bool attr[64] = {false};
+    if (!attr[c->device & 63]) {
+        DM_CUDA(cudaFuncSetAttribute(k_obs_occ, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
+        DM_CUDA(cudaFuncSetAttribute(k_obs_hop, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     200 * 1024));
+        attr[c->device & 63] = true;
     }
-    const int occ = std::max(1, (int)((200 * 1024) / std::max<size_t>(smem, 1)));
-    const int grid = (int)std::min<int64_t>(s.dimdw, (int64_t)num_sms(c) * std::min(occ, 8));
+    const int grid = (int)std::min<int64_t>(s.dimdw, (int64_t)num_sms(c) * 2);
     DM_REQUIRE((int64_t)na * grid * 2 <= (int64_t)c->red_partials.n, DMFTED_ERR_UNSUPPORTED,
                "reduction scratch too small for the observables");
-    k_obs<<<grid, kObsThreads, smem, c->stream>>>(a, c->nbath, psi, na, c->red_partials.p);
+    k_obs_occ<<<grid, kOccThreads, smem, c->stream>>>(a, c->nbath, psi, nocc, c->red_partials.p);
     DM_CHECK_LAUNCH();
-    k_obs_fold<<<div_up(na, 128), 128, 0, c->stream>>>(c->red_partials.p, grid, na, d_out);
+    k_obs_fold<<<div_up(nocc, 128), 128, 0, c->stream>>>(c->red_partials.p, grid, nocc, d_out);
+    DM_CHECK_LAUNCH();
+    c->launches += 2;
+    if (!hops) {
+        DM_CUDA(cudaMemsetAsync(d_out + nocc, 0, (size_t)(na - nocc) * sizeof(double), c->stream));
+        return;
+    }
+    const size_t hsmem = (size_t)2 * pv * kObsThreads * sizeof(double);
+    DM_REQUIRE(hsmem <= 200 * 1024, DMFTED_ERR_UNSUPPORTED, "too many bath levels for k_obs_hop");
+    const int occ = std::max(1, (int)((200 * 1024) / std::max<size_t>(hsmem, 1)));
+    const int hgrid = (int)std::min<int64_t>(s.dimdw, (int64_t)num_sms(c) * std::min(occ, 8));
+    DM_REQUIRE((int64_t)2 * pv * hgrid * 2 <= (int64_t)c->red_partials.n, DMFTED_ERR_UNSUPPORTED,
+               "reduction scratch too small for the observables");
+    k_obs_hop<<<hgrid, kObsThreads, hsmem, c->stream>>>(a, c->nbath, psi, c->red_partials.p);
+    DM_CHECK_LAUNCH();
+    k_obs_fold<<<div_up(2 * pv, 128), 128, 0, c->stream>>>(c->red_partials.p, hgrid, 2 * pv,
+                                                            d_out + nocc);
     DM_CHECK_LAUNCH();
     c->launches += 2;
 }
