@@ -618,6 +618,7 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         c->device = p->device;
         if (const char *e = getenv("DMFTED_HXV_NC")) c->tune_nc = atoi(e);
         if (const char *e = getenv("DMFTED_HXV_KERNEL")) c->tune_hxv = atoi(e);
+        if (const char *e = getenv("DMFTED_HXV_OCC")) c->tune_occ = atoi(e);
         if (const char *e = getenv("DMFTED_ELL_GROUP")) c->tune_ell_group = std::max(1, std::min(32, atoi(e)));
         if (const char *e = getenv("DMFTED_MIXED_TOL32")) c->mixed_tol32 = atof(e);
         if (const char *e = getenv("DMFTED_AUTOTUNE")) c->autotune = atoi(e) != 0;

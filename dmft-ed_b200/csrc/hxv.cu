@@ -650,10 +650,11 @@ __global__ void __launch_bounds__(256, kRvBlocks) k_hxv_rv(const HxvArgs<T> a) {
 // KU, KD: hops per row / per column after padding (7 or 8).
 constexpr uint32_t kLeanZero = 255u;
 
-// MODE 0: plain product; 1: fused Lanczos step (u and its alpha).
-template <typename T, int KU, int KD, int MODE>
-__global__ void __launch_bounds__(256, kRvBlocks) k_hxv_lean(const HxvArgs<T> a,
-                                                           const uint32_t *__restrict__ eux) {
+// MODE 0: plain product; 1: fused Lanczos step (u and its alpha).  MB: CTAs
+// of 256 threads per SM the register budget is set for.
+template <typename T, int KU, int KD, int MODE, int MB = kRvBlocks>
+__global__ void __launch_bounds__(256, MB) k_hxv_lean(const HxvArgs<T> a,
+                                                    const uint32_t *__restrict__ eux) {
     constexpr bool LZ = MODE >= 1;
     constexpr int NC = 16 / sizeof(T);
     constexpr int NV = 16 / sizeof(T);
@@ -1015,9 +1016,9 @@ static void launch_rv(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int n
     c->launches++;
 }
 
-template <typename T, int KU, int KD, int MODE>
-static void launch_lean_k(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
-    auto kern = k_hxv_lean<T, KU, KD, MODE>;
+template <typename T, int KU, int KD, int MODE, int MB>
+static void launch_lean_mb(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
+    auto kern = k_hxv_lean<T, KU, KD, MODE, MB>;
     static bool attr_set[64] = {false};
     if (!attr_set[c->device & 63]) {
         DM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1028,6 +1029,15 @@ static void launch_lean_k(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, i
     kern<<<grid, g.threads, g.smem, c->stream>>>(a, a.eux);
     DM_CHECK_LAUNCH();
     c->launches++;
+}
+
+// Three CTAs per SM (register cap 80, a few bytes of spills) measured 5-9 %
+// faster than two (128 registers) on the Ns=14 sectors in both precisions:
+// latency hiding pays more than the registers.  DMFTED_HXV_OCC=2 keeps two.
+template <typename T, int KU, int KD, int MODE>
+static void launch_lean_k(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int nvec) {
+    if (c->tune_occ == 2) launch_lean_mb<T, KU, KD, MODE, kRvBlocks>(c, a, g, nvec);
+    else launch_lean_mb<T, KU, KD, MODE, 3>(c, a, g, nvec);
 }
 
 // Hop counts padded to 7 or 8 (rows and columns independently).

@@ -218,6 +218,7 @@ struct dmfted_ctx {
     int gf_head64 = 20;                   // leading FP64 steps of a mixed-form GF chain
     int tune_nc = 0;                      // H*v columns per CTA override (0 = automatic)
     int tune_hxv = 0;                     // H*v kernel: 0 automatic, 1 k_hxv, 2 k_hxv_rv
+    int tune_occ = 3;                     // k_hxv_lean CTAs per SM (3: 80 registers; 2: 128)
     int tune_ell_group = 0;               // lanes per hop-table balance group (0: 8)
     dmfted::DBuf<double> d_wm, d_wr;      // Matsubara / real-axis grids
     dmfted::DBuf<double> d_bath_e, d_bath_v, d_hloc_aa;  // [nspin][norb][nbath], [nspin][norb]
