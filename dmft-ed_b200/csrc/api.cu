@@ -934,6 +934,28 @@ int dmfted_get_observables(dmfted_ctx *c, double *dens, double *dens_up, double 
     API_END
 }
 
+int dmfted_get_neigen(dmfted_ctx *c, int32_t *neigen, int32_t nsectors, int32_t *nstates_total) {
+    API_BEGIN
+    DM_REQUIRE(c && neigen && nstates_total, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(nsectors == c->nsectors, DMFTED_ERR_ARG, "get_neigen: wrong sector count");
+    for (int i = 0; i < nsectors; i++) neigen[i] = c->neigen_sector[i];
+    *nstates_total = c->nstates_total;
+    API_END
+}
+
+int dmfted_set_neigen(dmfted_ctx *c, const int32_t *neigen, int32_t nsectors,
+                      int32_t nstates_total) {
+    API_BEGIN
+    DM_REQUIRE(c && neigen, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(nsectors == c->nsectors, DMFTED_ERR_ARG, "set_neigen: wrong sector count");
+    DM_REQUIRE(nstates_total >= 1, DMFTED_ERR_ARG, "set_neigen: lanc_nstates_total < 1");
+    for (int i = 0; i < nsectors; i++)
+        DM_REQUIRE(neigen[i] >= 1, DMFTED_ERR_ARG, "set_neigen: neigen_sector entry < 1");
+    for (int i = 0; i < nsectors; i++) c->neigen_sector[i] = neigen[i];
+    c->nstates_total = nstates_total;
+    API_END
+}
+
 int dmfted_get_eigenspace(dmfted_ctx *c, int32_t cap, double *energies, int32_t *sectors,
                           int32_t *nstates, double *zeta) {
     API_BEGIN

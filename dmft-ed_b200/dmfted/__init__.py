@@ -97,6 +97,8 @@ EXPORTS = {
     "dmfted_time_hxv": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp]),
     "dmfted_hxv_timing": (C.c_int, [_vp, C.c_int32]),
     "dmfted_autotune_log": (C.c_int, [_vp, C.c_char_p, C.c_int32, C.POINTER(C.c_int32)]),
+    "dmfted_get_neigen": (C.c_int, [_vp, _ip, C.c_int32, C.POINTER(C.c_int32)]),
+    "dmfted_set_neigen": (C.c_int, [_vp, _ip, C.c_int32, C.c_int32]),
     "dmfted_get_hxv_timing": (C.c_int, [_vp, _dp, _lp, _dp]),
     "dmfted_get_timings": (C.c_int, [_vp, _dp, _lp]),
     "dmfted_launch_count": (C.c_int, [_vp, _lp, C.c_int32]),
@@ -319,6 +321,17 @@ class EDSolver:
 
     def ed_get_mag(self):
         return self.observables()["magz"]
+
+    def get_neigen(self):
+        """neigen_sector(:) and lanc_nstates_total as the next solve will use them."""
+        arr = np.zeros(self.nsectors, np.int32)
+        tot = C.c_int32()
+        _ck(lib().dmfted_get_neigen(self.ctx, _p(arr, C.c_int32), arr.size, C.byref(tot)))
+        return arr, tot.value
+
+    def set_neigen(self, neigen, nstates_total):
+        arr = np.ascontiguousarray(neigen, np.int32)
+        _ck(lib().dmfted_set_neigen(self.ctx, _p(arr, C.c_int32), arr.size, int(nstates_total)))
 
     def eigenspace(self, cap=4096):
         e = np.zeros(cap)

@@ -211,6 +211,17 @@ int dmfted_get_eigenspace(dmfted_ctx *ctx, int32_t cap, double *energies, int32_
 /* Ground-state energy of the last solve. */
 int dmfted_get_egs(dmfted_ctx *ctx, double *egs);
 
+/* The eigenspace sizes that ed_diag/ed_analysis adapt from one solve to the
+ * next: neigen_sector(1:Nsectors) and lanc_nstates_total
+ * (ED_DIAG.f90:248-398).  The lattice solve keeps one copy per inequivalent
+ * site and swaps it in and out of the single impurity context, as
+ * ed_solve_lattice does with neigen_sectorii / neigen_totalii
+ * (ED_MAIN.f90:419-423,597-611,655-656).  nsectors must equal the context's
+ * sector count ((Ns+1)^2); set rejects non-positive entries. */
+int dmfted_get_neigen(dmfted_ctx *ctx, int32_t *neigen, int32_t nsectors, int32_t *nstates_total);
+int dmfted_set_neigen(dmfted_ctx *ctx, const int32_t *neigen, int32_t nsectors,
+                      int32_t nstates_total);
+
 /* ---- gradients -----------------------------------------------------------
  * Hellmann-Feynman gradient of the thermal energy of the last solve with
  * respect to the user bath array (same layout and length as the bath):
