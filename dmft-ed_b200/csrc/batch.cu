@@ -414,10 +414,27 @@ __host__ __device__ inline int64_t eigs_aux_per_cta(int neigen, int kmax) {
 // each), the reorthogonalisation coefficients and the Ritz work space.
 constexpr int kDpart = 2 * (kEigsMaxSteps + 2);  // reorthogonalisation partials (doubles)
 static_assert(kDpart >= 2 * 32 * kEigsChunk, "partials of sliced groups");
+__host__ __device__ inline size_t eigs_ritz_doubles() {
+    return (ritz_smem(kEigsMaxSteps) + sizeof(double) - 1) / sizeof(double);
+}
 __host__ __device__ inline size_t eigs_smem() {
     return (size_t)4 * (kEigsMaxSteps + 2) * sizeof(double) + kDpart * sizeof(double) +
-           ritz_smem(kEigsMaxSteps);
+           eigs_ritz_doubles() * sizeof(double) + 3 * (size_t)(kEigsMaxSteps + 2) * sizeof(double);
 }
+
+// Partial reorthogonalisation (Simon, "The Lanczos algorithm with partial
+// reorthogonalization", Math. Comp. 42 (1984)): the level of orthogonality
+// w_{k+1,j} = <v_{k+1}, v_j> is estimated by the recurrence that the Lanczos
+// relation implies,
+//   b_{k+1} w_{k+1,j} = b_{j+1} w_{k,j+1} + (a_j - a_k) w_{k,j} + b_j w_{k,j-1}
+//                       - b_k w_{k-1,j}   (+ a rounding term),
+// and the new vector is reorthogonalised against the whole basis only when
+// max_j |w_{k+1,j}| exceeds sqrt(eps), and then the next vector as well.
+// Semi-orthogonality (|w| <= sqrt(eps)) keeps the Ritz values accurate to
+// O(eps |H|) and prevents spurious copies of converged eigenvalues; the
+// Ritz vectors are accurate to their residual estimates.  A full pass every
+// kProEvery steps bounds any error of the estimate.
+constexpr int kProEvery = 32;
 
 // Gram-Schmidt coefficients scf[j] = <v_j, y> scale_j, v_j = scale_j B_j,
 // for j < nv, over the job's elements.  The warps split into groups of
@@ -527,6 +544,12 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
     double *sal = dyn, *sbe = sal + (kEigsMaxSteps + 2), *ssc = sbe + (kEigsMaxSteps + 2);
     double *scf = ssc + (kEigsMaxSteps + 2), *dpart = scf + (kEigsMaxSteps + 2);
     double *rwork = dpart + kDpart;
+    // orthogonality estimates w_{k-1,.}, w_{k,.}, w_{k+1,.} (rotated)
+    double *om0 = rwork + eigs_ritz_doubles(), *om1 = om0 + (kEigsMaxSteps + 2),
+           *om2 = om1 + (kEigsMaxSteps + 2);
+    const double eps = sizeof(T) == 8 ? 1.1102230246251565e-16 : 5.9604644775390625e-8;
+    const double sqeps = sqrt(eps);
+    __shared__ double s_omax;
     const int ni = 1 << tb.norb;
     const int tid = threadIdx.x, bd = blockDim.x;
     const int rank = cta_rank<CL>();
@@ -561,6 +584,13 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
         sbe[0] = 0.0;
     }
     __syncthreads();
+    if (tid == 0) {
+        om1[0] = 1.0;  // w_{0,0}
+        s_omax = 0.0;
+    }
+    double anorm = 0.0;  // running Gershgorin bound of |T|, every thread
+    bool force = false;  // reorthogonalise this vector too (the one after a triggered pass)
+    __syncthreads();
     int n = 0;
     bool brk = false;
     for (int k = 0; k < J.kmax; k++) {
@@ -589,16 +619,62 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
         }
         job_sum<CL, 1>(a1, sm, tot);
         double wn = sqrt(tot[0]), bn = wn;
-        // full reorthogonalisation by classical Gram-Schmidt, repeated
-        // once when the first pass removed much of the vector (the DGKS
-        // test of ARPACK's dsaitr, |w'| < 0.717 |w|)
-        for (int pass = 0; pass < 2; pass++) {
-            reorth_dots<T, CL>(B, ld, k + 1, y, dim, dpart, scf, ssc);
-            a1[0] = reorth_update<T, CL>(B, ld, k + 1, y, dim, scf);
-            job_sum<CL, 1>(a1, sm, tot);
-            bn = sqrt(tot[0]);
-            if (bn >= kDgks * wn) break;
-            wn = bn;
+        anorm = fmax(anorm, fabs(ak) + sbe[k] + wn);
+        // orthogonality estimate of the new vector against v_0..v_{k-1}
+        // (identical in every CTA of a cluster: same scalars, same order)
+        bool reorth = force || (k % kProEvery) == kProEvery - 1 || !(wn > 0.0);
+        if (!reorth && k > 0) {
+            const double inv = 1.0 / wn, rnd = 2.0 * eps * anorm * inv;
+            double mx = 0.0;
+            for (int j = tid; j < k; j += bd) {
+                double t = sbe[j + 1] * om1[j + 1] + (sal[j] - ak) * om1[j] - sbe[k] * om0[j];
+                if (j > 0) t += sbe[j] * om1[j - 1];
+                t = t * inv;
+                t += copysign(rnd, t);
+                om2[j] = t;
+                mx = fmax(mx, fabs(t));
+            }
+            // block maximum (every thread of the CTA)
+            for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if ((tid & 31) == 0) dpart[tid >> 5] = mx;
+            __syncthreads();
+            if (tid == 0) {
+                double m = 0.0;
+                for (int w = 0; w < (bd >> 5); w++) m = fmax(m, dpart[w]);
+                s_omax = m;
+            }
+            __syncthreads();
+            reorth = s_omax > sqeps;
+            __syncthreads();
+        }
+        const bool triggered = reorth && !force && (k % kProEvery) != kProEvery - 1;
+        if (reorth) {
+            // full reorthogonalisation by classical Gram-Schmidt, repeated
+            // once when the first pass removed much of the vector (the DGKS
+            // test of ARPACK's dsaitr, |w'| < 0.717 |w|)
+            for (int pass = 0; pass < 2; pass++) {
+                reorth_dots<T, CL>(B, ld, k + 1, y, dim, dpart, scf, ssc);
+                a1[0] = reorth_update<T, CL>(B, ld, k + 1, y, dim, scf);
+                job_sum<CL, 1>(a1, sm, tot);
+                bn = sqrt(tot[0]);
+                if (bn >= kDgks * wn) break;
+                wn = bn;
+            }
+            for (int j = tid; j < k; j += bd) om2[j] = eps;
+        }
+        force = triggered;  // the vector after a triggered pass is reorthogonalised too
+        // w_{k+1,k}: local orthogonality (the alpha step), w_{k+1,k+1} = 1;
+        // then rotate the estimates
+        if (tid == 0) {
+            om2[k] = bn > 0.0 ? 2.0 * eps * anorm / bn : 0.0;
+            om2[k + 1] = 1.0;
+        }
+        __syncthreads();
+        {
+            double *t = om0;
+            om0 = om1;
+            om1 = om2;
+            om2 = t;
         }
         // b_{k+1} = |w|
         if (tid == 0) {
@@ -838,8 +914,8 @@ static int chain_cluster(dmfted_ctx *c, int njobs, int64_t dmax) {
 // rounds cancel clock drift).  The rule's size is kept unless a candidate is
 // more than 3 % faster; the choice then serves every later phase with that
 // key.  The phase is left with the results of a run at the chosen size
-// (re-run if another size ran last).  An environment override of the size,
-// or DMFTED_AUTOTUNE=0, keeps the fixed rule.
+// (re-run if another size ran last).  Enabled by DMFTED_AUTOTUNE=1; an
+// environment override of the size keeps the fixed rule.
 template <typename Run>
 static int tuned_cluster(dmfted_ctx *c, const char *kind, const char *override_env, int rule,
                          int64_t njobs, int64_t dmax, int precision, Run run) {

@@ -110,8 +110,9 @@ def test_batch_autotune_picks_measured_cluster_and_agrees():
     # with the fixed rule's; later solves of the same shapes re-use the
     # choices (no job shape is measured twice)
     m = split_model(25, 2, 2, beta=50.0, ust=2.0, jh=0.5)
-    env = {"DMFTED_BATCH_MAX_DIM": str(1 << 17), "DMFTED_BATCH_CLUSTER_MIN": "8"}
-    rule = solve(m, dict(env, DMFTED_AUTOTUNE="0"))
+    base = {"DMFTED_BATCH_MAX_DIM": str(1 << 17), "DMFTED_BATCH_CLUSTER_MIN": "8"}
+    rule = solve(m, dict(base, DMFTED_AUTOTUNE="0"))
+    env = dict(base, DMFTED_AUTOTUNE="1")  # the tuner is opt-in
     old = {k: os.environ.get(k) for k in env}
     os.environ.update(env)
     try:
