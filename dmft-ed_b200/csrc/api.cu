@@ -359,18 +359,24 @@ static void ed_analysis_finite_t(dmfted_ctx *c) {
 // Boltzmann weights of ED_OBSERVABLES.f90:128-129 (T=0: 1/Z over the ground
 // states); hops: include the hop terms of the Hellmann-Feynman gradient.
 static std::vector<double> thermal_observables(dmfted_ctx *c, bool hops) {
+    // every state's accumulators into its own slot, then one copy and one wait
     const int na = obs_count(c);
-    c->obs_d.alloc(na);
-    std::vector<double> acc(na, 0.0), one(na);
-    for (auto &st : c->states) {
-        SectorView s = sector_view(c, st.isector);
+    const size_t ns = c->states.size();
+    c->obs_d.alloc(std::max<size_t>(ns, 1) * na);
+    for (size_t i = 0; i < ns; i++) {
+        const auto &st = c->states[i];
+        observables_raw(c, sector_view(c, st.isector), c->states64.p + st.off,
+                        c->obs_d.p + i * na, hops);
+    }
+    std::vector<double> all(ns * na), acc(na, 0.0);
+    DM_CUDA(cudaMemcpyAsync(all.data(), c->obs_d.p, all.size() * sizeof(double),
+                            cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    for (size_t i = 0; i < ns; i++) {
+        const auto &st = c->states[i];
         const double peso =
             (c->finite_t ? std::exp(-c->p.beta * (st.e - c->egs)) : 1.0) / c->zeta;
-        observables_raw(c, s, c->states64.p + st.off, c->obs_d.p, hops);
-        DM_CUDA(cudaMemcpyAsync(one.data(), c->obs_d.p, na * sizeof(double), cudaMemcpyDeviceToHost,
-                                c->stream));
-        DM_CUDA(cudaStreamSynchronize(c->stream));
-        for (int q = 0; q < na; q++) acc[q] += peso * one[q];
+        for (int q = 0; q < na; q++) acc[q] += peso * all[i * na + q];
     }
     return acc;
 }

@@ -142,15 +142,22 @@ __global__ void __launch_bounds__(kObsThreads) k_obs_hop(HxvArgs<double> a, int 
     }
 }
 
-__global__ void k_obs_fold(const double *partials, int nblocks, int na, double *out) {
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < na; q += gridDim.x * blockDim.x) {
-        CSum s;
-        s.zero();
-        for (int b = 0; b < nblocks; b++)
-            s.merge(partials[((int64_t)q * nblocks + b) * 2 + 0],
-                    partials[((int64_t)q * nblocks + b) * 2 + 1]);
-        out[q] = s.value();
-    }
+// One warp per accumulator: the lanes stride over the CTA partials and fold
+// them with a fixed-order shuffle reduction (reproducible), so the partials'
+// loads are in flight together instead of one after the other.
+constexpr int kFoldWarps = 4;
+__global__ void __launch_bounds__(32 * kFoldWarps) k_obs_fold(const double *partials, int nblocks,
+                                                              int na, double *out) {
+    const int lane = threadIdx.x & 31;
+    const int q = blockIdx.x * kFoldWarps + (threadIdx.x >> 5);
+    if (q >= na) return;
+    CSum s;
+    s.zero();
+    for (int b = lane; b < nblocks; b += 32)
+        s.merge(partials[((int64_t)q * nblocks + b) * 2 + 0],
+                partials[((int64_t)q * nblocks + b) * 2 + 1]);
+    warp_reduce(s);
+    if (lane == 0) out[q] = s.value();
 }
 
 int obs_count(const dmfted_ctx *c) { return 3 * c->norb + 4 * c->norb * c->nbath; }
@@ -177,7 +184,8 @@ void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, doub
                "reduction scratch too small for the observables");
     k_obs_occ<<<grid, kOccThreads, smem, c->stream>>>(a, c->nbath, psi, nocc, c->red_partials.p);
     DM_CHECK_LAUNCH();
-    k_obs_fold<<<div_up(nocc, 128), 128, 0, c->stream>>>(c->red_partials.p, grid, nocc, d_out);
+    k_obs_fold<<<div_up(nocc, kFoldWarps), 32 * kFoldWarps, 0, c->stream>>>(c->red_partials.p,
+                                                                           grid, nocc, d_out);
     DM_CHECK_LAUNCH();
     c->launches += 2;
     if (!hops) {
@@ -192,8 +200,8 @@ void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, doub
                "reduction scratch too small for the observables");
     k_obs_hop<<<hgrid, kObsThreads, hsmem, c->stream>>>(a, c->nbath, psi, c->red_partials.p);
     DM_CHECK_LAUNCH();
-    k_obs_fold<<<div_up(2 * pv, 128), 128, 0, c->stream>>>(c->red_partials.p, hgrid, 2 * pv,
-                                                            d_out + nocc);
+    k_obs_fold<<<div_up(2 * pv, kFoldWarps), 32 * kFoldWarps, 0, c->stream>>>(
+        c->red_partials.p, hgrid, 2 * pv, d_out + nocc);
     DM_CHECK_LAUNCH();
     c->launches += 2;
 }
