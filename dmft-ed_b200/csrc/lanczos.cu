@@ -559,13 +559,80 @@ void lanczos_chain_fixed(dmfted_ctx *c, const SectorView &s, const double *v0, d
 // eigenvalue.
 namespace dmfted {
 
-// d_i = <s_i, w> for the nv stored vectors; one CTA per basis vector.
+// Partial reorthogonalisation of the grid-wide eigensolve (the batched
+// solver's rule, batch.cu): after the update of step k, one CTA advances the
+// orthogonality estimates w_{k+1,j} = <v_{k+1}, v_j> by Simon's recurrence
+//   b_{k+1} w_{k+1,j} = b_{j+1} w_{k,j+1} + (a_j - a_k) w_{k,j} + b_j w_{k,j-1}
+//                       - b_k w_{k-1,j}   (+ a rounding term)
+// and sets pf[0] when max_j |w_{k+1,j}| > sqrt(eps), when the previous step
+// triggered one (pf[1]) or every 32nd step; the reorthogonalisation and
+// renormalisation kernels of the step do nothing while pf[0] is clear.
+// om: three rotating rows of kLzMax+2 estimates; pf[2]: the running
+// Gershgorin bound of |T|.
+constexpr int kProRow = kLzMax + 2;
+__global__ void k_pro_init(double *om, double *pf) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        om[0] = 1.0;  // w_{0,0}
+        pf[0] = pf[1] = pf[2] = 0.0;
+    }
+}
+__global__ void __launch_bounds__(kRedThreads) k_pro(LanczosScalars lz, int k, double *om,
+                                                     double *pf, double eps) {
+    __shared__ double red[kRedThreads / 32];
+    __shared__ int s_need;
+    const int tid = threadIdx.x;
+    if (lz.status[ST_DONE] && lz.status[ST_STEPS] != k + 1) {
+        if (tid == 0) pf[0] = 0.0;  // the recurrence has ended: nothing to reorthogonalise
+        return;
+    }
+    const double *w0 = om + ((k + 2) % 3) * kProRow, *w1 = om + (k % 3) * kProRow;
+    double *w2 = om + ((k + 1) % 3) * kProRow;
+    const double ak = lz.alpha[k], bk = k > 0 ? lz.beta[k] : 0.0, bn = lz.beta[k + 1];
+    const double anorm = fmax(pf[2], fabs(ak) + bk + bn);
+    const bool force = pf[1] > 0.5, periodic = (k % 32) == 31;
+    bool need = force || periodic || !(bn > 0.0);
+    if (!need && k > 0) {
+        const double inv = 1.0 / bn, rnd = 2.0 * eps * anorm * inv;
+        double mx = 0.0;
+        for (int j = tid; j < k; j += blockDim.x) {
+            double t = lz.beta[j + 1] * w1[j + 1] + (lz.alpha[j] - ak) * w1[j] - bk * w0[j];
+            if (j > 0) t += lz.beta[j] * w1[j - 1];
+            t = t * inv;
+            t += copysign(rnd, t);
+            w2[j] = t;
+            mx = fmax(mx, fabs(t));
+        }
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if ((tid & 31) == 0) red[tid >> 5] = mx;
+        __syncthreads();
+        if (tid == 0) {
+            double m = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) m = fmax(m, red[w]);
+            s_need = m > sqrt(eps);
+        }
+        __syncthreads();
+        need = s_need != 0;
+    }
+    if (need)
+        for (int j = tid; j < k; j += blockDim.x) w2[j] = eps;
+    if (tid == 0) {
+        w2[k] = bn > 0.0 ? 2.0 * eps * anorm / bn : 0.0;
+        w2[k + 1] = 1.0;
+        pf[0] = need ? 1.0 : 0.0;
+        pf[1] = (need && !force && !periodic) ? 1.0 : 0.0;
+        pf[2] = anorm;
+    }
+}
+
+// d_i = <s_i, w> for the nv stored vectors; one CTA per basis vector.  pf:
+// the partial-reorthogonalisation flag (skip when pf[0] is clear), or null.
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_reorth_dots(const T *basis, int64_t ld, int nv,
-                                                             const T *w, int64_t n, double *dots) {
+                                                             const T *w, int64_t n, double *dots,
+                                                             const double *pf) {
     __shared__ double sm[64];
     const int i = blockIdx.x;
-    if (i >= nv) return;
+    if (i >= nv || (pf && pf[0] < 0.5)) return;
     CSum s;
     s.zero();
     const T *b = basis + (int64_t)i * ld;
@@ -578,8 +645,9 @@ __global__ void __launch_bounds__(kRedThreads) k_reorth_dots(const T *basis, int
 // w -= sum_i <v_i, w> v_i with v_i = sc_i s_i, i.e. coefficient d_i sc_i^2.
 template <typename T>
 __global__ void k_reorth_update(const T *basis, int64_t ld, int nv, const double *dots,
-                                const double *scale, T *w, int64_t n) {
+                                const double *scale, T *w, int64_t n, const double *pf) {
     __shared__ double cf[kLzMax + 8];
+    if (pf && pf[0] < 0.5) return;
     for (int i = threadIdx.x; i < nv; i += blockDim.x) cf[i] = dots[i] * scale[i] * scale[i];
     __syncthreads();
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
@@ -594,8 +662,9 @@ __global__ void k_reorth_update(const T *basis, int64_t ld, int nv, const double
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_lz_renorm(const T *w, int64_t n, LanczosScalars lz,
                                                            int k, double thr, double *partials,
-                                                           unsigned *counter) {
+                                                           unsigned *counter, const double *pf) {
     if (lz.status[ST_DONE] && lz.status[ST_STEPS] != k + 1) return;
+    if (pf && pf[0] < 0.5) return;  // not reorthogonalised: b_{k+1} of the update stands
     CSum s;
     s.zero();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -670,9 +739,11 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
         attr[c->device & 63] = true;
     }
     const int m = std::min<int64_t>(neigen, dim);
-    c->eig_aux.alloc((size_t)64 * 2 + (size_t)m * (kLzMax + 2) * 2 + kLzMax + 8);
+    c->eig_aux.alloc((size_t)64 * 2 + (size_t)m * (kLzMax + 2) * 2 + kLzMax + 8 + 3 * kProRow + 8);
     double *d_evals = c->eig_aux.p, *d_est = d_evals + 64, *d_Y = d_est + 64;
     double *d_coef = d_Y + (size_t)m * (kLzMax + 2), *d_dots = d_coef + (size_t)m * (kLzMax + 2);
+    double *d_om = d_dots + kLzMax + 8, *d_pf = d_om + 3 * kProRow;
+    const double eps = sizeof(T) == 8 ? 1.1102230246251565e-16 : 5.9604644775390625e-8;
     const int eg = ew_grid(c, dim);
     const int rg = red_grid(c, dim);
     c->s64b.alloc(dim);
@@ -680,8 +751,9 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
     k_convert<T, double><<<eg, 256, 0, c->stream>>>(c->s64b.p, basis, dim);
     k_lz_init<T><<<rg, kRedThreads, 0, c->stream>>>(basis, dim, lz, c->red_partials.p,
                                                      c->red_counter.p);
+    k_pro_init<<<1, 32, 0, c->stream>>>(d_om, d_pf);
     DM_CHECK_LAUNCH();
-    c->launches += 3;
+    c->launches += 4;
     int hst[8] = {0};
     int launched = 0;
     while (launched < kmax) {
@@ -692,16 +764,18 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
             T *y = basis + (size_t)(k + 1) * ld;
             hxv_lanczos_step<T>(c, s, x, xp, y, lz, k);
             launch_lz_update<T>(c, y, x, dim, lz, k, 1e-300);
+            k_pro<<<1, kRedThreads, 0, c->stream>>>(lz, k, d_om, d_pf, eps);
             for (int pass = 0; pass < 2; pass++) {
                 k_reorth_dots<T><<<k + 1, kRedThreads, 0, c->stream>>>(basis, (int64_t)ld, k + 1, y,
-                                                                       dim, d_dots);
+                                                                       dim, d_dots, d_pf);
                 k_reorth_update<T><<<eg, 256, 0, c->stream>>>(basis, (int64_t)ld, k + 1, d_dots,
-                                                             lz.scale, y, dim);
+                                                             lz.scale, y, dim, d_pf);
             }
             k_lz_renorm<T><<<rg, kRedThreads, 0, c->stream>>>(y, dim, lz, k, 1e-300,
-                                                              c->red_partials.p, c->red_counter.p);
+                                                              c->red_partials.p, c->red_counter.p,
+                                                              d_pf);
             DM_CHECK_LAUNCH();
-            c->launches += 5;
+            c->launches += 6;
         }
         k_ritz_multi<<<1, kRedThreads, ritz_smem(launched), c->stream>>>(lz, tol, m, d_evals, d_Y,
                                                                          d_est, 0);
