@@ -143,17 +143,36 @@ void hv_timer_end(dmfted_ctx *c, double bytes) {
     c->hv_ev_bytes.push_back(bytes);
 }
 
-// Folds the recorded pairs into the totals (waits for the stream).
+// Folds the recorded pairs into the totals (waits for both streams).  The
+// time is the union of the launches' intervals, all measured from the first
+// event: H*v launches of two concurrent chains overlap, and the union is the
+// device time during which any H*v ran (equal to the sum when they do not).
 static void hv_timer_collect(dmfted_ctx *c) {
     if (c->hv_ev.empty()) return;
     DM_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->stream2) DM_CUDA(cudaStreamSynchronize(c->stream2));
+    std::vector<std::pair<float, float>> iv;
+    const cudaEvent_t base = c->hv_ev.front().first;
     for (size_t i = 0; i < c->hv_ev_bytes.size(); i++) {
-        float ms = 0.f;
-        DM_CUDA(cudaEventElapsedTime(&ms, c->hv_ev[i].first, c->hv_ev[i].second));
-        c->hv_ms += ms;
+        float t0 = 0.f, t1 = 0.f;
+        DM_CUDA(cudaEventElapsedTime(&t0, base, c->hv_ev[i].first));
+        DM_CUDA(cudaEventElapsedTime(&t1, base, c->hv_ev[i].second));
+        iv.emplace_back(t0, t1);
         c->hv_bytes += c->hv_ev_bytes[i];
         c->hv_count++;
     }
+    std::sort(iv.begin(), iv.end());
+    double lo = -1.0, hi = -1.0;
+    for (auto &x : iv) {
+        if (x.first > hi) {
+            if (hi > lo) c->hv_ms += hi - lo;
+            lo = x.first;
+            hi = x.second;
+        } else {
+            hi = std::max<double>(hi, x.second);
+        }
+    }
+    if (hi > lo) c->hv_ms += hi - lo;
     for (auto &pr : c->hv_ev) {
         c->hv_ev_free.push_back(pr.first);
         c->hv_ev_free.push_back(pr.second);
@@ -628,6 +647,7 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         if (const char *e = getenv("DMFTED_ELL_GROUP")) c->tune_ell_group = std::max(1, std::min(32, atoi(e)));
         if (const char *e = getenv("DMFTED_MIXED_TOL32")) c->mixed_tol32 = atof(e);
         if (const char *e = getenv("DMFTED_AUTOTUNE")) c->autotune = atoi(e) != 0;
+        if (const char *e = getenv("DMFTED_CHAIN_LANES")) c->chain_lanes = atoi(e);
         if (const char *e = getenv("DMFTED_GF_HEAD64")) c->gf_head64 = std::max(0, atoi(e));
         if (const char *e = getenv("DMFTED_BATCH_MAX_DIM")) c->batch_max_dim = atoll(e);
         if (const char *e = getenv("DMFTED_BATCH_BUDGET_MB")) c->batch_budget = atoll(e) << 20;
@@ -655,6 +675,14 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         c->red_partials.alloc((size_t)2 * 64 * kMaxRedBlocks);
         c->red_counter.alloc(8);
         DM_CUDA(cudaMemsetAsync(c->red_counter.p, 0, 8 * sizeof(unsigned), c->stream));
+        if (c->chain_lanes >= 2) {
+            DM_CUDA(cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking));
+            DM_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+            DM_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+            c->red_partials2.alloc((size_t)2 * 64 * kMaxRedBlocks);
+            c->red_counter2.alloc(8);
+            DM_CUDA(cudaMemsetAsync(c->red_counter2.p, 0, 8 * sizeof(unsigned), c->stream));
+        }
         c->red_out.alloc(16);
         c->lz_d.alloc((size_t)kLzSlots * kLzStride);
         c->lz_s.alloc((size_t)kLzSlots * 8);
@@ -693,14 +721,18 @@ int dmfted_free(dmfted_ctx *c) {
     // a device error still pending from this context's last work is reported
     // here rather than left for the next context to trip over
     cudaError_t pending = c->stream ? cudaStreamSynchronize(c->stream) : cudaSuccess;
-    cudaStream_t st = c->stream;
+    if (c->stream2 && pending == cudaSuccess) pending = cudaStreamSynchronize(c->stream2);
+    cudaStream_t st = c->stream, st2 = c->stream2;
     for (cudaEvent_t e : c->hv_ev_free) cudaEventDestroy(e);
     for (auto &pr : c->hv_ev) {
         cudaEventDestroy(pr.first);
         cudaEventDestroy(pr.second);
     }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     delete c;
     if (st) cudaStreamDestroy(st);
+    if (st2) cudaStreamDestroy(st2);
     DM_REQUIRE(pending == cudaSuccess, DMFTED_ERR_CUDA,
                std::string("device error pending at free: ") + cudaGetErrorString(pending));
     API_END

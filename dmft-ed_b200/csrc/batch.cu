@@ -1160,6 +1160,24 @@ static void run_batch_chains_cl(dmfted_ctx *c, int CL, const std::vector<ChainJo
     }
 }
 
+// The context's per-lane resources -- stream, reduction scratch, chain
+// buffers -- exchanged with the second set while the guard lives, so that
+// everything queued meanwhile (launches, copies, timing events) goes to the
+// second stream with its own scratch.
+struct SecondLane {
+    dmfted_ctx *c;
+    explicit SecondLane(dmfted_ctx *cc) : c(cc) { swap(); }
+    ~SecondLane() { swap(); }
+    SecondLane(const SecondLane &) = delete;
+    SecondLane &operator=(const SecondLane &) = delete;
+    void swap() {
+        std::swap(c->stream, c->stream2);
+        c->red_partials.swap(c->red_partials2);
+        c->red_counter.swap(c->red_counter2);
+        c->chainbuf.swap(c->chainbuf2);
+    }
+};
+
 void batch_chains_gf(dmfted_ctx *c, const std::vector<ChainRec> &recs, int precision) {
     const dmfted_params &p = c->p;
     const int L = p.lmats + p.lreal;
@@ -1216,22 +1234,50 @@ void batch_chains_gf(dmfted_ctx *c, const std::vector<ChainRec> &recs, int preci
                           else run_batch_chains_cl<float>(c, cl, jobs, alpha, beta, nsteps, norm2, nrec);
                       });
     }
-    // chains too large for one CTA: the grid-wide recurrence, in order
-    for (int i = 0; i < nrec; i++) {
-        if (batched[i]) continue;
+    // chains too large for one CTA: the grid-wide recurrence, two at a time
+    // (the second on the second lane) so that each chain's kernels fill the
+    // SMs the other leaves idle in its last wave, and its bandwidth-bound
+    // updates overlap the other's H*v
+    std::vector<int> grid_recs;
+    for (int i = 0; i < nrec; i++)
+        if (!batched[i]) grid_recs.push_back(i);
+    auto start_vector = [&](int i, DBuf<double> &v0) {
         const ChainRec &r = recs[i];
         const SectorView si = sector_view(c, r.isector), sj = chain_view(c, r.jsector);
-        c->s64b.alloc(sj.dim);
-        gf_apply_op(c, si, sj, r.iorb, r.ispin, r.particle != 0, c->states64.p + r.psi_off,
-                    c->s64b.p, norm2 + i);
-        LanczosScalars lz = lz_slot(c, 1, r.nlanc);
-        lanczos_chain(c, sj, c->s64b.p, precision, lz);
+        v0.alloc(sj.dim);
+        gf_apply_op(c, si, sj, r.iorb, r.ispin, r.particle != 0, c->states64.p + r.psi_off, v0.p,
+                    norm2 + i);
+    };
+    auto run_chain = [&](int i, const double *v0, int slot) {
+        const ChainRec &r = recs[i];
+        LanczosScalars lz = lz_slot(c, slot, r.nlanc);
+        lanczos_chain(c, chain_view(c, r.jsector), v0, precision, lz);
         DM_CUDA(cudaMemcpyAsync(alpha + (size_t)i * kChainStride, lz.alpha,
                                 kChainStride * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
         DM_CUDA(cudaMemcpyAsync(beta + (size_t)i * kChainStride, lz.beta,
                                 kChainStride * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
         DM_CUDA(cudaMemcpyAsync(nsteps + i, lz.status + 1, sizeof(int), cudaMemcpyDeviceToDevice,
                                 c->stream));
+    };
+    const bool two = c->chain_lanes >= 2 && c->stream2;
+    for (size_t g = 0; g < grid_recs.size(); g += two ? 2 : 1) {
+        const int ia = grid_recs[g];
+        const int ib = two && g + 1 < grid_recs.size() ? grid_recs[g + 1] : -1;
+        start_vector(ia, c->s64b);
+        if (ib >= 0) {
+            start_vector(ib, c->s64d);
+            DM_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+            DM_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+        }
+        run_chain(ia, c->s64b.p, 1);
+        if (ib >= 0) {
+            {
+                SecondLane lane(c);
+                run_chain(ib, c->s64d.p, 2);  // slot 2: free during a solve
+            }
+            DM_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+            DM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+        }
     }
     if (L <= 0) return;
     std::vector<ChainCF> cf(nrec);

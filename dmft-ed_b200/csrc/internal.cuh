@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/dmfted.h"
@@ -96,6 +97,10 @@ struct DBuf {
     DBuf(const DBuf &) = delete;
     DBuf &operator=(const DBuf &) = delete;
     ~DBuf() { release(); }
+    void swap(DBuf &o) {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+    }
     void alloc(size_t count) {
         if (count <= n && p) return;
         release();
@@ -203,6 +208,16 @@ struct dmfted_ctx {
     // reduction scratch and Lanczos scalars
     dmfted::DBuf<double> red_partials;  // grid-reduction (hi, lo) pairs
     dmfted::DBuf<unsigned> red_counter;  // ticket counters (left at 0)
+    // second lane: a stream with its own reduction scratch, chain buffers and
+    // start vector, so that two Green's-function chains run concurrently
+    // (batch.cu, SecondLane)
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    dmfted::DBuf<double> red_partials2;
+    dmfted::DBuf<unsigned> red_counter2;
+    dmfted::DBuf<uint8_t> chainbuf2;
+    dmfted::DBuf<double> s64d;
+    int chain_lanes = 2;                // grid-wide chains run two at a time (1: in turn)
     dmfted::DBuf<double> red_out;        // small result slots
     dmfted::DBuf<double> lz_d;           // Lanczos scalar slots
     dmfted::DBuf<int> lz_s;              // Lanczos status slots

@@ -143,3 +143,17 @@ def test_batch_autotune_picks_measured_cluster_and_agrees():
     keys = [l.split(" ->")[0] for l in s.autotune_log()]
     assert len(keys) == len(set(keys))  # each job shape measured once
     s.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_grid_chains_on_two_lanes_equal_in_turn(precision):
+    # the grid-wide chains run two at a time on two streams, each with its own
+    # reduction scratch and buffers: the same fixed-order arithmetic as one at
+    # a time, so the results are bit-identical (odd number of chains included)
+    m = split_model(23, 2, 2, beta=50.0, ust=2.0, jh=0.5)
+    one = solve(m, {"DMFTED_BATCH_MAX_DIM": "0", "DMFTED_CHAIN_LANES": "1"}, precision=precision)
+    two = solve(m, {"DMFTED_BATCH_MAX_DIM": "0", "DMFTED_CHAIN_LANES": "2"}, precision=precision)
+    assert np.array_equal(one["g"], two["g"])
+    assert np.array_equal(one["e"], two["e"])
+    for k in ("dens", "docc", "magz"):
+        assert np.array_equal(one["obs"][k], two["obs"][k]), k
