@@ -144,6 +144,73 @@ __global__ void k_ell_build(int ns, const ClassTab ct, int norb, int nbath, int 
 // least used so far in that slot.  Balanced quads mean fewer shared-memory
 // wavefronts per gather; the set of hops of a row is unchanged.  One thread
 // per group of 32 lanes.
+//
+// The greedy order is then improved per quarter warp by hill climbing: swap
+// two slots of one row when that lowers the summed cost of the two slots,
+// where a slot's cost is its wavefront count (the largest number of distinct
+// target rows in one quad) and, below that, the sum of squared quad loads
+// (which steers the search across plateaus of equal wavefront count).  On the
+// 3432-row class of 14 sites at 7 particles this cuts the gather wavefronts
+// of the H*v by 22 % over the greedy order (5399 -> 4184 per column tile;
+// 3010 would be conflict-free).
+constexpr int kClimbRows = 8, kClimbW = 16, kClimbPasses = 32;
+
+__device__ int climb_slot_cost(const uint32_t (&t)[kClimbRows][kClimbW], const int *self, const int *c,
+                               int m, int q) {
+    int load[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < m; i++) {
+        const uint32_t ti = q < c[i] ? t[i][q] : (uint32_t)self[i];
+        bool dup = false;
+        for (int j = 0; j < i; j++) dup |= (q < c[j] ? t[j][q] : (uint32_t)self[j]) == ti;
+        if (!dup) load[ti & 7u]++;
+    }
+    int mx = 0, sq = 0;
+    for (int b = 0; b < 8; b++) {
+        mx = max(mx, load[b]);
+        sq += load[b] * load[b];
+    }
+    return mx * 64 + sq;
+}
+
+__device__ void climb_quarter(uint32_t *e, int64_t rows, const int64_t *rr, const uint8_t *cnt,
+                              int64_t off, int m) {
+    uint32_t ent[kClimbRows][kClimbW], t[kClimbRows][kClimbW];
+    int c[kClimbRows], self[kClimbRows];
+    for (int i = 0; i < m; i++) {
+        c[i] = min((int)cnt[off + rr[i]], kClimbW);
+        self[i] = (int)rr[i];
+        for (int q = 0; q < c[i]; q++) {
+            ent[i][q] = e[(int64_t)q * rows + rr[i]];
+            t[i][q] = ell_col(ent[i][q]);
+        }
+    }
+    for (int pass = 0; pass < kClimbPasses; pass++) {
+        bool improved = false;
+        for (int i = 0; i < m; i++)
+            for (int a = 0; a < c[i]; a++)
+                for (int b = a + 1; b < c[i]; b++) {
+                    const int before = climb_slot_cost(t, self, c, m, a) + climb_slot_cost(t, self, c, m, b);
+                    uint32_t x = t[i][a];
+                    t[i][a] = t[i][b];
+                    t[i][b] = x;
+                    const int after = climb_slot_cost(t, self, c, m, a) + climb_slot_cost(t, self, c, m, b);
+                    if (after < before) {
+                        improved = true;
+                        x = ent[i][a];
+                        ent[i][a] = ent[i][b];
+                        ent[i][b] = x;
+                    } else {
+                        x = t[i][a];
+                        t[i][a] = t[i][b];
+                        t[i][b] = x;
+                    }
+                }
+        if (!improved) break;
+    }
+    for (int i = 0; i < m; i++)
+        for (int q = 0; q < c[i]; q++) e[(int64_t)q * rows + rr[i]] = ent[i][q];
+}
+
 __global__ void k_ell_balance(int ns, int n, int64_t off, int W, int vw, int gsize,
                               const uint8_t *cnt, uint32_t *ell) {
     const int64_t rows = binom_d(ns, n);
@@ -181,6 +248,16 @@ __global__ void k_ell_balance(int ns, int n, int64_t off, int W, int vw, int gsi
             }
             load[q][ell_col(e[(int64_t)q * rows + r]) & 7u]++;
         }
+    }
+    if (gsize != kClimbRows || wmax > kClimbW) return;
+    for (int l0 = 0; l0 < 32; l0 += kClimbRows) {
+        int64_t rr[kClimbRows];
+        int m = 0;
+        for (int i = 0; i < kClimbRows; i++) {
+            const int64_t r = blk * span + (int64_t)(l0 + i) * vw + par;
+            if (r < rows) rr[m++] = r;
+        }
+        if (m > 1) climb_quarter(e, rows, rr, cnt, off, m);
     }
 }
 

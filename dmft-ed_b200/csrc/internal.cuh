@@ -217,7 +217,8 @@ struct dmfted_ctx {
     dmfted::DBuf<unsigned> red_counter2;
     dmfted::DBuf<uint8_t> chainbuf2;
     dmfted::DBuf<double> s64d;
-    int chain_lanes = 2;                // grid-wide chains run two at a time (1: in turn)
+    int chain_lanes = 2;
+    int64_t gs_restarts = 0;            // FP64 ground-state runs restarted on their true residual                // grid-wide chains run two at a time (1: in turn)
     dmfted::DBuf<double> red_out;        // small result slots
     dmfted::DBuf<double> lz_d;           // Lanczos scalar slots
     dmfted::DBuf<int> lz_s;              // Lanczos status slots

@@ -132,6 +132,20 @@ def test_ground_state_energy(precision):
     s.close()
 
 
+@pytest.mark.parametrize("precision", [dmfted.FP64, dmfted.MIXED])
+@pytest.mark.parametrize("seed,nup,ndw", [(2, 4, 4), (3, 3, 4), (4, 4, 5), (5, 5, 5)])
+def test_ground_state_vector_residual(precision, seed, nup, ndw):
+    # the returned vector, not only the energy, meets the stopping bound: a
+    # Lanczos run that went on past convergence must not hand back a mix of
+    # a Ritz pair and its copy
+    m = O.seeded_model(seed, norb=1, nbath=8, u=2.0 + 0.3 * seed, beta=100.0)
+    s = solver_for(m, precision=precision)
+    e0, psi, _ = s.lanczos_gs(s.sector_index(nup, ndw))
+    H = O.sparse_h(m, O.build_sector(m.ns, nup, ndw))
+    assert np.linalg.norm(H @ psi - e0 * psi) < 1e-9
+    s.close()
+
+
 def test_lanc_tridiag_matches_oracle():
     # sp_lanc_tridiag contract on the physical particle chain c^+_up |GS>
     m = cfg1(3)
