@@ -32,7 +32,24 @@ namespace dmfted {
 enum { ST_DONE = 0, ST_STEPS = 1, ST_CONV = 2, ST_RITZ_VALID = 3, ST_BREAK = 4 };
 
 // w = u - a_k sc_k s_k (in place in u), then b_{k+1} = |w|.  VW elements
-// per thread per pass (16-byte accesses when n is a multiple of VW).
+// per thread per pass (16-byte accesses when n is a multiple of VW); the
+// vector form issues the loads of kUpdUnroll passes before using them, so
+// that each SM keeps enough bytes in flight to cover the HBM latency.
+constexpr int kUpdUnroll = 4;
+
+template <typename T, int VW>
+__device__ __forceinline__ void lz_update_vec(uint4 &qu, const uint4 &qs, double coef, CSum &s) {
+    T a[VW], b[VW];
+    memcpy(a, &qu, 16);
+    memcpy(b, &qs, 16);
+#pragma unroll
+    for (int q = 0; q < VW; q++) {
+        a[q] = (T)((double)a[q] - coef * (double)b[q]);
+        s.add((double)a[q] * (double)a[q]);
+    }
+    memcpy(&qu, a, 16);
+}
+
 template <typename T, int VW>
 __global__ void __launch_bounds__(kRedThreads) k_lz_update(T *u, const T *scur, int64_t n,
                                                            LanczosScalars lz, int k, double thr,
@@ -41,8 +58,24 @@ __global__ void __launch_bounds__(kRedThreads) k_lz_update(T *u, const T *scur, 
     const double coef = lz.alpha[k] * lz.scale[k];
     CSum s;
     s.zero();
-    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * VW; i < n;
-         i += (int64_t)gridDim.x * blockDim.x * VW) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * VW;
+    int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * VW;
+    if constexpr (VW > 1) {
+        for (; i + (kUpdUnroll - 1) * stride < n; i += kUpdUnroll * stride) {
+            uint4 qu[kUpdUnroll], qs[kUpdUnroll];
+#pragma unroll
+            for (int q = 0; q < kUpdUnroll; q++) {
+                qu[q] = *reinterpret_cast<const uint4 *>(u + i + q * stride);
+                qs[q] = *reinterpret_cast<const uint4 *>(scur + i + q * stride);
+            }
+#pragma unroll
+            for (int q = 0; q < kUpdUnroll; q++) {
+                lz_update_vec<T, VW>(qu[q], qs[q], coef, s);
+                *reinterpret_cast<uint4 *>(u + i + q * stride) = qu[q];
+            }
+        }
+    }
+    for (; i < n; i += stride) {
         if constexpr (VW == 1) {
             const T wt = (T)((double)u[i] - coef * (double)scur[i]);
             u[i] = wt;
@@ -50,15 +83,7 @@ __global__ void __launch_bounds__(kRedThreads) k_lz_update(T *u, const T *scur, 
         } else {
             uint4 qu = *reinterpret_cast<const uint4 *>(u + i);
             const uint4 qs = *reinterpret_cast<const uint4 *>(scur + i);
-            T a[VW], b[VW];
-            memcpy(a, &qu, 16);
-            memcpy(b, &qs, 16);
-#pragma unroll
-            for (int q = 0; q < VW; q++) {
-                a[q] = (T)((double)a[q] - coef * (double)b[q]);
-                s.add((double)a[q] * (double)a[q]);
-            }
-            memcpy(&qu, a, 16);
+            lz_update_vec<T, VW>(qu, qs, coef, s);
             *reinterpret_cast<uint4 *>(u + i) = qu;
         }
     }
