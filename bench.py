@@ -465,7 +465,7 @@ def main():
     per_launch = hvt["bytes"] / max(1, hvt["launches"])
     # ncu DRAM bytes of the fused FP32 step on the 7/7 sector, scaled by the
     # algorithmic bytes per launch
-    prof = ncu_traffic("k_hxv_lz_ns14_fp32")
+    prof = ncu_traffic("k_hxv_lean_lz_ns14_fp32")
     traffic = prof * per_launch / (3 * dim * 4) if prof else None
     g_err = float(np.abs(mixed["g"] - fp64["g"]).max())
     e_err = abs(mixed["e0"] - fp64["e0"]) / abs(fp64["e0"])
