@@ -138,6 +138,50 @@ __device__ inline void tridiag_evec(const double *a, const double *b, int n, dou
     for (int i = 0; i < n; i++) yv[i] *= sg;
 }
 
+// Lowest m eigenvalues of T_n, one warp per eigenvalue (warp w takes j = w,
+// w + nwarps, ...), all warps at once: multisection on 32 points per round,
+// the new bracket between the last lane whose Sturm count is at most j and the
+// next (a ballot, no block barrier).  Sturm counts are latency-bound chains,
+// so 32 points per eigenvalue in parallel cost far less than the whole block
+// on one eigenvalue after another.  a, b in shared memory; lane 0 writes
+// evals[j]; the caller synchronises the block before reading them.
+__device__ inline void tridiag_eigs_warp(const double *a, const double *b, int n, int m,
+                                         double *evals) {
+    const int lane = threadIdx.x & 31, nw = (int)(blockDim.x >> 5);
+    double lo = INFINITY, hi = -INFINITY, amax = 0.0;
+    for (int i = lane; i < n; i += 32) {
+        const double r = (i > 0 ? fabs(b[i]) : 0.0) + (i + 1 < n ? fabs(b[i + 1]) : 0.0);
+        lo = fmin(lo, a[i] - r);
+        hi = fmax(hi, a[i] + r);
+        amax = fmax(amax, fabs(a[i]) + r);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    }
+    const double pad = 2.2e-16 * fmax(amax, 1e-300) * 4.0 + 1e-300;
+    lo -= pad;
+    hi += pad;
+    const double am = fmax(fabs(lo), fabs(hi));
+    const double pivmin = 1e-300 + 2.2e-16 * 2.2e-16 * fmax(am * am, 1e-300);
+    for (int j = (int)(threadIdx.x >> 5); j < m; j += nw) {
+        double l = lo, h = hi;
+        for (int round = 0; round < 96; round++) {
+            if (h - l <= 2.0 * 2.2e-16 * fmax(fabs(l), fabs(h)) + 1e-300) break;
+            const double x = l + (h - l) * (double)(lane + 1) / 33.0;
+            const unsigned below = __ballot_sync(0xffffffffu, sturm_count(a, b, n, x, pivmin) <= j);
+            const int t = below == 0xffffffffu ? 32 : __ffs(~below) - 1;
+            const double nl = t == 0 ? l : l + (h - l) * (double)t / 33.0;
+            const double nh = t == 32 ? h : l + (h - l) * (double)(t + 1) / 33.0;
+            l = nl;
+            h = nh;
+        }
+        if (lane == 0) evals[j] = 0.5 * (l + h);
+    }
+}
+
 // Dynamic shared memory of the two Ritz kernels for n steps.
 __host__ __device__ inline size_t ritz_smem(int n) { return (size_t)8 * n * sizeof(double) + n + 16; }
 
@@ -155,9 +199,11 @@ __device__ inline bool ritz_multi_dev(const double *sa, const double *sb, int n,
     unsigned char *sw = reinterpret_cast<unsigned char *>(work + 6 * n);
     if (threadIdx.x == 0) okflag = 1;
     const int m = min(mwant, n);
+    tridiag_eigs_warp(sa, sb, n, m, evals);
+    __syncthreads();
     for (int j = 0; j < m; j++) {
-        const double e = tridiag_eig(sa, sb, n, j);
         if (threadIdx.x == 0) {
+            const double e = evals[j];
             tridiag_evec(sa, sb, n, e, yv, ws, sw);
             // orthogonalise against the lower eigenvectors (close eigenvalues)
             for (int q = 0; q < j; q++) {
@@ -170,12 +216,10 @@ __device__ inline bool ritz_multi_dev(const double *sa, const double *sb, int n,
             nr = 1.0 / sqrt(nr);
             const double sg = yv[0] < 0.0 ? -nr : nr;
             for (int i = 0; i < n; i++) Y[(int64_t)j * n + i] = yv[i] * sg;
-            evals[j] = e;
             est[j] = fabs(bn) * fabs(Y[(int64_t)j * n + n - 1]);
             const double eps23 = 3.666852862501036e-11;
             if (!(est[j] <= tol * fmax(eps23, fabs(e)))) okflag = 0;
         }
-        __syncthreads();
     }
     __syncthreads();
     const bool ok = okflag != 0;
