@@ -695,7 +695,8 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
             __syncthreads();
             const int m = min(J.neigen, n);
             const bool ok = ritz_multi_dev(rwork, rwork + n, n, J.neigen, tol, sbe[n], evp,
-                                           Y, coef, rwork + 2 * n);
+                                           Y, coef, rwork + 2 * n,
+                                           (int)eigs_ritz_doubles() - 2 * n);
             if (ok && n >= m && m == J.neigen) break;
         }
     }
@@ -705,7 +706,8 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
     for (int i = tid; i < n; i += bd) rwork[n + i] = i > 0 ? sbe[i] : 0.0;
     __syncthreads();
     const int mm = min(J.neigen, n);
-    ritz_multi_dev(rwork, rwork + n, n, mm, tol, sbe[n], evp, Y, coef, rwork + 2 * n);
+    ritz_multi_dev(rwork, rwork + n, n, mm, tol, sbe[n], evp, Y, coef, rwork + 2 * n,
+                   (int)eigs_ritz_doubles() - 2 * n);
     if (rank == 0)
         for (int j = tid; j < mm; j += bd) evals[(int64_t)J.slot * kEigsMaxEigen + j] = evp[j];
     for (int t = tid; t < mm * n; t += bd) coef[t] = Y[t] * ssc[t % n];

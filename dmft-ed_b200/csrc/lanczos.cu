@@ -761,7 +761,7 @@ __global__ void __launch_bounds__(kRedThreads) k_lz_renorm(const T *w, int64_t n
 // ARPACK's test or the recurrence broke down.  Dynamic shared memory:
 // ritz_smem(n).  Y lives in global memory (m*n doubles).
 __global__ void k_ritz_multi(LanczosScalars lz, double tol, int mwant, double *evals, double *Y,
-                             double *est, int final_pass) {
+                             double *est, int final_pass, int work_cap) {
     extern __shared__ double rs[];
     const int n = lz.status[ST_STEPS];
     if (n <= 0) return;
@@ -771,7 +771,8 @@ __global__ void k_ritz_multi(LanczosScalars lz, double tol, int mwant, double *e
         sb[i] = i > 0 ? lz.beta[i] : 0.0;
     }
     __syncthreads();
-    const bool ok = ritz_multi_dev(sa, sb, n, mwant, tol, lz.beta[n], evals, Y, est, rs + 2 * n);
+    const bool ok = ritz_multi_dev(sa, sb, n, mwant, tol, lz.beta[n], evals, Y, est, rs + 2 * n,
+                                   work_cap - 2 * n);
     if (threadIdx.x == 0 && !final_pass) {
         const int m = min(mwant, n);
         if (lz.status[ST_BREAK] || (ok && n >= m && m == mwant) || (ok && n == lz.kmax)) {
@@ -779,6 +780,22 @@ __global__ void k_ritz_multi(LanczosScalars lz, double tol, int mwant, double *e
             lz.status[ST_DONE] = 1;
         }
     }
+}
+
+// Dynamic shared memory of k_ritz_multi for up to n steps and m pairs: a, b
+// and the eigenvector work spaces of up to 8 concurrent inverse iterations,
+// within 200 KB (returned in doubles through cap as well).
+constexpr size_t kRitzMultiSmemMax = 200 * 1024;
+static size_t ritz_multi_smem(int n, int m, int *cap) {
+    int lanes = std::max(1, std::min(m, 8));
+    size_t d = 2 * (size_t)n + (size_t)lanes * ritz_evec_doubles(n);
+    while (lanes > 1 && d * sizeof(double) > kRitzMultiSmemMax) {
+        lanes--;
+        d = 2 * (size_t)n + (size_t)lanes * ritz_evec_doubles(n);
+    }
+    d = std::max(d, (ritz_smem(n) + sizeof(double) - 1) / sizeof(double));
+    *cap = (int)d;
+    return d * sizeof(double);
 }
 
 // coef[j*n + i] = Y[j*n + i] * scale_i
@@ -800,7 +817,7 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
     static bool attr[64] = {false};
     if (!attr[c->device & 63]) {
         DM_CUDA(cudaFuncSetAttribute(k_ritz_multi, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)ritz_smem(kLzMax)));
+                                     (int)std::max(kRitzMultiSmemMax, ritz_smem(kLzMax))));
         attr[c->device & 63] = true;
     }
     const int m = std::min<int64_t>(neigen, dim);
@@ -842,8 +859,9 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
             DM_CHECK_LAUNCH();
             c->launches += 6;
         }
-        k_ritz_multi<<<1, kRedThreads, ritz_smem(launched), c->stream>>>(lz, tol, m, d_evals, d_Y,
-                                                                         d_est, 0);
+        int cap = 0;
+        const size_t rsm = ritz_multi_smem(launched, m, &cap);
+        k_ritz_multi<<<1, kRedThreads, rsm, c->stream>>>(lz, tol, m, d_evals, d_Y, d_est, 0, cap);
         DM_CHECK_LAUNCH();
         c->launches++;
         DM_CUDA(cudaMemcpyAsync(hst, lz.status, sizeof(hst), cudaMemcpyDeviceToHost, c->stream));
@@ -852,7 +870,9 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
     }
     const int n = hst[ST_STEPS];
     const int mm = std::min(m, n);
-    k_ritz_multi<<<1, kRedThreads, ritz_smem(n), c->stream>>>(lz, tol, mm, d_evals, d_Y, d_est, 1);
+    int cap = 0;
+    const size_t rsm = ritz_multi_smem(n, mm, &cap);
+    k_ritz_multi<<<1, kRedThreads, rsm, c->stream>>>(lz, tol, mm, d_evals, d_Y, d_est, 1, cap);
     k_ritz_coefs<<<div_up((int64_t)mm * n, 256), 256, 0, c->stream>>>(d_Y, lz.scale, mm, n, d_coef);
     for (int j = 0; j < mm; j++) {
         double *v = vecs + (size_t)j * dim;

@@ -185,40 +185,56 @@ __device__ inline void tridiag_eigs_warp(const double *a, const double *b, int n
 // Dynamic shared memory of the two Ritz kernels for n steps.
 __host__ __device__ inline size_t ritz_smem(int n) { return (size_t)8 * n * sizeof(double) + n + 16; }
 
+// Doubles of one eigenvector work space of ritz_multi_dev (vector, the four
+// factor arrays of tridiag_evec, its pivot flags).
+__host__ __device__ inline int ritz_evec_doubles(int n) { return 5 * n + (n + 7) / 8 + 1; }
+
 // Lowest min(mwant, n) Ritz pairs of T_n with all threads of the block: a, b
-// in shared memory, work = ritz_smem(n) - 2n doubles of shared memory after
-// them.  evals[j], Y[j*n + i] (eigenvector j, first component positive,
-// re-orthogonalised against the lower ones in the small space) and the Ritz
-// estimate est[j] = b_n |Y[j*n + n-1]|.  Returns, in every thread, whether
-// every estimate passes ARPACK's test est <= tol * max(eps^(2/3), |theta|).
+// in shared memory, work = work_cap doubles of shared memory after them (at
+// least ritz_evec_doubles(n)).  evals[j], Y[j*n + i] (eigenvector j, first
+// component positive, re-orthogonalised against the lower ones in the small
+// space) and the Ritz estimate est[j] = b_n |Y[j*n + n-1]|.  Returns, in every
+// thread, whether every estimate passes ARPACK's test est <= tol *
+// max(eps^(2/3), |theta|).  The eigenvalues are found one warp each; the
+// inverse iterations run on lane 0 of as many warps as work spaces fit in
+// work; the re-orthogonalisation, in order of j, on thread 0.
 __device__ inline bool ritz_multi_dev(const double *sa, const double *sb, int n, int mwant,
                                       double tol, double bn, double *evals, double *Y, double *est,
-                                      double *work) {
+                                      double *work, int work_cap) {
     __shared__ int okflag;
-    double *yv = work, *ws = work + n;
-    unsigned char *sw = reinterpret_cast<unsigned char *>(work + 6 * n);
     if (threadIdx.x == 0) okflag = 1;
     const int m = min(mwant, n);
     tridiag_eigs_warp(sa, sb, n, m, evals);
     __syncthreads();
-    for (int j = 0; j < m; j++) {
-        if (threadIdx.x == 0) {
-            const double e = evals[j];
-            tridiag_evec(sa, sb, n, e, yv, ws, sw);
+    const int per = ritz_evec_doubles(n);
+    const int lanes = max(1, min(min(m, work_cap / per), (int)(blockDim.x >> 5)));
+    const int w = (int)(threadIdx.x >> 5);
+    if ((threadIdx.x & 31) == 0 && w < lanes) {
+        double *yv = work + (size_t)w * per, *ws = yv + n;
+        unsigned char *sw = reinterpret_cast<unsigned char *>(ws + 4 * n);
+        for (int j = w; j < m; j += lanes) {
+            tridiag_evec(sa, sb, n, evals[j], yv, ws, sw);
+            for (int i = 0; i < n; i++) Y[(int64_t)j * n + i] = yv[i];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < m; j++) {
+            double *yj = Y + (int64_t)j * n;
             // orthogonalise against the lower eigenvectors (close eigenvalues)
             for (int q = 0; q < j; q++) {
                 double d = 0.0;
-                for (int i = 0; i < n; i++) d += Y[(int64_t)q * n + i] * yv[i];
-                for (int i = 0; i < n; i++) yv[i] -= d * Y[(int64_t)q * n + i];
+                for (int i = 0; i < n; i++) d += Y[(int64_t)q * n + i] * yj[i];
+                for (int i = 0; i < n; i++) yj[i] -= d * Y[(int64_t)q * n + i];
             }
             double nr = 0.0;
-            for (int i = 0; i < n; i++) nr += yv[i] * yv[i];
+            for (int i = 0; i < n; i++) nr += yj[i] * yj[i];
             nr = 1.0 / sqrt(nr);
-            const double sg = yv[0] < 0.0 ? -nr : nr;
-            for (int i = 0; i < n; i++) Y[(int64_t)j * n + i] = yv[i] * sg;
-            est[j] = fabs(bn) * fabs(Y[(int64_t)j * n + n - 1]);
+            const double sg = yj[0] < 0.0 ? -nr : nr;
+            for (int i = 0; i < n; i++) yj[i] *= sg;
+            est[j] = fabs(bn) * fabs(yj[n - 1]);
             const double eps23 = 3.666852862501036e-11;
-            if (!(est[j] <= tol * fmax(eps23, fabs(e)))) okflag = 0;
+            if (!(est[j] <= tol * fmax(eps23, fabs(evals[j])))) okflag = 0;
         }
     }
     __syncthreads();
