@@ -145,7 +145,9 @@ __global__ void k_ell_build(int ns, const ClassTab ct, int norb, int nbath, int 
 // wavefronts per gather; the set of hops of a row is unchanged.  One thread
 // per group of 32 lanes.
 //
-// The greedy order is then improved per quarter warp by hill climbing: swap
+// In classes whose words have at most 8 hops (those the lean H*v kernel
+// serves), k_ell_climb then improves the greedy order per quarter warp by
+// hill climbing: swap
 // two slots of one row when that lowers the summed cost of the two slots,
 // where a slot's cost is its wavefront count (the largest number of distinct
 // target rows in one quad) and, below that, the sum of squared quad loads
@@ -249,16 +251,28 @@ __global__ void k_ell_balance(int ns, int n, int64_t off, int W, int vw, int gsi
             load[q][ell_col(e[(int64_t)q * rows + r]) & 7u]++;
         }
     }
-    if (gsize != kClimbRows || wmax > kClimbW) return;
-    for (int l0 = 0; l0 < 32; l0 += kClimbRows) {
-        int64_t rr[kClimbRows];
-        int m = 0;
-        for (int i = 0; i < kClimbRows; i++) {
-            const int64_t r = blk * span + (int64_t)(l0 + i) * vw + par;
-            if (r < rows) rr[m++] = r;
-        }
-        if (m > 1) climb_quarter(e, rows, rr, cnt, off, m);
+}
+
+// The hill climbing of k_ell_balance's groups, one thread per quarter warp
+// (launched after the greedy pass, in classes whose words have at most 8
+// hops, with gsize 8 and at most kClimbW hops per word).
+__global__ void k_ell_climb(int ns, int n, int64_t off, int W, int vw, const uint8_t *cnt,
+                            uint32_t *ell) {
+    const int64_t rows = binom_d(ns, n);
+    const int64_t span = vw == 2 ? 64 : 32;
+    const int64_t nq = ((rows + span - 1) / span) * vw * 4;
+    const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (g >= nq) return;
+    const int64_t grp = g / 4, blk = grp / vw, par = grp % vw;
+    const int l0 = (int)(g % 4) * kClimbRows;
+    uint32_t *e = ell + (int64_t)W * off;
+    int64_t rr[kClimbRows];
+    int m = 0;
+    for (int i = 0; i < kClimbRows; i++) {
+        const int64_t r = blk * span + (int64_t)(l0 + i) * vw + par;
+        if (r < rows) rr[m++] = r;
     }
+    if (m > 1) climb_quarter(e, rows, rr, cnt, off, m);
 }
 
 // Lean gather table of one class from its balanced ELL table (same slot
@@ -436,15 +450,33 @@ void fock_set_couplings(dmfted_ctx *c) {
             d_eb, t.cnt.p, t.ell.p, t.diag.p, t.diag_f.p, rebuild ? 1 : 0);
         DM_CHECK_LAUNCH();
         c->launches++;
+        // most hops per word of each class (picks the lean H*v's hop counts,
+        // and the classes whose gather order is worth the climb)
+        if (rebuild) {
+            std::vector<uint8_t> hc(c->nstore);
+            DM_CUDA(cudaMemcpyAsync(hc.data(), t.cnt.p, c->nstore, cudaMemcpyDeviceToHost,
+                                    c->stream));
+            DM_CUDA(cudaStreamSynchronize(c->stream));
+            t.cls_max.assign(c->ns + 1, 0);
+            for (int n = 0; n <= c->ns; n++)
+                for (int64_t r = 0; r < c->binom[n]; r++)
+                    t.cls_max[n] = std::max<int>(t.cls_max[n], hc[c->class_poff[n] + r]);
+        }
         // gather grouping of the H*v: two rows per thread for even class sizes
         for (int n = 0; rebuild && n <= c->ns; n++) {
             const int vw = (c->binom[n] % 2 == 0) ? 2 : 1;
             const int64_t ng = ((c->binom[n] + (vw == 2 ? 63 : 31)) / (vw == 2 ? 64 : 32)) * vw;
+            const int gsize = c->tune_ell_group > 0 ? c->tune_ell_group : 8;
             k_ell_balance<<<div_up(ng, 64), 64, 0, c->stream>>>(
-                c->ns, n, c->class_poff[n], std::max(c->W, 1), vw,
-                c->tune_ell_group > 0 ? c->tune_ell_group : 8, t.cnt.p, t.ell.p);
+                c->ns, n, c->class_poff[n], std::max(c->W, 1), vw, gsize, t.cnt.p, t.ell.p);
             DM_CHECK_LAUNCH();
             c->launches++;
+            if (t.cls_max[n] <= 8 && gsize == kClimbRows && std::max(c->W, 1) <= kClimbW) {
+                k_ell_climb<<<div_up(ng * 4, 64), 64, 0, c->stream>>>(
+                    c->ns, n, c->class_poff[n], std::max(c->W, 1), vw, t.cnt.p, t.ell.p);
+                DM_CHECK_LAUNCH();
+                c->launches++;
+            }
         }
         if (rebuild) {
             for (int n = 0; n <= c->ns; n++) {
@@ -454,15 +486,6 @@ void fock_set_couplings(dmfted_ctx *c) {
                 DM_CHECK_LAUNCH();
                 c->launches++;
             }
-            // most hops per word of each class (picks the lean H*v's hop counts)
-            std::vector<uint8_t> hc(c->nstore);
-            DM_CUDA(cudaMemcpyAsync(hc.data(), t.cnt.p, c->nstore, cudaMemcpyDeviceToHost,
-                                    c->stream));
-            DM_CUDA(cudaStreamSynchronize(c->stream));
-            t.cls_max.assign(c->ns + 1, 0);
-            for (int n = 0; n <= c->ns; n++)
-                for (int64_t r = 0; r < c->binom[n]; r++)
-                    t.cls_max[n] = std::max<int>(t.cls_max[n], hc[c->class_poff[n] + r]);
         }
         c->ell_pattern[s] = pattern;
     }
