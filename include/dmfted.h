@@ -20,7 +20,9 @@
  *   - the user bath array has the set_dmft_bath layout: e(ispin,iorb,k) then
  *     v(ispin,iorb,k), k fastest              (ED_BATH/dmft_aux.f90:493-512).
  *
- * One context per process and GPU, one CUDA stream per context; calls on a
+ * One context per process and GPU.  A context queues its work on its own CUDA
+ * stream; the grid-wide Green's-function chains also use a second stream of
+ * the context, joined back to the first before the call returns.  Calls on a
  * context are not thread-safe (the reference's module state is not either).
  */
 #ifndef DMFTED_H
