@@ -242,8 +242,12 @@ def differentiation_workload(dmfted, device, steps, warmup, solver64, isec, bath
 
 
 def make_solver(dmfted, precision, device):
+    # LANC_NSTATES_SECTOR = 1: the workload is the sector's ground state (the
+    # reference then asks sp_eigh for one eigenpair and keeps one state per
+    # sector); the default 6 adds the degenerate-copy probes of ed_diag
     p = dmfted.default_params(nbath=NBATH, uloc=[U], beta=BETA, xmu=0.0, lmats=LMATS, lreal=0,
-                              lanc_ngfiter=NGF, precision=precision, device=device)
+                              lanc_ngfiter=NGF, precision=precision, device=device,
+                              lanc_nstates_sector=1)
     return dmfted.EDSolver(p)
 
 
@@ -483,6 +487,7 @@ def main():
         config={"workload": "impurity solve Ns=14 (Nbath=13, U=3, beta=100) sector 7/7 "
                             "dim 11778624: Lanczos GS (residual tol 1e-12) + observables + "
                             "particle/hole chains (200 steps) + G, Sigma on Lmats=4096",
+                "lanc_nstates_sector": 1,
                 "precision": "mixed (FP32 vectors, compensated FP64 alpha/beta, FP64 refinement, GF chains with 20 leading FP64 steps)",
                 "parallelism": (f"lattice: {world} inequivalent sites, one per GPU, all-reduce "
                                 f"of G, Sigma and observables per step" if world > 1 else

@@ -12,8 +12,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libdmfted.so")
 SOURCES = ["api.cu", "fock.cu", "hxv.cu", "lanczos.cu", "gf.cu", "observables.cu", "chi2.cu",
-           "batch.cu", "noalloc.cu"]
-HEADERS = ["internal.cuh", "reduce.cuh", "hxv.cuh", "tridiag.cuh"]
+           "batch.cu", "noalloc.cu", "dense.cu", "diag.cu"]
+HEADERS = ["internal.cuh", "reduce.cuh", "hxv.cuh", "tridiag.cuh", "sector.cuh"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -41,7 +41,7 @@ def build(force=False, verbose=False, checked=False):
     nvcc = os.environ.get("NVCC", "nvcc")
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
         extra = ["-DDMFTED_DEVICE_CHECKS"] if checked else []
@@ -49,8 +49,15 @@ def build(force=False, verbose=False, checked=False):
                os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(obj)
+    # one nvcc per source file, in parallel (the files are independent)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     cmd = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", OUT, *objs]
     subprocess.run(cmd, check=True)
     return OUT

@@ -181,74 +181,6 @@ static void hv_timer_collect(dmfted_ctx *c) {
     c->hv_ev_bytes.clear();
 }
 
-static void states_reset(dmfted_ctx *c) { c->states.clear(); }
-
-static int64_t state_dim(const dmfted_ctx *c, int isector) {
-    return c->binom[c->getnup[isector - 1]] * c->binom[c->getndw[isector - 1]];
-}
-
-static int64_t states_used(const dmfted_ctx *c) {
-    int64_t u = 0;
-    for (auto &s : c->states)
-        if (!s.src) u = std::max<int64_t>(u, s.off + state_dim(c, s.isector));
-    return u;
-}
-
-// Grows the eigenspace store to hold `need` elements, keeping the first
-// `used` ones.
-static void states_reserve(dmfted_ctx *c, int64_t used, int64_t need) {
-    if ((size_t)need > c->states64.n) {
-        const size_t cap = std::max<size_t>((size_t)need, c->states64.n * 2);
-        double *np = nullptr;
-        cudaError_t err = cudaMalloc((void **)&np, cap * sizeof(double));
-        DM_REQUIRE(err == cudaSuccess, DMFTED_ERR_NOMEM, "cudaMalloc for the eigenspace failed");
-        if (c->states64.p && used > 0)
-            DM_CUDA(cudaMemcpyAsync(np, c->states64.p, used * sizeof(double),
-                                    cudaMemcpyDeviceToDevice, c->stream));
-        DM_CUDA(cudaStreamSynchronize(c->stream));
-        c->states64.release();
-        c->states64.p = np;
-        c->states64.n = cap;
-    }
-}
-
-// Energy-ordered insertion after equal energies (es_insert_state_c,
-// ED_EIGENSPACE.f90:157-213: traverse until e <= next).
-static void states_insert(dmfted_ctx *c, const dmfted_ctx::State &st) {
-    auto it = c->states.begin();
-    while (it != c->states.end() && !(st.e <= it->e)) ++it;
-    c->states.insert(it, st);
-}
-
-static void states_add(dmfted_ctx *c, double e, int isector, const double *psi, int64_t dim) {
-    const int64_t used = states_used(c);        // elements in use (<= states64.n)
-    const int64_t off = (used + 31) / 32 * 32;  // 256-byte aligned start of the new vector
-    states_reserve(c, used, off + dim);
-    DM_CUDA(cudaMemcpyAsync(c->states64.p + off, psi, dim * sizeof(double), cudaMemcpyDeviceToDevice,
-                            c->stream));
-    DM_CUDA(cudaStreamSynchronize(c->stream));  // psi is a scratch buffer the next sector reuses
-    states_insert(c, dmfted_ctx::State{e, isector, off, nullptr});
-}
-
-// Copies every state still held by the batch pool into the store.
-static void states_materialize(dmfted_ctx *c) {
-    int64_t used = states_used(c), need = (used + 31) / 32 * 32;
-    for (auto &s : c->states)
-        if (s.src) need = (need + state_dim(c, s.isector) + 31) / 32 * 32;
-    states_reserve(c, used, need);
-    int64_t off = (used + 31) / 32 * 32;
-    for (auto &s : c->states) {
-        if (!s.src) continue;
-        const int64_t dim = state_dim(c, s.isector);
-        DM_CUDA(cudaMemcpyAsync(c->states64.p + off, s.src, dim * sizeof(double),
-                                cudaMemcpyDeviceToDevice, c->stream));
-        s.off = off;
-        s.src = nullptr;
-        off = (off + dim + 31) / 32 * 32;
-    }
-    DM_CUDA(cudaStreamSynchronize(c->stream));
-}
-
 __global__ void k_interleave_split(const double *z, double *re, double *im, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -277,63 +209,6 @@ static void real_to_host_c128(dmfted_ctx *c, const double *d, int64_t n, double 
     DM_CUDA(cudaMemcpyAsync(host, c->wv64.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost,
                             c->stream));
     DM_CUDA(cudaStreamSynchronize(c->stream));
-}
-
-// es_add_state with a size limit (ED_EIGENSPACE.f90:126-151): below the
-// limit insert; at the limit insert only below the highest energy, which is
-// popped first (es_pop_state, :219-299).
-static void states_add_capped(dmfted_ctx *c, double e, int isector, const double *psi, int64_t dim,
-                              int size, bool deferred = false) {
-    const bool take = (int)c->states.size() < size;
-    if (!take && !(!c->states.empty() && e < c->states.back().e)) return;
-    if (!take) c->states.pop_back();
-    if (deferred) states_insert(c, dmfted_ctx::State{e, isector, -1, psi});
-    else states_add(c, e, isector, psi, dim);
-}
-
-// ed_diag_c, finite-temperature branch (ED_DIAG.f90:93-228): for every sector
-// the lowest Neigen = min(dim, neigen_sector) eigenpairs go into the list of
-// at most lanc_nstates_total states.
-static int64_t ed_diag_finite_t(dmfted_ctx *c, const std::vector<int> &list) {
-    const dmfted_params &p = c->p;
-    states_reset(c);
-    int64_t hv = 0;
-    // sectors small enough for one CTA run together first; every sector then
-    // enters the list in the reference's order
-    // Eigenpairs are FP64 in both precision modes: a Krylov basis kept in
-    // FP32 is orthogonal only to ~1e-7, and the recurrence then returns
-    // spurious copies of converged eigenvalues, which change the kept list.
-    // (DMFTED_FT_EIGS_FP32=1 selects FP32 vectors here for measurement.)
-    const int eprec = c->ft_eigs_fp32 ? p.precision : DMFTED_FP64;
-    std::vector<BatchEig> batched;
-    batch_eigs(c, list, eprec, batched);
-    std::vector<double> ev(kLzMax + 8);
-    for (size_t li = 0; li < list.size(); li++) {
-        const int isector = list[li];
-        SectorView s = sector_view(c, isector);
-        if (batched[li].m >= 0) {
-            hv += batched[li].steps;
-            // the batch pool keeps these vectors: only the survivors are copied
-            for (int i = 0; i < batched[li].m; i++)
-                states_add_capped(c, batched[li].evals[i], isector,
-                                  batched[li].vecs + (size_t)i * s.dim, s.dim, c->nstates_total,
-                                  true);
-            continue;
-        }
-        const int neigen = (int)std::min<int64_t>(s.dim, c->neigen_sector[isector - 1]);
-        if (neigen <= 0) continue;
-        const int nit = (int)std::min<int64_t>(s.dim, p.lanc_niter);
-        c->eigvecs.alloc((size_t)neigen * s.dim);
-        int steps = 0;
-        const int m = lanczos_eigs(c, s, neigen, eprec, p.lanc_tolerance, nit, ev.data(),
-                                   c->eigvecs.p, &steps);
-        hv += steps;
-        for (int i = 0; i < m; i++)
-            states_add_capped(c, ev[i], isector, c->eigvecs.p + (size_t)i * s.dim, s.dim,
-                              c->nstates_total);
-    }
-    states_materialize(c);
-    return hv;
 }
 
 // ed_analysis, finite-temperature part (ED_DIAG.f90:248-398): Z from the full
@@ -420,28 +295,7 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     for (auto &e : ev) DM_CUDA(cudaEventCreate(&e));
     DM_CUDA(cudaEventRecord(ev[0], c->stream));
     // ---- diagonalisation ------------------------------------------------
-    states_reset(c);
-    double oldzero = 1000.0;
-    const double gsth = p.gs_threshold;
-    int64_t hv_diag = 0;
-    if (c->finite_t) hv_diag = ed_diag_finite_t(c, list);
-    for (int isector : (c->finite_t ? std::vector<int>() : list)) {
-        SectorView s = sector_view(c, isector);
-        c->s64a.alloc(s.dim);
-        const int nit = (int)std::min<int64_t>(s.dim, p.lanc_niter);
-        LanczosResult r = lanczos_gs(c, s, c->s64a.p, nullptr, p.precision, p.lanc_tolerance, nit);
-        hv_diag += r.steps;
-        const double enemin = r.e0;
-        // T=0 state selection, ED_DIAG.f90:202-214
-        if (enemin < oldzero - 10.0 * gsth) {
-            oldzero = enemin;
-            states_reset(c);
-            states_add(c, enemin, isector, c->s64a.p, s.dim);
-        } else if (std::fabs(enemin - oldzero) <= gsth) {
-            oldzero = std::min(oldzero, enemin);
-            states_add(c, enemin, isector, c->s64a.p, s.dim);
-        }
-    }
+    const int64_t hv_diag = ed_diag(c, list);
     DM_REQUIRE(!c->states.empty(), DMFTED_ERR_NOTCONV, "ed_solve: no state kept");
     if (c->finite_t) {
         ed_analysis_finite_t(c);
@@ -875,6 +729,38 @@ int dmfted_lanczos_gs(dmfted_ctx *c, int32_t isector, double *e0, double *psi, i
     *e0 = r.e0;
     if (niter) *niter = r.steps;
     if (psi) real_to_host_c128(c, c->s64a.p, s.dim, psi);
+    API_END
+}
+
+int dmfted_gs_lanczos(dmfted_ctx *c, int32_t isector, int32_t neigen, int32_t nitermax,
+                      double tol, double *evals, double *evecs, int32_t *nfound) {
+    API_BEGIN
+    DM_REQUIRE(c && evals, DMFTED_ERR_ARG, "null argument");
+    DM_CUDA(cudaSetDevice(c->device));
+    DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "sp_eigh: bath not set");
+    DM_REQUIRE(isector >= 1 && isector <= c->nsectors, DMFTED_ERR_ARG, "sector out of range");
+    DM_REQUIRE(neigen >= 1, DMFTED_ERR_ARG, "sp_eigh: Neigen < 1");
+    const int64_t dim = (int64_t)c->getdimup[isector - 1] * c->getdimdw[isector - 1];
+    const int ne = (int)std::min<int64_t>(neigen, dim);
+    // the call's own iteration limit and tolerance, restored on every exit
+    struct Restore {
+        dmfted_params &p;
+        int32_t niter;
+        double tol;
+        ~Restore() {
+            p.lanc_niter = niter;
+            p.lanc_tolerance = tol;
+        }
+    } restore{c->p, c->p.lanc_niter, c->p.lanc_tolerance};
+    if (nitermax > 0) c->p.lanc_niter = nitermax;
+    if (tol > 0.0) c->p.lanc_tolerance = tol;
+    if (evecs) c->gsvec.alloc((size_t)ne * dim);
+    int64_t steps = 0;
+    const int m = sector_eigenpairs(c, isector, ne, evals, evecs ? c->gsvec.p : nullptr, &steps);
+    if (evecs)
+        for (int k = 0; k < m; k++)
+            real_to_host_c128(c, c->gsvec.p + (int64_t)k * dim, dim, evecs + 2 * (int64_t)k * dim);
+    if (nfound) *nfound = m;
     API_END
 }
 

@@ -29,6 +29,7 @@
 
 #include "internal.cuh"
 #include "reduce.cuh"
+#include "sector.cuh"
 #include "tridiag.cuh"
 
 namespace cg = cooperative_groups;
@@ -36,86 +37,6 @@ namespace cg = cooperative_groups;
 namespace dmfted {
 
 constexpr int kBatchThreads = 1024;  // one CTA per SM runs one job at a time
-
-// ---------------------------------------------------------------- tables --
-// Hop tables of one spin in the precision T of the vectors.
-template <typename T>
-struct BatchSpin {
-    const uint8_t *cnt;
-    const uint32_t *ell;
-    const T *diag;
-    const T *par;
-};
-
-template <typename T>
-struct BatchTables {
-    const uint32_t *words;
-    const int32_t *rank;
-    BatchSpin<T> sp[2];  // up, down
-    const T *dint;
-    int64_t poff[kMaxNs + 1];   // padded class offsets
-    int64_t binom[kMaxNs + 1];  // class sizes
-    int64_t nrank;              // entries of the rank table (2^Ns)
-    int norb, P, W;
-};
-
-template <typename T>
-static BatchTables<T> batch_tables(const dmfted_ctx *c) {
-    BatchTables<T> b{};
-    b.words = c->words.p;
-    b.rank = c->rank.p;
-    for (int s = 0; s < 2; s++) {
-        const SpinTables &t = (s == 1 && !c->spin_shared) ? c->spin[1] : c->spin[0];
-        b.sp[s].cnt = t.cnt.p;
-        b.sp[s].ell = t.ell.p;
-        if constexpr (sizeof(T) == 8) {
-            b.sp[s].diag = (const T *)t.diag.p;
-            b.sp[s].par = (const T *)t.par.p;
-        } else {
-            b.sp[s].diag = (const T *)t.diag_f.p;
-            b.sp[s].par = (const T *)t.par_f.p;
-        }
-    }
-    if constexpr (sizeof(T) == 8) b.dint = (const T *)c->dint.p;
-    else b.dint = (const T *)c->dint_f.p;
-    for (int n = 0; n <= c->ns; n++) {
-        b.poff[n] = c->class_poff[n];
-        b.binom[n] = c->binom[n];
-    }
-    b.nrank = (int64_t)1 << c->ns;
-    b.norb = c->norb;
-    b.P = c->P;
-    b.W = std::max(c->W, 1);
-    return b;
-}
-
-// Geometry of one sector inside a job (reference order iup + DimUp*idw).
-template <typename T>
-struct Sec {
-    uint32_t dimup, dimdw, dim;
-    const uint32_t *wu, *wd;
-    const uint8_t *cu, *cd;
-    const uint32_t *eu, *ed;
-    const T *du, *dd;
-};
-
-template <typename T>
-__device__ __forceinline__ Sec<T> make_sec(const BatchTables<T> &tb, int nup, int ndw) {
-    Sec<T> s;
-    s.dimup = (uint32_t)tb.binom[nup];
-    s.dimdw = (uint32_t)tb.binom[ndw];
-    s.dim = s.dimup * s.dimdw;
-    const int64_t ou = tb.poff[nup], od = tb.poff[ndw];
-    s.wu = tb.words + ou;
-    s.wd = tb.words + od;
-    s.cu = tb.sp[0].cnt + ou;
-    s.cd = tb.sp[1].cnt + od;
-    s.eu = tb.sp[0].ell + (int64_t)tb.W * ou;
-    s.ed = tb.sp[1].ell + (int64_t)tb.W * od;
-    s.du = tb.sp[0].diag + ou;
-    s.dd = tb.sp[1].diag + od;
-    return s;
-}
 
 // Couplings of both spins and the impurity diagonal, staged once per CTA.
 template <typename T>
@@ -258,7 +179,7 @@ constexpr int kChainStride = kLzMax + 2;
 // against every job in a checked build (the checks are uniform over the CTAs
 // of a cluster, so a skipped job is skipped by all of them).
 struct BatchCaps {
-    int64_t work, vec, aux, states, slots;
+    int64_t work, vec, aux, states, slots, lock;
 };
 
 template <typename T, int CL>
@@ -396,10 +317,10 @@ struct EigsJob {
     int64_t basis_off; // elements of T: (kmax + 1) vectors of ld elements
     int64_t vec_off;   // FP64 eigenvectors: neigen x dim
     int64_t aux_off;   // FP64 scratch: Y and coefficients (2 x neigen x kmax)
+    int64_t lock_off;  // locked FP64 vectors (dim apart) in the lock pool
+    int nlock;         // how many (0: plain run)
 };
 
-constexpr int kEigsMaxSteps = 512;
-constexpr int kEigsMaxEigen = 64;
 constexpr int kEigsChunk = 4;  // basis vectors per reorthogonalisation dot pass
 constexpr int kMaxWaves = 64;  // launches of one batched eigensolve (memory budget)
 constexpr double kDgks = 0.717;  // second Gram-Schmidt pass below this norm ratio
@@ -536,11 +457,46 @@ __device__ __forceinline__ CSum reorth_update(const T *B, uint32_t ld, int nv, T
     return nrm;
 }
 
+// y -= X X^T y over the job's elements for the nlock locked FP64 vectors X
+// (dim apart, orthonormal), four at a time, twice (classical Gram-Schmidt
+// with a repeat); returns this thread's share of |y|^2.
+template <typename T, int CL>
+__device__ CSum lock_orth(const double *X, int nlock, T *y, uint32_t dim, BatchSmem<T> &sm) {
+    const int rank = cta_rank<CL>();
+    const uint32_t i0 = (uint32_t)(rank * blockDim.x + threadIdx.x), st = CL * blockDim.x;
+    for (int pass = 0; pass < 2; pass++)
+        for (int j0 = 0; j0 < nlock; j0 += 4) {
+            CSum d[4];
+#pragma unroll
+            for (int t = 0; t < 4; t++) d[t].zero();
+            for (uint32_t i = i0; i < dim; i += st) {
+                const double yi = (double)y[i];
+#pragma unroll
+                for (int t = 0; t < 4; t++)
+                    if (j0 + t < nlock) d[t].add(X[(int64_t)(j0 + t) * dim + i] * yi);
+            }
+            double tot[4];
+            job_sum<CL, 4>(d, sm, tot);
+            for (uint32_t i = i0; i < dim; i += st) {
+                double acc = (double)y[i];
+#pragma unroll
+                for (int t = 0; t < 4; t++)
+                    if (j0 + t < nlock) acc -= tot[t] * X[(int64_t)(j0 + t) * dim + i];
+                y[i] = (T)acc;
+            }
+        }
+    CSum nrm;
+    nrm.zero();
+    for (uint32_t i = i0; i < dim; i += st) nrm.add((double)y[i] * (double)y[i]);
+    return nrm;
+}
+
 // One sector's eigensolve, run by CL CTAs (a cluster) or by one CTA.
 template <typename T, int CL>
 __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn, const EigsJob &J,
                          T *basis_pool, double *vec_pool, double *aux_pool, double *evals,
-                         int *steps_out, double tol, int ncheck, const BatchCaps &cap) {
+                         int *steps_out, double tol, int ncheck, const BatchCaps &cap,
+                         const double *lock_pool) {
     double *sal = dyn, *sbe = sal + (kEigsMaxSteps + 2), *ssc = sbe + (kEigsMaxSteps + 2);
     double *scf = ssc + (kEigsMaxSteps + 2), *dpart = scf + (kEigsMaxSteps + 2);
     double *rwork = dpart + kDpart;
@@ -562,8 +518,10 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
         !DM_IN(J.vec_off + (int64_t)J.neigen * dim - 1, cap.vec) ||
         !DM_IN(J.aux_off + (rank + 1) * eigs_aux_per_cta(J.neigen, J.kmax) - 1, cap.aux) ||
         !DM_IN(J.slot, cap.slots) || !DM_IN(J.kmax, kEigsMaxSteps + 1) ||
-        !DM_IN(J.neigen, kEigsMaxEigen + 1))
+        !DM_IN(J.neigen, kEigsMaxEigen + 1) ||
+        (J.nlock > 0 && !DM_IN(J.lock_off + (int64_t)J.nlock * dim - 1, cap.lock)))
         return;
+    const double *X = lock_pool + J.lock_off;
     T *B = basis_pool + J.basis_off;
     // private Ritz scratch of this CTA: Y, coefficients, eigenvalues
     const int64_t nk = (int64_t)J.neigen * J.kmax;
@@ -577,6 +535,7 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
         B[i] = v;
         a1[0].add((double)v * (double)v);
     }
+    if (J.nlock > 0) a1[0] = lock_orth<T, CL>(X, J.nlock, B, dim, sm);
     double tot[1];
     job_sum<CL, 1>(a1, sm, tot);
     if (tid == 0) {
@@ -618,6 +577,12 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
             a1[0].add((double)w * (double)w);
         }
         job_sum<CL, 1>(a1, sm, tot);
+        if (J.nlock > 0) {
+            // H keeps the locked vectors' complement invariant only up to
+            // their residuals: project the new vector every step
+            a1[0] = lock_orth<T, CL>(X, J.nlock, y, dim, sm);
+            job_sum<CL, 1>(a1, sm, tot);
+        }
         double wn = sqrt(tot[0]), bn = wn;
         anorm = fmax(anorm, fabs(ak) + sbe[k] + wn);
         // orthogonality estimate of the new vector against v_0..v_{k-1}
@@ -748,7 +713,8 @@ template <typename T, int CL>
 __global__ void __launch_bounds__(kBatchThreads, 1)
     k_batch_eigs(const BatchTables<T> tb, const EigsJob *jobs, int nbig, int njobs,
                  unsigned *queue, T *basis_pool, double *vec_pool, double *aux_pool,
-                 double *evals, int *steps_out, double tol, int ncheck, const BatchCaps cap) {
+                 double *evals, int *steps_out, double tol, int ncheck, const BatchCaps cap,
+                 const double *lock_pool) {
     __shared__ BatchSmem<T> sm;
     extern __shared__ double dyn[];
     stage_tables(tb, sm);
@@ -757,14 +723,14 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
             const int jid = next_job<CL>(queue, sm);
             if (jid >= nbig) break;
             eigs_job<T, CL>(tb, sm, dyn, jobs[jid], basis_pool, vec_pool, aux_pool, evals,
-                            steps_out, tol, ncheck, cap);
+                            steps_out, tol, ncheck, cap, lock_pool);
         }
     }
     for (;;) {
         const int jid = nbig + next_job<1>(queue + 1, sm);
         if (jid >= njobs) break;
         eigs_job<T, 1>(tb, sm, dyn, jobs[jid], basis_pool, vec_pool, aux_pool, evals, steps_out,
-                       tol, ncheck, cap);
+                       tol, ncheck, cap, lock_pool);
     }
 }
 
@@ -994,8 +960,9 @@ static void run_batch_eigs(dmfted_ctx *c, int j0, int nbig, int j1, int wave, do
                       reinterpret_cast<T *>(c->bwork.p), c->bvec.p, c->baux.p, c->bscal.p,
                       c->bint.p + 2 * kMaxWaves, tol, std::max(1, c->p.lanc_ncheck),
                       BatchCaps{(int64_t)(c->bwork.n / sizeof(T)), (int64_t)c->bvec.n,
-                                (int64_t)c->baux.n, 0,
-                                (int64_t)(c->bscal.n / kEigsMaxEigen)});
+                                (int64_t)c->baux.n, 0, (int64_t)(c->bscal.n / kEigsMaxEigen),
+                                (int64_t)c->lockpool.n},
+                      (const double *)c->lockpool.p);
 }
 
 template <typename T>
@@ -1011,8 +978,9 @@ static void run_batch_eigs_cl(dmfted_ctx *c, int CL, int j0, int nbig, int j1, i
 }
 
 
-static void batch_eigs_cl(dmfted_ctx *c, const std::vector<int> &list, int precision,
-                          std::vector<BatchEig> &res, int CL) {
+static void batch_eigs_cl(dmfted_ctx *c, const std::vector<int> &list,
+                          const std::vector<int> &want, int precision, std::vector<BatchEig> &res,
+                          int CL, const std::vector<LockSpec> *locks) {
     const dmfted_params &p = c->p;
     res.assign(list.size(), BatchEig());
     const bool fp64 = precision == DMFTED_FP64;
@@ -1023,11 +991,8 @@ static void batch_eigs_cl(dmfted_ctx *c, const std::vector<int> &list, int preci
     size_t vec = 0, aux = 0;
     for (size_t i = 0; i < list.size(); i++) {
         const SectorView s = sector_view(c, list[i]);
-        const int neigen = (int)std::min<int64_t>(s.dim, c->neigen_sector[list[i] - 1]);
-        if (neigen <= 0) {
-            res[i].m = 0;  // ed_diag skips the sector
-            continue;
-        }
+        const int neigen = (int)std::min<int64_t>(s.dim, want[i]);
+        if (neigen <= 0) continue;
         const int kmax = (int)std::min<int64_t>(std::min(p.lanc_niter, kLzMax - 2), s.dim);
         if (c->batch_max_dim <= 0 || s.dim > c->batch_max_dim || kmax > kEigsMaxSteps ||
             neigen > kEigsMaxEigen)
@@ -1041,6 +1006,9 @@ static void batch_eigs_cl(dmfted_ctx *c, const std::vector<int> &list, int preci
         J.basis_off = 0;
         J.vec_off = (int64_t)vec;
         J.aux_off = (int64_t)aux;
+        J.lock_off = locks ? (*locks)[i].off : 0;
+        J.nlock = locks ? (*locks)[i].n : 0;
+        DM_REQUIRE(J.nlock == 0 || fp64, DMFTED_ERR_ARG, "locked eigensolve needs FP64");
         bsize.push_back((size_t)(kmax + 1) * round_up((size_t)s.dim, 32));
         vec += (size_t)neigen * s.dim;
         const bool big = CL > 1 && s.dim >= c->batch_cluster_min * CL;
@@ -1117,16 +1085,22 @@ static void batch_eigs_cl(dmfted_ctx *c, const std::vector<int> &list, int preci
     }
 }
 
-void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, int precision,
-                std::vector<BatchEig> &res) {
+void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<int> &want,
+                int precision, std::vector<BatchEig> &res, const std::vector<LockSpec> *locks) {
     int64_t dmax = 0, nj = 0;
-    for (int is : list)
-        if (c->neigen_sector[is - 1] > 0 && sector_view(c, is).dim <= c->batch_max_dim) {
-            dmax = std::max(dmax, sector_view(c, is).dim);
+    for (size_t i = 0; i < list.size(); i++)
+        if (want[i] > 0 && sector_view(c, list[i]).dim <= c->batch_max_dim) {
+            dmax = std::max(dmax, sector_view(c, list[i]).dim);
             nj++;
         }
-    tuned_cluster(c, "eigs", "DMFTED_BATCH_CLUSTER_EIGS", eigs_cluster(c, dmax), nj, dmax,
-                  precision, [&](int cl) { batch_eigs_cl(c, list, precision, res, cl); });
+    if (nj == 0) {
+        res.assign(list.size(), BatchEig());
+        return;
+    }
+    const bool probe = locks != nullptr;
+    tuned_cluster(c, probe ? "eigs-probe" : "eigs", "DMFTED_BATCH_CLUSTER_EIGS",
+                  eigs_cluster(c, dmax), nj, dmax, precision,
+                  [&](int cl) { batch_eigs_cl(c, list, want, precision, res, cl, locks); });
 }
 
 template <typename T, int CL>

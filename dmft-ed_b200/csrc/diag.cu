@@ -1,0 +1,405 @@
+// Diagonalisation of the sectors: ed_diag_c (ED_DIAG.f90:93-228) and the
+// eigenspace list it fills (ED_EIGENSPACE.f90:126-213).
+//
+// Every sector gets Neigen = min(dim, neigen_sector) eigenpairs, and the
+// reference's branch choice (ED_DIAG.f90:136-137): the dense eigensolve
+// (dense.cu) when Neigen == dim or dim <= lanc_dim_threshold, otherwise the
+// Lanczos solvers -- one CTA or cluster per sector up to batch_max_dim states
+// (batch.cu), grid-wide above (lanczos.cu).
+//
+// A Lanczos run from one start vector sees one copy of each degenerate
+// eigenvalue, where the reference's ARPACK-based sp_eigh returns the
+// copies.  So a run is followed by probe runs: Lanczos from a fresh start
+// vector kept orthogonal to every eigenvector found so far (the found vectors
+// are "locked"), which finds the lowest eigenvalue of H on their complement.
+// A probe whose eigenvalue belongs to the wanted set adds it and triggers the
+// next probe; the first probe that finds nothing new ends the sector.
+//   - finite temperature: the first run asks for Neigen pairs; a probe
+//     eigenvalue is new when fewer than Neigen pairs are known or it lies
+//     below the Neigen-th lowest known one.  The lowest Neigen go to the
+//     state list, es_add_state with the lanc_nstates_total cap.
+//   - zero temperature: only eigenvalues within 11*gs_threshold of a sector's
+//     lowest one can survive the ground-state selection (an eigenvalue e of
+//     a sector whose lowest is e0 is kept only if |e - oldzero| <= gs_threshold
+//     while oldzero <= e0 + 10*gs_threshold), so the first run asks for the
+//     lowest pair and the probes for the degenerate copies within that
+//     window, up to Neigen.  With Neigen == 1 no probe runs: the reference
+//     keeps one state per sector then too.  The selection of ED_DIAG.f90:202-214
+//     then runs over the sectors in order.
+// The first run at T=0 on the grid path is the precision-aware ground-state
+// Lanczos (FP64 or mixed); every other eigenpair is FP64 (an FP32 Krylov
+// basis returns spurious copies of converged eigenvalues).
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace dmfted {
+
+// ---------------------------------------------------------------------------
+// State list (es_add_state / es_insert_state, ED_EIGENSPACE.f90:126-213): the
+// kept eigenvectors in one device pool, energy-ordered.
+void states_reset(dmfted_ctx *c) { c->states.clear(); }
+
+static int64_t state_dim(const dmfted_ctx *c, int isector) {
+    return c->binom[c->getnup[isector - 1]] * c->binom[c->getndw[isector - 1]];
+}
+
+static int64_t states_used(const dmfted_ctx *c) {
+    int64_t u = 0;
+    for (auto &s : c->states)
+        if (!s.src) u = std::max<int64_t>(u, s.off + state_dim(c, s.isector));
+    return u;
+}
+
+// Grows the eigenspace store to hold `need` elements, keeping the first
+// `used` ones.
+static void states_reserve(dmfted_ctx *c, int64_t used, int64_t need) {
+    if ((size_t)need > c->states64.n) {
+        const size_t cap = std::max<size_t>((size_t)need, c->states64.n * 2);
+        double *np = nullptr;
+        cudaError_t err = cudaMalloc((void **)&np, cap * sizeof(double));
+        DM_REQUIRE(err == cudaSuccess, DMFTED_ERR_NOMEM, "cudaMalloc for the eigenspace failed");
+        if (c->states64.p && used > 0)
+            DM_CUDA(cudaMemcpyAsync(np, c->states64.p, used * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+        DM_CUDA(cudaStreamSynchronize(c->stream));
+        c->states64.release();
+        c->states64.p = np;
+        c->states64.n = cap;
+    }
+}
+
+// Energy-ordered insertion after equal energies (es_insert_state_c,
+// ED_EIGENSPACE.f90:157-213: traverse until e <= next).
+static void states_insert(dmfted_ctx *c, const dmfted_ctx::State &st) {
+    auto it = c->states.begin();
+    while (it != c->states.end() && !(st.e <= it->e)) ++it;
+    c->states.insert(it, st);
+}
+
+// Copies every state whose vector is still held elsewhere into the store.
+static void states_materialize(dmfted_ctx *c) {
+    int64_t used = states_used(c), need = (used + 31) / 32 * 32;
+    for (auto &s : c->states)
+        if (s.src) need = (need + state_dim(c, s.isector) + 31) / 32 * 32;
+    states_reserve(c, used, need);
+    int64_t off = (used + 31) / 32 * 32;
+    for (auto &s : c->states) {
+        if (!s.src) continue;
+        const int64_t dim = state_dim(c, s.isector);
+        DM_CUDA(cudaMemcpyAsync(c->states64.p + off, s.src, dim * sizeof(double),
+                                cudaMemcpyDeviceToDevice, c->stream));
+        s.off = off;
+        s.src = nullptr;
+        off = (off + dim + 31) / 32 * 32;
+    }
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+// es_add_state with a size limit (ED_EIGENSPACE.f90:126-151): below the
+// limit insert; at the limit insert only below the highest energy, which is
+// popped first (es_pop_state, :219-299).  The vector stays where it is until
+// states_materialize.
+static void states_add_capped(dmfted_ctx *c, double e, int isector, const double *psi, int size) {
+    const bool take = (int)c->states.size() < size;
+    if (!take && !(!c->states.empty() && e < c->states.back().e)) return;
+    if (!take) c->states.pop_back();
+    states_insert(c, dmfted_ctx::State{e, isector, -1, psi});
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+
+enum Branch { kDense = 0, kBatch = 1, kGrid = 2 };
+
+struct SectorJob {
+    int isector = 0;
+    SectorView s{};
+    int neigen = 0;   // Neigen = min(dim, neigen_sector)
+    Branch br = kDense;
+    int cap = 0;      // lock-pool slots (vectors) of the sector
+    int64_t base = 0; // first slot's element offset in c->lockpool
+    std::vector<double> e;  // eigenvalues found, in slot order
+    bool probing = false;
+    int steps = 0;
+    const double *dense_vecs = nullptr;  // dense branch: vectors in c->dense_vec
+};
+
+bool batch_fits(const dmfted_ctx *c, const SectorJob &j, int want) {
+    const int kmax = (int)std::min<int64_t>(std::min(c->p.lanc_niter, kLzMax - 2), j.s.dim);
+    return c->batch_max_dim > 0 && j.s.dim <= c->batch_max_dim && kmax <= kEigsMaxSteps &&
+           want <= kEigsMaxEigen;
+}
+
+double *slot_ptr(dmfted_ctx *c, const SectorJob &j, int k) {
+    return c->lockpool.p + j.base + (int64_t)k * j.s.dim;
+}
+
+// Whether probe eigenvalue mu joins the sector's wanted set.
+bool probe_accepts(const dmfted_ctx *c, const SectorJob &j, double mu, bool finite_t) {
+    const int n = (int)j.e.size();
+    if (n >= j.cap) return false;
+    if (!finite_t) {
+        if (n >= j.neigen) return false;
+        const double e0 = *std::min_element(j.e.begin(), j.e.end());
+        const double window =
+            11.0 * c->p.gs_threshold + 4.0 * c->p.lanc_tolerance * std::max(1.0, std::fabs(e0));
+        return mu <= e0 + window;
+    }
+    if (n < j.neigen) return true;
+    std::vector<double> srt = j.e;
+    std::sort(srt.begin(), srt.end());
+    const double top = srt[j.neigen - 1];
+    return mu < top - 1e-12 * std::max(1.0, std::fabs(top));
+}
+
+}  // namespace
+
+// Eigenpairs of the sectors in `jobs` (filled: isector, neigen); mode T=0
+// (cluster of the lowest eigenvalue) or finite T (lowest Neigen), or the
+// single-sector contract of dmfted_gs_lanczos (finite-T rule).  On return
+// every job holds its eigenvalues in j.e and its vectors in the lock pool (or
+// dense_vecs), in slot order.  Returns the H*v products used.
+static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool finite_t) {
+    const dmfted_params &p = c->p;
+    const int eprec = c->ft_eigs_fp32 ? p.precision : DMFTED_FP64;
+    int64_t hv = 0;
+    // branch choice (ED_DIAG.f90:133-137; MPI_SIZE = 1)
+    int64_t pool = 0;
+    for (auto &j : jobs) {
+        j.s = sector_view(c, j.isector);
+        const bool dense = j.neigen == j.s.dim || j.s.dim <= std::max(p.lanc_dim_threshold, 1);
+        if (dense) {
+            j.br = kDense;
+            continue;
+        }
+        const int first = finite_t ? j.neigen : 1;
+        j.br = batch_fits(c, j, first) ? kBatch : kGrid;
+        j.cap = (int)std::min<int64_t>(j.s.dim, finite_t ? 2 * j.neigen : j.neigen);
+        j.base = pool;
+        pool += (((int64_t)j.cap * j.s.dim) + 31) / 32 * 32;
+    }
+    if (pool > 0) c->lockpool.alloc((size_t)pool);
+    // ---- dense sectors --------------------------------------------------
+    {
+        std::vector<int> dl, dw;
+        std::vector<size_t> at;
+        for (size_t i = 0; i < jobs.size(); i++)
+            if (jobs[i].br == kDense) {
+                dl.push_back(jobs[i].isector);
+                dw.push_back(jobs[i].neigen);
+                at.push_back(i);
+            }
+        if (!dl.empty()) {
+            std::vector<DenseEig> dr;
+            dense_eigs(c, dl, dw, dr);
+            for (size_t k = 0; k < dl.size(); k++) {
+                SectorJob &j = jobs[at[k]];
+                j.e = dr[k].evals;
+                j.dense_vecs = dr[k].vecs;
+            }
+        }
+    }
+    // ---- first Lanczos run ---------------------------------------------------
+    {
+        std::vector<int> bl, bw;
+        std::vector<size_t> at;
+        for (size_t i = 0; i < jobs.size(); i++)
+            if (jobs[i].br == kBatch) {
+                bl.push_back(jobs[i].isector);
+                bw.push_back(finite_t ? jobs[i].neigen : 1);
+                at.push_back(i);
+            }
+        if (!bl.empty()) {
+            std::vector<BatchEig> br;
+            batch_eigs(c, bl, bw, eprec, br);
+            for (size_t k = 0; k < bl.size(); k++) {
+                SectorJob &j = jobs[at[k]];
+                j.steps += br[k].steps;
+                hv += br[k].steps;
+                const int m = std::min(std::max(br[k].m, 0), j.cap);
+                j.e.assign(br[k].evals.begin(), br[k].evals.begin() + m);
+                if (m > 0)
+                    DM_CUDA(cudaMemcpyAsync(slot_ptr(c, j, 0), br[k].vecs,
+                                            (size_t)m * j.s.dim * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, c->stream));
+            }
+        }
+    }
+    std::vector<double> ev(kLzMax + 8);
+    for (auto &j : jobs) {
+        if (j.br != kGrid) continue;
+        const int nit = (int)std::min<int64_t>(j.s.dim, p.lanc_niter);
+        if (!finite_t) {
+            LanczosResult r =
+                lanczos_gs(c, j.s, slot_ptr(c, j, 0), nullptr, p.precision, p.lanc_tolerance, nit);
+            j.steps += r.steps;
+            hv += r.steps;
+            j.e.assign(1, r.e0);
+        } else {
+            int steps = 0;
+            c->eigvecs.alloc((size_t)j.neigen * j.s.dim);
+            const int m = std::min(lanczos_eigs(c, j.s, j.neigen, eprec, p.lanc_tolerance, nit,
+                                                ev.data(), c->eigvecs.p, &steps),
+                                   j.cap);
+            j.steps += steps;
+            hv += steps;
+            j.e.assign(ev.begin(), ev.begin() + m);
+            if (m > 0)
+                DM_CUDA(cudaMemcpyAsync(slot_ptr(c, j, 0), c->eigvecs.p,
+                                        (size_t)m * j.s.dim * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+        }
+    }
+    // ---- probes for degenerate copies -----------------------------------------
+    // (FP64 only: the measurement-only FP32 eigenpairs skip them)
+    const bool probes = eprec == DMFTED_FP64;
+    for (auto &j : jobs)
+        j.probing = probes && j.br != kDense && j.neigen > 1 && !j.e.empty() &&
+                    (int)j.e.size() < j.cap;
+    for (int round = 0;; round++) {
+        std::vector<int> bl, bw;
+        std::vector<LockSpec> locks;
+        std::vector<size_t> at;
+        bool any = false;
+        for (size_t i = 0; i < jobs.size(); i++) {
+            SectorJob &j = jobs[i];
+            if (!j.probing) continue;
+            any = true;
+            if (j.br == kBatch && batch_fits(c, j, 1)) {
+                bl.push_back(j.isector);
+                bw.push_back(1);
+                LockSpec ls;
+                ls.off = j.base;
+                ls.n = (int)j.e.size();
+                locks.push_back(ls);
+                at.push_back(i);
+            }
+        }
+        if (!any) break;
+        DM_REQUIRE(round < 4 * kDenseMaxEigen, DMFTED_ERR_NOTCONV,
+                   "ed_diag: degenerate-copy probes did not end");
+        if (!bl.empty()) {
+            std::vector<BatchEig> br;
+            batch_eigs(c, bl, bw, DMFTED_FP64, br, &locks);
+            for (size_t k = 0; k < bl.size(); k++) {
+                SectorJob &j = jobs[at[k]];
+                j.steps += br[k].steps;
+                hv += br[k].steps;
+                if (br[k].m >= 1 && probe_accepts(c, j, br[k].evals[0], finite_t)) {
+                    DM_CUDA(cudaMemcpyAsync(slot_ptr(c, j, (int)j.e.size()), br[k].vecs,
+                                            j.s.dim * sizeof(double), cudaMemcpyDeviceToDevice,
+                                            c->stream));
+                    j.e.push_back(br[k].evals[0]);
+                } else {
+                    j.probing = false;
+                }
+            }
+        }
+        for (auto &j : jobs) {
+            if (!j.probing || j.br != kGrid) continue;
+            const int nit = (int)std::min<int64_t>(j.s.dim, p.lanc_niter);
+            int steps = 0;
+            c->eigvecs.alloc((size_t)j.s.dim);
+            const int m = lanczos_eigs(c, j.s, 1, DMFTED_FP64, p.lanc_tolerance, nit, ev.data(),
+                                       c->eigvecs.p, &steps, slot_ptr(c, j, 0), (int)j.e.size());
+            j.steps += steps;
+            hv += steps;
+            if (m >= 1 && probe_accepts(c, j, ev[0], finite_t)) {
+                DM_CUDA(cudaMemcpyAsync(slot_ptr(c, j, (int)j.e.size()), c->eigvecs.p,
+                                        j.s.dim * sizeof(double), cudaMemcpyDeviceToDevice,
+                                        c->stream));
+                j.e.push_back(ev[0]);
+            } else {
+                j.probing = false;
+            }
+        }
+        for (auto &j : jobs)
+            if (j.probing && (int)j.e.size() >= j.cap) j.probing = false;
+    }
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    return hv;
+}
+
+// Eigenpairs of job j in ascending energy (ties in slot order), at most
+// `keep`: (energy, device vector).
+static std::vector<std::pair<double, const double *>> ordered_pairs(dmfted_ctx *c,
+                                                                    const SectorJob &j, int keep) {
+    std::vector<int> idx(j.e.size());
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return j.e[a] < j.e[b]; });
+    std::vector<std::pair<double, const double *>> out;
+    for (int k = 0; k < (int)idx.size() && k < keep; k++) {
+        const double *v = j.br == kDense ? j.dense_vecs + (int64_t)idx[k] * j.s.dim
+                                         : slot_ptr(c, j, idx[k]);
+        out.emplace_back(j.e[idx[k]], v);
+    }
+    return out;
+}
+
+int64_t ed_diag(dmfted_ctx *c, const std::vector<int> &list) {
+    const dmfted_params &p = c->p;
+    states_reset(c);
+    std::vector<SectorJob> jobs;
+    for (int isector : list) {
+        SectorJob j;
+        j.isector = isector;
+        j.neigen = (int)std::min<int64_t>(state_dim(c, isector), c->neigen_sector[isector - 1]);
+        if (j.neigen <= 0) continue;
+        jobs.push_back(j);
+    }
+    const int64_t hv = sector_spectra(c, jobs, c->finite_t);
+    if (c->finite_t) {
+        // ED_DIAG.f90:196-200: i = 1..Neigen into the capped list
+        for (auto &j : jobs)
+            for (auto &pr : ordered_pairs(c, j, j.neigen))
+                states_add_capped(c, pr.first, j.isector, pr.second, c->nstates_total);
+    } else {
+        // ED_DIAG.f90:202-214
+        double oldzero = 1000.0;
+        const double gsth = p.gs_threshold;
+        for (auto &j : jobs)
+            for (auto &pr : ordered_pairs(c, j, j.neigen)) {
+                const double enemin = pr.first;
+                if (enemin < oldzero - 10.0 * gsth) {
+                    oldzero = enemin;
+                    states_reset(c);
+                    states_insert(c, dmfted_ctx::State{enemin, j.isector, -1, pr.second});
+                } else if (std::fabs(enemin - oldzero) <= gsth) {
+                    oldzero = std::min(oldzero, enemin);
+                    states_insert(c, dmfted_ctx::State{enemin, j.isector, -1, pr.second});
+                }
+            }
+    }
+    states_materialize(c);
+    return hv;
+}
+
+// One sector's lowest neigen eigenpairs with the branch choice of ed_diag_c
+// and the degenerate copies (the finite-temperature rule).  evals_h:
+// neigen doubles; vecs (device, may be null): neigen x dim FP64.  Returns
+// the number found; *steps: H*v products.
+int sector_eigenpairs(dmfted_ctx *c, int isector, int neigen, double *evals_h, double *vecs,
+                      int64_t *steps) {
+    std::vector<SectorJob> jobs(1);
+    jobs[0].isector = isector;
+    jobs[0].neigen = (int)std::min<int64_t>(state_dim(c, isector), neigen);
+    const bool ft = neigen > 1;
+    const int64_t hv = sector_spectra(c, jobs, ft);
+    if (steps) *steps = hv;
+    const auto pr = ordered_pairs(c, jobs[0], jobs[0].neigen);
+    const int64_t dim = state_dim(c, isector);
+    for (size_t k = 0; k < pr.size(); k++) {
+        evals_h[k] = pr[k].first;
+        if (vecs)
+            DM_CUDA(cudaMemcpyAsync(vecs + (int64_t)k * dim, pr[k].second, dim * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    }
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    return (int)pr.size();
+}
+
+}  // namespace dmfted

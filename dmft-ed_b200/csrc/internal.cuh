@@ -264,6 +264,15 @@ struct dmfted_ctx {
     dmfted::DBuf<double> bscal;           // chain alpha / beta, norm2; eigenvalues
     dmfted::DBuf<int> bint;               // queue counter, step counts
     dmfted::DBuf<double> bcf;             // continued-fraction terms (chain x frequency)
+    // dense small-sector eigensolve (dense.cu)
+    dmfted::DBuf<double> dense_work, dense_vec, dense_eval;
+    dmfted::DBuf<int> dense_int;
+    dmfted::DBuf<uint8_t> dense_jobs;
+    // eigenvectors found so far per sector of a diagonalisation (diag.cu):
+    // the first pass, then every probe run, which also reads them as the
+    // locked vectors it keeps its Krylov space orthogonal to
+    dmfted::DBuf<double> lockpool;
+    dmfted::DBuf<double> gsvec;  // eigenvectors returned by dmfted_gs_lanczos
     int64_t launches = 0;
     // live timing of the H*v launches (dmfted_hxv_timing)
     bool hv_timing = false;
@@ -305,6 +314,8 @@ SectorView sector_view(const dmfted_ctx *c, int isector);
 SectorView chain_view(const dmfted_ctx *c, int isector);
 
 // ---- batch.cu ------------------------------------------------------------
+constexpr int kEigsMaxSteps = 512;  // Lanczos steps of one batched eigensolve job
+constexpr int kEigsMaxEigen = 64;   // eigenpairs of one batched eigensolve job
 // Lowest eigenpairs of many sectors, one CTA per sector.  For every entry of
 // `list`: results[i].m >= 0 when the sector ran here (m eigenpairs, values in
 // evals, FP64 vectors at vecs, dim apart), -1 when it must take the grid path
@@ -314,8 +325,16 @@ struct BatchEig {
     std::vector<double> evals;
     const double *vecs = nullptr;
 };
-void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, int precision,
-                std::vector<BatchEig> &results);
+// want[i]: eigenpairs wanted of sector list[i] (0: skip).  locks (may be
+// null): per entry the FP64 vectors to keep the run orthogonal to, as
+// (offset into c->lockpool, count); FP64 only.
+struct LockSpec {
+    int64_t off = 0;
+    int n = 0;
+};
+void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<int> &want,
+                int precision, std::vector<BatchEig> &results,
+                const std::vector<LockSpec> *locks = nullptr);
 // Green's-function chains: one record per chain, in accumulation order.
 struct ChainRec {
     int64_t psi_off;  // state vector in states64
@@ -326,6 +345,34 @@ struct ChainRec {
 // path above it) and adds all of them to the Matsubara / real-axis G.
 void batch_chains_gf(dmfted_ctx *c, const std::vector<ChainRec> &recs, int precision);
 void fock_build_map(dmfted_ctx *c, int isector, int32_t *d_map);  // combined map
+
+// ---- dense.cu ------------------------------------------------------------
+// Dense eigensolve (Jacobi, one CTA per sector) of the sectors ed_diag_c
+// hands to eigh: the lowest want[i] eigenpairs of sector list[i] (want 0:
+// skipped, m = -1).  Vectors are FP64 at vecs, dim apart, owned by the
+// context until the next call.
+constexpr int kDenseMaxDim = 1024;
+constexpr int kDenseMaxEigen = 64;
+struct DenseEig {
+    int m = -1, sweeps = 0;
+    std::vector<double> evals;
+    const double *vecs = nullptr;
+};
+void dense_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<int> &want,
+                std::vector<DenseEig> &res);
+
+// ---- diag.cu ---------------------------------------------------------------
+// ed_diag_c (ED_DIAG.f90:93-228): every sector of `list` diagonalised with the
+// reference's branch choice, then the state selection of the temperature
+// regime; fills c->states.  Returns the H*v products used.
+int64_t ed_diag(dmfted_ctx *c, const std::vector<int> &list);
+// The lowest neigen eigenpairs of one sector, degenerate copies included, with
+// ed_diag_c's branch choice (the contract of dmfted_gs_lanczos).  evals_h:
+// neigen doubles; vecs (device, may be null): neigen x dim FP64.  Returns the
+// number found; *steps (may be null): H*v products used.
+int sector_eigenpairs(dmfted_ctx *c, int isector, int neigen, double *evals_h, double *vecs,
+                      int64_t *steps);
+void states_reset(dmfted_ctx *c);
 
 // ---- hxv.cu --------------------------------------------------------------
 // y = H x for nvec vectors of sector s (plain product).
@@ -371,8 +418,11 @@ void lanczos_chain_fixed(dmfted_ctx *c, const SectorView &s, const double *v0, d
 // Lowest neigen eigenpairs of sector s (full reorthogonalisation).  vecs:
 // device, neigen*dim FP64 (row j = eigenvector j, normalised); evals_h host.
 // Returns the number of pairs found (min(neigen, dim, steps)).
+// locked/nlock: FP64 vectors (dim apart, orthonormal) the run keeps its
+// Krylov space orthogonal to (Lanczos on (1-XX^T) H (1-XX^T)); needs FP64.
 int lanczos_eigs(dmfted_ctx *c, const SectorView &s, int neigen, int precision, double tol,
-                 int nitermax, double *evals_h, double *vecs, int *steps);
+                 int nitermax, double *evals_h, double *vecs, int *steps,
+                 const double *locked = nullptr, int nlock = 0);
 
 // ---- gf.cu ---------------------------------------------------------------
 // vv = c^+_{iorb,ispin} psi (particle) or c psi (hole) in sector sj;

@@ -804,9 +804,23 @@ __global__ void k_ritz_coefs(const double *Y, const double *scale, int m, int n,
         coef[t] = Y[t] * scale[t % n];
 }
 
+// w -= X X^T w for the nlock FP64 locked vectors X (dim apart, orthonormal):
+// two classical Gram-Schmidt passes.  dots: nlock doubles; ones: nlock ones.
+static void lock_orth(dmfted_ctx *c, const double *X, int nlock, double *w, int64_t dim,
+                      double *dots, const double *ones) {
+    for (int pass = 0; pass < 2; pass++) {
+        k_reorth_dots<double><<<nlock, kRedThreads, 0, c->stream>>>(X, dim, nlock, w, dim, dots,
+                                                                    nullptr);
+        k_reorth_update<double><<<ew_grid(c, dim), 256, 0, c->stream>>>(X, dim, nlock, dots, ones,
+                                                                        w, dim, nullptr);
+    }
+    DM_CHECK_LAUNCH();
+    c->launches += 4;
+}
+
 template <typename T>
 static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, int nitermax,
-                    int ncheck, double *evals_h, double *vecs) {
+                    int ncheck, double *evals_h, double *vecs, const double *locked, int nlock) {
     const int64_t dim = s.dim;
     const int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
     const size_t ld = (size_t)((dim + 31) / 32 * 32);
@@ -821,15 +835,25 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
         attr[c->device & 63] = true;
     }
     const int m = std::min<int64_t>(neigen, dim);
-    c->eig_aux.alloc((size_t)64 * 2 + (size_t)m * (kLzMax + 2) * 2 + kLzMax + 8 + 3 * kProRow + 8);
+    DM_REQUIRE(nlock == 0 || sizeof(T) == 8, DMFTED_ERR_ARG, "locked eigensolve needs FP64");
+    DM_REQUIRE(nlock <= kLzMax, DMFTED_ERR_ARG, "too many locked vectors");
+    c->eig_aux.alloc((size_t)64 * 2 + (size_t)m * (kLzMax + 2) * 2 + kLzMax + 8 + 3 * kProRow + 8 +
+                     2 * (size_t)(kLzMax + 8));
     double *d_evals = c->eig_aux.p, *d_est = d_evals + 64, *d_Y = d_est + 64;
     double *d_coef = d_Y + (size_t)m * (kLzMax + 2), *d_dots = d_coef + (size_t)m * (kLzMax + 2);
     double *d_om = d_dots + kLzMax + 8, *d_pf = d_om + 3 * kProRow;
+    double *d_ldots = d_pf + 8, *d_ones = d_ldots + kLzMax + 8;
+    if (nlock > 0) {
+        std::vector<double> ones(nlock, 1.0);
+        DM_CUDA(cudaMemcpyAsync(d_ones, ones.data(), nlock * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream));
+    }
     const double eps = sizeof(T) == 8 ? 1.1102230246251565e-16 : 5.9604644775390625e-8;
     const int eg = ew_grid(c, dim);
     const int rg = red_grid(c, dim);
     c->s64b.alloc(dim);
     k_random_start<<<eg, 256, 0, c->stream>>>(c->s64b.p, dim, 1234567ull);
+    if (nlock > 0) lock_orth(c, locked, nlock, c->s64b.p, dim, d_ldots, d_ones);
     k_convert<T, double><<<eg, 256, 0, c->stream>>>(c->s64b.p, basis, dim);
     k_lz_init<T><<<rg, kRedThreads, 0, c->stream>>>(basis, dim, lz, c->red_partials.p,
                                                      c->red_counter.p);
@@ -846,6 +870,10 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
             T *y = basis + (size_t)(k + 1) * ld;
             hxv_lanczos_step<T>(c, s, x, xp, y, lz, k);
             launch_lz_update<T>(c, y, x, dim, lz, k, 1e-300);
+            // locked vectors: H keeps the space orthogonal to them only up to
+            // their residuals, so the new vector is projected every step
+            if (nlock > 0)
+                lock_orth(c, locked, nlock, reinterpret_cast<double *>(y), dim, d_ldots, d_ones);
             k_pro<<<1, kRedThreads, 0, c->stream>>>(lz, k, d_om, d_pf, eps);
             for (int pass = 0; pass < 2; pass++) {
                 k_reorth_dots<T><<<k + 1, kRedThreads, 0, c->stream>>>(basis, (int64_t)ld, k + 1, y,
@@ -853,9 +881,10 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
                 k_reorth_update<T><<<eg, 256, 0, c->stream>>>(basis, (int64_t)ld, k + 1, d_dots,
                                                              lz.scale, y, dim, d_pf);
             }
+            // after a projection the norm is always recomputed
             k_lz_renorm<T><<<rg, kRedThreads, 0, c->stream>>>(y, dim, lz, k, 1e-300,
                                                               c->red_partials.p, c->red_counter.p,
-                                                              d_pf);
+                                                              nlock > 0 ? nullptr : d_pf);
             DM_CHECK_LAUNCH();
             c->launches += 6;
         }
@@ -890,14 +919,15 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
 }
 
 int lanczos_eigs(dmfted_ctx *c, const SectorView &s, int neigen, int precision, double tol,
-                 int nitermax, double *evals_h, double *vecs, int *steps) {
+                 int nitermax, double *evals_h, double *vecs, int *steps, const double *locked,
+                 int nlock) {
     const int ncheck = std::max(1, c->p.lanc_ncheck);
     int m;
-    if (precision == DMFTED_FP64)
-        m = eigs_run<double>(c, s, neigen, tol, nitermax, ncheck, evals_h, vecs);
+    if (precision == DMFTED_FP64 || nlock > 0)
+        m = eigs_run<double>(c, s, neigen, tol, nitermax, ncheck, evals_h, vecs, locked, nlock);
     else
         m = eigs_run<float>(c, s, neigen, std::max(tol, c->mixed_tol32), nitermax, ncheck, evals_h,
-                            vecs);
+                            vecs, nullptr, 0);
     int st[8];
     DM_CUDA(cudaMemcpy(st, lz_slot(c, 0, 1).status, sizeof(st), cudaMemcpyDeviceToHost));
     if (steps) *steps = st[ST_STEPS];

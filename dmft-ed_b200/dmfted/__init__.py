@@ -78,6 +78,8 @@ EXPORTS = {
     "dmfted_hxv_device_f64": (C.c_int, [_vp, _vp, _vp, C.c_int32]),
     "dmfted_hxv_device_f32": (C.c_int, [_vp, _vp, _vp, C.c_int32]),
     "dmfted_lanczos_gs": (C.c_int, [_vp, C.c_int32, _dp, _dp, _ip]),
+    "dmfted_gs_lanczos": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_double, _dp, _dp,
+                                    _ip]),
     "dmfted_lanc_tridiag": (C.c_int, [_vp, C.c_int32, _dp, C.c_int32, _dp, _dp, _ip]),
     "dmfted_lanc_tridiag_noalloc": (C.c_int, [_vp, C.c_int32, _vp, C.c_int32, _vp, _vp, _vp, _vp]),
     "dmfted_ed_solve": (C.c_int, [_vp, _dp, C.c_int32, _ip, C.c_int32]),
@@ -266,6 +268,23 @@ class EDSolver:
                                     _p(psi.view(np.float64)) if want_vector else None,
                                     C.byref(nit)))
         return e0.value, psi, nit.value
+
+    def gs_lanczos(self, isector, neigen, nitermax=0, tol=0.0, want_vectors=True):
+        """sp_eigh / eigh of one sector as ed_diag_c calls them
+        (ED_DIAG.f90:133-194): the lowest neigen eigenpairs, degenerate copies
+        included.  Returns (evals, vecs[n, dim] complex or None)."""
+        dim = self.sector_dim(isector)
+        ne = min(neigen, dim)
+        ev = np.zeros(ne)
+        vec = np.zeros(2 * ne * dim) if want_vectors else None
+        nf = C.c_int32()
+        _ck(lib().dmfted_gs_lanczos(self.ctx, isector, neigen, nitermax, tol, _p(ev),
+                                    _p(vec) if want_vectors else None, C.byref(nf)))
+        n = nf.value
+        if not want_vectors:
+            return ev[:n], None
+        v = vec.view(np.complex128).reshape(ne, dim)[:n]
+        return ev[:n], v
 
     def lanc_tridiag(self, isector, vvinit, nlanc):
         """sp_lanc_tridiag(spHtimesV_cc, vvinit, alfa, beta) on sector isector."""

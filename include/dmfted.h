@@ -157,6 +157,20 @@ int dmfted_hxv_device_f32(dmfted_ctx *ctx, const float *d_v, float *d_hv, int32_
  * follows params.precision. */
 int dmfted_lanczos_gs(dmfted_ctx *ctx, int32_t isector, double *e0, double *psi, int32_t *niter);
 
+/* The eigenpairs of one sector as ed_diag_c computes them: stands in for the
+ * sp_eigh call (ED_DIAG.f90:169-183) and the dense eigh branch (:184-194) with
+ * the reference's choice between them -- eigh when neigen == dim or
+ * dim <= lanc_dim_threshold (:136-137), Lanczos otherwise.  Returns the
+ * lowest min(neigen, dim) eigenvalues in ascending order, degenerate copies
+ * included (Lanczos runs are followed by probe runs orthogonal to the pairs
+ * found, until a probe finds nothing new).  evals[neigen]; evecs (may be NULL)
+ * complex128 eig_basis(Dim, neigen) column-major, i.e. vector i at
+ * evecs + 2*i*dim, in the H%map order.  nitermax, tol: the sp_eigh arguments
+ * (<= 0 takes lanc_niter / lanc_tolerance).  *nfound: pairs returned.
+ * neigen == 1 follows params.precision; more pairs are FP64. */
+int dmfted_gs_lanczos(dmfted_ctx *ctx, int32_t isector, int32_t neigen, int32_t nitermax,
+                      double tol, double *evals, double *evecs, int32_t *nfound);
+
 /* Three-term Lanczos tridiagonalisation from a given start vector, the
  * contract of sp_lanc_tridiag (build_gf_normal.f90:118-127): vvinit complex128
  * of length getdim(isector) (normalised here), alanc[nlanc], blanc[nlanc]

@@ -447,16 +447,126 @@ def solve_sector_t0(model, nup, ndw, lmats=4096, lreal=0, wini=-5.0, wfin=5.0, e
 
 # ------------------------------------------------ finite-T pipeline ---
 def _sector_eigs(model, hmap, k):
-    """Lowest k eigenpairs of the sector H: dense eigh (the reference's small-
-    sector branch, ED_DIAG.f90:184-194) or ARPACK eigsh ('SA')."""
+    """Lowest k eigenpairs of the sector H, degenerate copies included: dense
+    eigh (the reference's small-sector branch, ED_DIAG.f90:184-194, used here up
+    to 2500 states) or ARPACK eigsh ('SA', the eigensolver family of sp_eigh,
+    with the reference's Nblock = 3*Neigen+5 as the minimum of ncv)."""
     H = sparse_h(model, hmap)
     if hmap.size <= 2500:
         w, V = np.linalg.eigh(H.toarray())
         return w[:k], V[:, :k]
     import scipy.sparse.linalg as sla
-    w, V = sla.eigsh(H, k=k, which="SA", tol=1e-14)
+    ncv = min(hmap.size, max(3 * k + 5, 2 * k + 1, 20))
+    w, V = sla.eigsh(H, k=k, which="SA", tol=1e-14, ncv=ncv)
     o = np.argsort(w)
     return w[o], V[:, o]
+
+
+def _gf_and_obs(model, states, egs, zeta, finite_t, lmats, lreal, wini, wfin, eps, ngfiter,
+                nthreads):
+    """Observables (ED_OBSERVABLES.f90:113-160, weights exp(-beta(Ei-Egs))/Z or
+    1/Z at T=0) and the particle/hole chains of every kept state
+    (build_gf_normal.f90:71-180) summed with add_to_lanczos_gf_normal
+    (:442-488), followed by get_sigma_normal.  states: [(e, nup, ndw, psi)]."""
+    ns, no = model.ns, model.norb
+    obs = {k: np.zeros(no) for k in ["dens", "dens_up", "dens_dw", "docc", "magz"]}
+    wm = matsubara(model.beta, lmats)
+    wr = realaxis(wini, wfin, lreal)
+    gm = np.zeros((model.nspin, no, lmats), np.complex128)
+    gr = np.zeros((model.nspin, no, lreal), np.complex128)
+    chains = []
+    for e, a, b, psi in states:
+        hm = build_sector(ns, a, b)
+        peso = (np.exp(-model.beta * (e - egs)) if finite_t else 1.0) / zeta
+        psi = np.asarray(psi).astype(np.complex128)
+        o = observables_state(model, hm, psi, peso)
+        for k in obs:
+            obs[k] += o[k]
+        for ispin in range(model.nspin):
+            for iorb in range(no):
+                isite = (iorb + 1) + ispin * ns
+                for particle, dn in ((True, 1), (False, -1)):
+                    jn = (a + dn, b) if ispin == 0 else (a, b + dn)
+                    if not (0 <= jn[0] <= ns and 0 <= jn[1] <= ns):
+                        continue
+                    jmap = build_sector(ns, *jn)
+                    n2, vv = gf_vvinit(particle, isite, hm, jmap, psi)
+                    vv = vv / np.sqrt(n2)
+                    nlanc = min(jmap.size, ngfiter)
+                    al, bl, _ = lanczos_tridiag(model, jmap, vv, nlanc, nthreads=nthreads)
+                    gmt = np.zeros(lmats, np.complex128)
+                    grt = np.zeros(lreal, np.complex128)
+                    add_to_lanczos_gf(n2, e, egs, zeta, finite_t, model.beta, al, bl,
+                                      1 if particle else -1, wm, wr, eps, gmt, grt)
+                    gm[ispin, iorb] += gmt
+                    gr[ispin, iorb] += grt
+                    chains.append(dict(ispin=ispin, iorb=iorb, particle=particle, norm2=n2,
+                                       alpha=al, beta=bl, e=e, sector=(a, b)))
+    sm = np.zeros_like(gm)
+    for ispin in range(model.nspin):
+        for iorb in range(no):
+            sm[ispin, iorb] = sigma_normal(model.e[ispin, iorb], model.v[ispin, iorb], model.xmu,
+                                           model.hloc[ispin, ispin, iorb, iorb].real, 1j * wm,
+                                           gm[ispin, iorb])
+    return obs, gm, gr, sm, chains, wm
+
+
+def solve_t0(model, sectors=None, nstates_sector=6, gs_threshold=1e-9, dim_threshold=256,
+             lmats=4096, lreal=0, wini=-5.0, wfin=5.0, eps=0.01, ngfiter=200, nitermax=512,
+             tol=1e-12, nthreads=1):
+    """Zero-temperature impurity solve (lanc_nstates_total = 1) over the given
+    sectors [(nup, ndw)] in the reference's order (default: all of them):
+    ed_diag_c's T=0 branch (ED_DIAG.f90:93-228).  Every sector yields
+    Neigen = min(dim, lanc_nstates_sector) eigenpairs (ED_SETUP.f90:423-425),
+    from a dense eigh when Neigen == dim or dim <= lanc_dim_threshold
+    (:136-137,184-194), else from the Lanczos branch.  Each eigenvalue in turn,
+    sector by sector, goes through the ground-state selection of :202-214:
+    below oldzero - 10*gs_threshold it empties the list and becomes oldzero;
+    within gs_threshold of oldzero it is added and oldzero = min(oldzero, e).
+    Z = the number of kept states (ed_analysis, :278-283).  The Lanczos branch
+    with Neigen = 1 is the restated plain Lanczos ground state; with Neigen > 1
+    it is ARPACK (the eigensolver family of sp_eigh), which returns
+    degenerate copies."""
+    ns = model.ns
+    if sectors is None:
+        sectors = [(a, b) for a in range(ns + 1) for b in range(ns + 1)]
+    from math import comb
+    states = []  # [e, nup, ndw, psi]
+    oldzero = 1000.0
+    nl_total = 0
+    for a, b in sectors:
+        dim = comb(ns, a) * comb(ns, b)
+        neigen = min(dim, nstates_sector)
+        hm = build_sector(ns, a, b)
+        if neigen == 1 and dim > dim_threshold:
+            e0, psi, nl = lanczos_gs(model, hm, nitermax=nitermax, threshold=tol,
+                                     nthreads=nthreads)
+            nl_total += nl
+            w, V = [e0], psi[:, None]
+        else:
+            w, V = _sector_eigs(model, hm, neigen)
+        for i in range(neigen):
+            en = float(w[i])
+            if en < oldzero - 10.0 * gs_threshold:
+                oldzero = en
+                states = [[en, a, b, V[:, i]]]
+            elif abs(en - oldzero) <= gs_threshold:
+                oldzero = min(oldzero, en)
+                states.append([en, a, b, V[:, i]])
+    # es_add_state keeps the list energy-ordered, after equal energies
+    ordered = []
+    for st in states:
+        i = 0
+        while i < len(ordered) and not (st[0] <= ordered[i][0]):
+            i += 1
+        ordered.insert(i, st)
+    egs = min(s[0] for s in ordered)
+    zeta = float(len(ordered))
+    obs, gm, gr, sm, chains, wm = _gf_and_obs(model, ordered, egs, zeta, False, lmats, lreal,
+                                              wini, wfin, eps, ngfiter, nthreads)
+    return dict(states=[(s[0], s[1], s[2]) for s in ordered], psis=[s[3] for s in ordered],
+                egs=egs, e0=egs, zeta=zeta, obs=obs, gmats=gm, greal=gr, smats=sm, chains=chains,
+                wm=wm, nlanc=nl_total)
 
 
 def solve_finite_t(model, lmats=256, lreal=0, wini=-5.0, wfin=5.0, eps=0.01, ngfiter=200,

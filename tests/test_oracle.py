@@ -164,3 +164,75 @@ def test_chi2_gradient_finite_difference():
                                                                                  False)) / (2 * h)
                        for u in np.eye(a.size)])
         assert np.abs(gr - fd).max() <= 1e-6 * np.abs(gr).max() + 1e-12
+
+
+# ------------------------------------------------ T=0 state selection ---
+def degenerate_models():
+    """Models whose ground state is degenerate inside one sector (two identical
+    orbitals): (model, kept-state count, sectors holding them)."""
+    out = []
+    # (a) U = Ust, Jh = 0, one bath site per orbital: (3,3) holds four ground
+    # states (dim 16, dense branch), (2,4) and (4,2) one each
+    e = np.array([[[-0.8287], [-0.8287]]])
+    v = np.array([[[0.4474], [0.4474]]])
+    out.append((O.Model(norb=2, nbath=1, nspin=1, uloc=(3.0, 3.0, 0.0), ust=3.0, jh=0.0, e=e, v=v),
+                6, {(3, 3): 4, (2, 4): 1, (4, 2): 1}))
+    # (b) U = 0, symmetric bath of two sites per orbital: a zero-energy
+    # level per orbital and spin, 16 ground states over nine sectors, four of
+    # them in (3,3) (dim 400, Lanczos branch)
+    e = np.array([[[-0.6, 0.6], [-0.6, 0.6]]])
+    v = np.array([[[0.5, 0.5], [0.5, 0.5]]])
+    cnt = {(a, b): (2 if a == 3 else 1) * (2 if b == 3 else 1) for a in (2, 3, 4) for b in (2, 3, 4)}
+    out.append((O.Model(norb=2, nbath=2, nspin=1, uloc=(0.0, 0.0, 0.0), e=e, v=v), 16, cnt))
+    return out
+
+
+@pytest.mark.parametrize("im", [0, 1])
+def test_t0_keeps_degenerate_states_inside_a_sector(im):
+    m, nkeep, where = degenerate_models()[im]
+    r = O.solve_t0(m, lmats=64, nthreads=4)
+    assert r["zeta"] == nkeep and len(r["states"]) == nkeep
+    got = {}
+    for e, a, b in r["states"]:
+        got[(a, b)] = got.get((a, b), 0) + 1
+        assert abs(e - r["egs"]) <= 1e-9
+    assert got == where
+    # the kept vectors of one sector are orthonormal eigenvectors
+    for (a, b), n in where.items():
+        vs = np.array([p for p, s in zip(r["psis"], r["states"]) if (s[1], s[2]) == (a, b)])
+        assert np.allclose(vs @ vs.T, np.eye(n), atol=1e-10)
+    # particle + hole weights add up to one per (orbital, spin) and state
+    assert abs(sum(c["norm2"] for c in r["chains"]) - nkeep * m.norb) < 1e-10
+
+
+@pytest.mark.parametrize("im", [0, 1])
+def test_t0_degenerate_equals_low_temperature_limit(im):
+    # The T=0 average over the whole degenerate ground manifold (Z = count) is
+    # the beta -> infinity limit of the thermal average: at beta = 1000 the
+    # finite-temperature pipeline (a separate code path: every sector's
+    # spectrum, es_add_state's capped list, Boltzmann weights) gives the same
+    # observables and G(iwn), the excited states' weights being exp(-500).
+    import dataclasses
+    m, nkeep, _ = degenerate_models()[im]
+    m = dataclasses.replace(m, beta=1000.0)
+    r = O.solve_t0(m, lmats=128, nthreads=4)
+    f = O.solve_finite_t(m, lmats=128, nstates_total=24, nthreads=4)
+    assert abs(f["zeta"] - nkeep) < 1e-9  # beta * (spread of the copies, ~1e-14)
+    for k in ("dens", "docc", "magz"):
+        assert np.allclose(r["obs"][k], f["obs"][k], atol=1e-9), k
+    assert np.abs(r["gmats"] - f["gmats"]).max() < 1e-9
+    if im == 0:
+        # one state per sector (the selection without the in-sector partners)
+        # is a different, wrong answer here
+        one = O.solve_t0(m, nstates_sector=1, dim_threshold=0, lmats=128, nthreads=4)
+        assert one["zeta"] < nkeep
+        assert np.abs(one["gmats"] - f["gmats"]).max() > 1e-4
+
+
+def test_t0_single_sector_matches_sector_solve():
+    m = O.seeded_model(11, nbath=5, u=3.0)
+    a = O.solve_t0(m, sectors=[(3, 3)], lmats=256)
+    b = O.solve_sector_t0(m, 3, 3, lmats=256)
+    assert a["zeta"] == 1.0
+    assert abs(a["e0"] - b["e0"]) < 1e-10 * abs(b["e0"])
+    assert np.abs(a["gmats"] - b["gmats"]).max() < 1e-8
