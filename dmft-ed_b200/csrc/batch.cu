@@ -319,6 +319,7 @@ struct EigsJob {
     int64_t aux_off;   // FP64 scratch: Y and coefficients (2 x neigen x kmax)
     int64_t lock_off;  // locked FP64 vectors (dim apart) in the lock pool
     int nlock;         // how many (0: plain run)
+    double top;        // probe: eigenvalues above this are not wanted (early stop)
 };
 
 constexpr int kEigsChunk = 4;  // basis vectors per reorthogonalisation dot pass
@@ -531,7 +532,7 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
     CSum a1[1];
     a1[0].zero();
     for (uint32_t i = i0; i < dim; i += st) {
-        const T v = (T)random_start_value(i, 1234567ull);
+        const T v = (T)random_start_value(i, eigs_seed(J.nlock));
         B[i] = v;
         a1[0].add((double)v * (double)v);
     }
@@ -649,7 +650,7 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
         }
         __syncthreads();
         n = k + 1;
-        if (bn < 1e-300) {
+        if (bn < 1e-300 || bn <= kEigsBreakRel * anorm) {
             brk = true;
             break;
         }
@@ -663,6 +664,9 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
                                            Y, coef, rwork + 2 * n,
                                            (int)eigs_ritz_doubles() - 2 * n);
             if (ok && n >= m && m == J.neigen) break;
+            // a probe whose lowest Ritz value stays above the acceptance
+            // threshold by ten times its residual estimate found nothing new
+            if (J.nlock > 0 && evp[0] > J.top && coef[0] <= 0.1 * (evp[0] - J.top)) break;
         }
     }
     (void)brk;
@@ -1008,6 +1012,7 @@ static void batch_eigs_cl(dmfted_ctx *c, const std::vector<int> &list,
         J.aux_off = (int64_t)aux;
         J.lock_off = locks ? (*locks)[i].off : 0;
         J.nlock = locks ? (*locks)[i].n : 0;
+        J.top = locks ? (*locks)[i].top : INFINITY;
         DM_REQUIRE(J.nlock == 0 || fp64, DMFTED_ERR_ARG, "locked eigensolve needs FP64");
         bsize.push_back((size_t)(kmax + 1) * round_up((size_t)s.dim, 32));
         vec += (size_t)neigen * s.dim;

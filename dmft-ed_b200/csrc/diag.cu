@@ -31,6 +31,9 @@
 // basis returns spurious copies of converged eigenvalues).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <ctime>
 #include <numeric>
 #include <vector>
 
@@ -138,22 +141,26 @@ double *slot_ptr(dmfted_ctx *c, const SectorJob &j, int k) {
     return c->lockpool.p + j.base + (int64_t)k * j.s.dim;
 }
 
-// Whether probe eigenvalue mu joins the sector's wanted set.
-bool probe_accepts(const dmfted_ctx *c, const SectorJob &j, double mu, bool finite_t) {
+// The largest probe eigenvalue the sector still wants (+inf: any).
+double probe_top(const dmfted_ctx *c, const SectorJob &j, bool finite_t) {
     const int n = (int)j.e.size();
-    if (n >= j.cap) return false;
     if (!finite_t) {
-        if (n >= j.neigen) return false;
         const double e0 = *std::min_element(j.e.begin(), j.e.end());
-        const double window =
-            11.0 * c->p.gs_threshold + 4.0 * c->p.lanc_tolerance * std::max(1.0, std::fabs(e0));
-        return mu <= e0 + window;
+        return e0 + 11.0 * c->p.gs_threshold +
+               4.0 * c->p.lanc_tolerance * std::max(1.0, std::fabs(e0));
     }
-    if (n < j.neigen) return true;
+    if (n < j.neigen) return 1e300;
     std::vector<double> srt = j.e;
     std::sort(srt.begin(), srt.end());
     const double top = srt[j.neigen - 1];
-    return mu < top - 1e-12 * std::max(1.0, std::fabs(top));
+    return top - 1e-12 * std::max(1.0, std::fabs(top));
+}
+
+// Whether probe eigenvalue mu joins the sector's wanted set.
+bool probe_accepts(const dmfted_ctx *c, const SectorJob &j, double mu, bool finite_t) {
+    const int n = (int)j.e.size();
+    if (n >= j.cap || (!finite_t && n >= j.neigen)) return false;
+    return finite_t ? mu < probe_top(c, j, true) : mu <= probe_top(c, j, false);
 }
 
 }  // namespace
@@ -165,6 +172,26 @@ bool probe_accepts(const dmfted_ctx *c, const SectorJob &j, double mu, bool fini
 // dense_vecs), in slot order.  Returns the H*v products used.
 static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool finite_t) {
     const dmfted_params &p = c->p;
+    const bool dbg = getenv("DMFTED_DEBUG_EIGS") != nullptr;
+    double t_last = 0.0;
+    auto stamp = [&](const char *what) {
+        if (!dbg) return;
+        DM_CUDA(cudaStreamSynchronize(c->stream));
+        timespec ts;
+        clock_gettime(CLOCK_MONOTONIC, &ts);
+        const double t = ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+        if (t_last > 0.0) fprintf(stderr, "[eigs] %s: %.3f ms\n", what, t - t_last);
+        t_last = t;
+    };
+    stamp("start");
+    auto show = [&](const char *what, const SectorJob &j, int steps, int m, const double *ev,
+                    int nlock) {
+        if (!dbg) return;
+        fprintf(stderr, "[eigs] %s sector %d dim %lld nlock %d steps %d m %d:", what, j.isector,
+                (long long)j.s.dim, nlock, steps, m);
+        for (int i = 0; i < m; i++) fprintf(stderr, " %.15g", ev[i]);
+        fprintf(stderr, "\n");
+    };
     const int eprec = c->ft_eigs_fp32 ? p.precision : DMFTED_FP64;
     int64_t hv = 0;
     // branch choice (ED_DIAG.f90:133-137; MPI_SIZE = 1)
@@ -203,6 +230,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
             }
         }
     }
+    stamp("dense branch");
     // ---- first Lanczos run ---------------------------------------------------
     {
         std::vector<int> bl, bw;
@@ -220,6 +248,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
                 SectorJob &j = jobs[at[k]];
                 j.steps += br[k].steps;
                 hv += br[k].steps;
+                show("batch first", j, br[k].steps, std::max(br[k].m, 0), br[k].evals.data(), 0);
                 const int m = std::min(std::max(br[k].m, 0), j.cap);
                 j.e.assign(br[k].evals.begin(), br[k].evals.begin() + m);
                 if (m > 0)
@@ -229,6 +258,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
             }
         }
     }
+    stamp("batched first runs");
     std::vector<double> ev(kLzMax + 8);
     for (auto &j : jobs) {
         if (j.br != kGrid) continue;
@@ -239,6 +269,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
             j.steps += r.steps;
             hv += r.steps;
             j.e.assign(1, r.e0);
+            show("grid gs", j, r.steps, 1, &r.e0, 0);
         } else {
             int steps = 0;
             c->eigvecs.alloc((size_t)j.neigen * j.s.dim);
@@ -247,6 +278,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
                                    j.cap);
             j.steps += steps;
             hv += steps;
+            show("grid first", j, steps, m, ev.data(), 0);
             j.e.assign(ev.begin(), ev.begin() + m);
             if (m > 0)
                 DM_CUDA(cudaMemcpyAsync(slot_ptr(c, j, 0), c->eigvecs.p,
@@ -254,6 +286,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
                                         cudaMemcpyDeviceToDevice, c->stream));
         }
     }
+    stamp("grid first runs");
     // ---- probes for degenerate copies -----------------------------------------
     // (FP64 only: the measurement-only FP32 eigenpairs skip them)
     const bool probes = eprec == DMFTED_FP64;
@@ -275,6 +308,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
                 LockSpec ls;
                 ls.off = j.base;
                 ls.n = (int)j.e.size();
+                ls.top = probe_top(c, j, finite_t);
                 locks.push_back(ls);
                 at.push_back(i);
             }
@@ -289,6 +323,8 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
                 SectorJob &j = jobs[at[k]];
                 j.steps += br[k].steps;
                 hv += br[k].steps;
+                show("batch probe", j, br[k].steps, std::max(br[k].m, 0), br[k].evals.data(),
+                     (int)j.e.size());
                 if (br[k].m >= 1 && probe_accepts(c, j, br[k].evals[0], finite_t)) {
                     DM_CUDA(cudaMemcpyAsync(slot_ptr(c, j, (int)j.e.size()), br[k].vecs,
                                             j.s.dim * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -305,9 +341,11 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
             int steps = 0;
             c->eigvecs.alloc((size_t)j.s.dim);
             const int m = lanczos_eigs(c, j.s, 1, DMFTED_FP64, p.lanc_tolerance, nit, ev.data(),
-                                       c->eigvecs.p, &steps, slot_ptr(c, j, 0), (int)j.e.size());
+                                       c->eigvecs.p, &steps, slot_ptr(c, j, 0), (int)j.e.size(),
+                                       probe_top(c, j, finite_t));
             j.steps += steps;
             hv += steps;
+            show("grid probe", j, steps, m, ev.data(), (int)j.e.size());
             if (m >= 1 && probe_accepts(c, j, ev[0], finite_t)) {
                 DM_CUDA(cudaMemcpyAsync(slot_ptr(c, j, (int)j.e.size()), c->eigvecs.p,
                                         j.s.dim * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -319,6 +357,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
         }
         for (auto &j : jobs)
             if (j.probing && (int)j.e.size() >= j.cap) j.probing = false;
+        stamp("probe round");
     }
     DM_CUDA(cudaStreamSynchronize(c->stream));
     return hv;

@@ -316,6 +316,18 @@ SectorView chain_view(const dmfted_ctx *c, int isector);
 // ---- batch.cu ------------------------------------------------------------
 constexpr int kEigsMaxSteps = 512;  // Lanczos steps of one batched eigensolve job
 constexpr int kEigsMaxEigen = 64;   // eigenpairs of one batched eigensolve job
+// An eigensolve ends at an invariant subspace: b_{k+1} <= kEigsBreakRel * |T|.
+// Continuing from the rounding-level residual would restart the recurrence in
+// a random direction and put several copies of an eigenvalue into one T,
+// whose eigenvectors inverse iteration cannot separate; the copies are found
+// by the probe runs instead (diag.cu).
+constexpr double kEigsBreakRel = 1e-12;
+// Start-vector seed of the probe run that holds nlock locked vectors (the
+// first run's seed for nlock = 0): a fresh random direction each time, since
+// the first run's start vector lies in the Krylov space already explored.
+__host__ __device__ inline uint64_t eigs_seed(int nlock) {
+    return 1234567ull + 0x9E3779B97F4A7C15ull * (uint64_t)nlock;
+}
 // Lowest eigenpairs of many sectors, one CTA per sector.  For every entry of
 // `list`: results[i].m >= 0 when the sector ran here (m eigenpairs, values in
 // evals, FP64 vectors at vecs, dim apart), -1 when it must take the grid path
@@ -331,6 +343,7 @@ struct BatchEig {
 struct LockSpec {
     int64_t off = 0;
     int n = 0;
+    double top = 1e300;  // the run may stop once its lowest Ritz value is surely above this
 };
 void batch_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<int> &want,
                 int precision, std::vector<BatchEig> &results,
@@ -420,9 +433,11 @@ void lanczos_chain_fixed(dmfted_ctx *c, const SectorView &s, const double *v0, d
 // Returns the number of pairs found (min(neigen, dim, steps)).
 // locked/nlock: FP64 vectors (dim apart, orthonormal) the run keeps its
 // Krylov space orthogonal to (Lanczos on (1-XX^T) H (1-XX^T)); needs FP64.
+// top: a locked run (probe) may stop once its lowest Ritz value exceeds top by
+// ten times its residual estimate (nothing wanted below top is left).
 int lanczos_eigs(dmfted_ctx *c, const SectorView &s, int neigen, int precision, double tol,
                  int nitermax, double *evals_h, double *vecs, int *steps,
-                 const double *locked = nullptr, int nlock = 0);
+                 const double *locked = nullptr, int nlock = 0, double top = 1e300);
 
 // ---- gf.cu ---------------------------------------------------------------
 // vv = c^+_{iorb,ispin} psi (particle) or c psi (hole) in sector sj;

@@ -686,6 +686,11 @@ __global__ void __launch_bounds__(kRedThreads) k_pro(LanczosScalars lz, int k, d
         pf[0] = need ? 1.0 : 0.0;
         pf[1] = (need && !force && !periodic) ? 1.0 : 0.0;
         pf[2] = anorm;
+        if (bn <= kEigsBreakRel * anorm) {
+            // invariant subspace: the run ends here (k_lz_renorm keeps it)
+            lz.status[ST_DONE] = 1;
+            lz.status[ST_BREAK] = 1;
+        }
     }
 }
 
@@ -745,7 +750,7 @@ __global__ void __launch_bounds__(kRedThreads) k_lz_renorm(const T *w, int64_t n
             lz.beta[k + 1] = b;
             lz.scale[k + 1] = b > 0.0 ? 1.0 / b : 0.0;
             lz.status[ST_STEPS] = k + 1;
-            lz.status[ST_DONE] = 0;
+            lz.status[ST_DONE] = lz.status[ST_BREAK] ? 1 : 0;
             if (b < thr) {
                 lz.status[ST_DONE] = 1;
                 lz.status[ST_BREAK] = 1;
@@ -761,7 +766,7 @@ __global__ void __launch_bounds__(kRedThreads) k_lz_renorm(const T *w, int64_t n
 // ARPACK's test or the recurrence broke down.  Dynamic shared memory:
 // ritz_smem(n).  Y lives in global memory (m*n doubles).
 __global__ void k_ritz_multi(LanczosScalars lz, double tol, int mwant, double *evals, double *Y,
-                             double *est, int final_pass, int work_cap) {
+                             double *est, int final_pass, int work_cap, double top) {
     extern __shared__ double rs[];
     const int n = lz.status[ST_STEPS];
     if (n <= 0) return;
@@ -779,6 +784,9 @@ __global__ void k_ritz_multi(LanczosScalars lz, double tol, int mwant, double *e
             lz.status[ST_CONV] = 1;
             lz.status[ST_DONE] = 1;
         }
+        // a probe whose lowest Ritz value stays above top by ten times its
+        // residual estimate found nothing it is looking for
+        if (evals[0] > top && est[0] <= 0.1 * (evals[0] - top)) lz.status[ST_DONE] = 1;
     }
 }
 
@@ -820,7 +828,8 @@ static void lock_orth(dmfted_ctx *c, const double *X, int nlock, double *w, int6
 
 template <typename T>
 static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, int nitermax,
-                    int ncheck, double *evals_h, double *vecs, const double *locked, int nlock) {
+                    int ncheck, double *evals_h, double *vecs, const double *locked, int nlock,
+                    double top) {
     const int64_t dim = s.dim;
     const int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
     const size_t ld = (size_t)((dim + 31) / 32 * 32);
@@ -852,7 +861,7 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
     const int eg = ew_grid(c, dim);
     const int rg = red_grid(c, dim);
     c->s64b.alloc(dim);
-    k_random_start<<<eg, 256, 0, c->stream>>>(c->s64b.p, dim, 1234567ull);
+    k_random_start<<<eg, 256, 0, c->stream>>>(c->s64b.p, dim, eigs_seed(nlock));
     if (nlock > 0) lock_orth(c, locked, nlock, c->s64b.p, dim, d_ldots, d_ones);
     k_convert<T, double><<<eg, 256, 0, c->stream>>>(c->s64b.p, basis, dim);
     k_lz_init<T><<<rg, kRedThreads, 0, c->stream>>>(basis, dim, lz, c->red_partials.p,
@@ -871,9 +880,14 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
             hxv_lanczos_step<T>(c, s, x, xp, y, lz, k);
             launch_lz_update<T>(c, y, x, dim, lz, k, 1e-300);
             // locked vectors: H keeps the space orthogonal to them only up to
-            // their residuals, so the new vector is projected every step
-            if (nlock > 0)
+            // their residuals, so the new vector is projected every step, and
+            // its norm is taken again before the orthogonality estimates use it
+            if (nlock > 0) {
                 lock_orth(c, locked, nlock, reinterpret_cast<double *>(y), dim, d_ldots, d_ones);
+                k_lz_renorm<T><<<rg, kRedThreads, 0, c->stream>>>(
+                    y, dim, lz, k, 1e-300, c->red_partials.p, c->red_counter.p, nullptr);
+                c->launches++;
+            }
             k_pro<<<1, kRedThreads, 0, c->stream>>>(lz, k, d_om, d_pf, eps);
             for (int pass = 0; pass < 2; pass++) {
                 k_reorth_dots<T><<<k + 1, kRedThreads, 0, c->stream>>>(basis, (int64_t)ld, k + 1, y,
@@ -881,16 +895,16 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
                 k_reorth_update<T><<<eg, 256, 0, c->stream>>>(basis, (int64_t)ld, k + 1, d_dots,
                                                              lz.scale, y, dim, d_pf);
             }
-            // after a projection the norm is always recomputed
             k_lz_renorm<T><<<rg, kRedThreads, 0, c->stream>>>(y, dim, lz, k, 1e-300,
                                                               c->red_partials.p, c->red_counter.p,
-                                                              nlock > 0 ? nullptr : d_pf);
+                                                              d_pf);
             DM_CHECK_LAUNCH();
             c->launches += 6;
         }
         int cap = 0;
         const size_t rsm = ritz_multi_smem(launched, m, &cap);
-        k_ritz_multi<<<1, kRedThreads, rsm, c->stream>>>(lz, tol, m, d_evals, d_Y, d_est, 0, cap);
+        k_ritz_multi<<<1, kRedThreads, rsm, c->stream>>>(lz, tol, m, d_evals, d_Y, d_est, 0, cap,
+                                                         top);
         DM_CHECK_LAUNCH();
         c->launches++;
         DM_CUDA(cudaMemcpyAsync(hst, lz.status, sizeof(hst), cudaMemcpyDeviceToHost, c->stream));
@@ -901,7 +915,8 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
     const int mm = std::min(m, n);
     int cap = 0;
     const size_t rsm = ritz_multi_smem(n, mm, &cap);
-    k_ritz_multi<<<1, kRedThreads, rsm, c->stream>>>(lz, tol, mm, d_evals, d_Y, d_est, 1, cap);
+    k_ritz_multi<<<1, kRedThreads, rsm, c->stream>>>(lz, tol, mm, d_evals, d_Y, d_est, 1, cap,
+                                                     top);
     k_ritz_coefs<<<div_up((int64_t)mm * n, 256), 256, 0, c->stream>>>(d_Y, lz.scale, mm, n, d_coef);
     for (int j = 0; j < mm; j++) {
         double *v = vecs + (size_t)j * dim;
@@ -920,14 +935,15 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
 
 int lanczos_eigs(dmfted_ctx *c, const SectorView &s, int neigen, int precision, double tol,
                  int nitermax, double *evals_h, double *vecs, int *steps, const double *locked,
-                 int nlock) {
+                 int nlock, double top) {
     const int ncheck = std::max(1, c->p.lanc_ncheck);
     int m;
     if (precision == DMFTED_FP64 || nlock > 0)
-        m = eigs_run<double>(c, s, neigen, tol, nitermax, ncheck, evals_h, vecs, locked, nlock);
+        m = eigs_run<double>(c, s, neigen, tol, nitermax, ncheck, evals_h, vecs, locked, nlock,
+                             nlock > 0 ? top : 1e300);
     else
         m = eigs_run<float>(c, s, neigen, std::max(tol, c->mixed_tol32), nitermax, ncheck, evals_h,
-                            vecs, nullptr, 0);
+                            vecs, nullptr, 0, 1e300);
     int st[8];
     DM_CUDA(cudaMemcpy(st, lz_slot(c, 0, 1).status, sizeof(st), cudaMemcpyDeviceToHost));
     if (steps) *steps = st[ST_STEPS];

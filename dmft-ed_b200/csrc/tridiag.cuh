@@ -87,8 +87,17 @@ __device__ inline double tridiag_eig(const double *a, const double *b, int n, in
 // Eigenvector y of T_n (diag a[0..n), off-diagonal b[1..n)) for eigenvalue
 // lam: three steps of inverse iteration, Gaussian elimination with partial
 // pivoting on the tridiagonal.  Single thread.  ws: 5n doubles, sw: n bytes.
+// nprev > 0: lam belongs to a cluster of eigenvalues (several copies of an
+// eigenvalue, as a Lanczos run past rounding-level growth of a degenerate
+// partner holds them) and prev[q*n..] (q < nprev) are the eigenvectors of
+// the cluster's lower members.  Inverse iteration alone would return the same
+// vector for every member; as in LAPACK's dstein, the iteration then starts
+// from a pseudo-random vector (seed: the member's index) and is
+// re-orthogonalised against the lower members after every solve, which
+// converges to an orthonormal basis of the cluster's invariant subspace.
 __device__ inline void tridiag_evec(const double *a, const double *b, int n, double lam, double *yv,
-                             double *ws, unsigned char *sw) {
+                             double *ws, unsigned char *sw, const double *prev = nullptr,
+                             int nprev = 0) {
     double *D = ws, *U1 = ws + n, *U2 = ws + 2 * n, *M = ws + 3 * n;
     double nrm = 0.0;
     for (int i = 0; i < n; i++) nrm = fmax(nrm, fabs(a[i] - lam) + (i > 0 ? fabs(b[i]) : 0.0));
@@ -116,8 +125,12 @@ __device__ inline void tridiag_evec(const double *a, const double *b, int n, dou
     // reciprocal pivots: independent divisions here, multiplications on the
     // serial back substitutions below
     for (int i = 0; i < n; i++) D[i] = 1.0 / D[i];
-    for (int i = 0; i < n; i++) yv[i] = 1.0 / sqrt((double)n);
-    for (int it = 0; it < 3; it++) {
+    if (nprev > 0)
+        for (int i = 0; i < n; i++) yv[i] = random_start_value(i, 977ull + 131ull * (uint64_t)nprev) - 0.5;
+    else
+        for (int i = 0; i < n; i++) yv[i] = 1.0 / sqrt((double)n);
+    const int iters = nprev > 0 ? 5 : 3;
+    for (int it = 0; it < iters; it++) {
         for (int i = 0; i < n - 1; i++) {
             if (sw[i]) {
                 const double t = yv[i];
@@ -129,6 +142,13 @@ __device__ inline void tridiag_evec(const double *a, const double *b, int n, dou
         yv[n - 1] *= D[n - 1];
         if (n > 1) yv[n - 2] = (yv[n - 2] - U1[n - 2] * yv[n - 1]) * D[n - 2];
         for (int i = n - 3; i >= 0; i--) yv[i] = (yv[i] - U1[i] * yv[i + 1] - U2[i] * yv[i + 2]) * D[i];
+        for (int rep = 0; rep < 2 && nprev > 0; rep++)
+            for (int q = 0; q < nprev; q++) {
+                const double *pq = prev + (int64_t)q * n;
+                double d = 0.0;
+                for (int i = 0; i < n; i++) d += pq[i] * yv[i];
+                for (int i = 0; i < n; i++) yv[i] -= d * pq[i];
+            }
         double ss = 0.0;
         for (int i = 0; i < n; i++) ss += yv[i] * yv[i];
         ss = 1.0 / sqrt(ss);
@@ -212,8 +232,20 @@ __device__ inline bool ritz_multi_dev(const double *sa, const double *sb, int n,
     if ((threadIdx.x & 31) == 0 && w < lanes) {
         double *yv = work + (size_t)w * per, *ws = yv + n;
         unsigned char *sw = reinterpret_cast<unsigned char *>(ws + 4 * n);
-        for (int j = w; j < m; j += lanes) {
-            tridiag_evec(sa, sb, n, evals[j], yv, ws, sw);
+        // clusters: consecutive eigenvalues closer than 1e-3 |T| (dstein's
+        // ORTOL); lane w takes clusters w, w + lanes, ..., each member in turn
+        double tn = 0.0;
+        for (int i = 0; i < n; i++)
+            tn = fmax(tn, fabs(sa[i]) + (i > 0 ? fabs(sb[i]) : 0.0) + (i + 1 < n ? fabs(sb[i + 1]) : 0.0));
+        const double ortol = 1e-3 * tn;
+        int g = -1;
+        for (int j = 0, head = 0; j < m; j++) {
+            if (j == 0 || evals[j] - evals[j - 1] > ortol) {
+                head = j;
+                g++;
+            }
+            if (g % lanes != w) continue;
+            tridiag_evec(sa, sb, n, evals[j], yv, ws, sw, Y + (int64_t)head * n, j - head);
             for (int i = 0; i < n; i++) Y[(int64_t)j * n + i] = yv[i];
         }
     }
