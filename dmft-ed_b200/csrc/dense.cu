@@ -3,56 +3,66 @@
 // solver, taken when dim <= lanc_dim_threshold or Neigen == dim
 // (ED_DIAG.f90:136-137,184-194).
 //
-// One CTA of kDenseThreads threads diagonalises one sector, and the CTAs of a
-// launch take sectors from an atomic queue, largest first.  The matrix is
-// built from the context's factored hop tables (the elements ed_buildH_c
-// inserts, build_h.f90:29-53 with Himp/Hint/Hbath/Himp_bath) and diagonalised
-// by the cyclic Jacobi method with the round-robin ("chess tournament")
-// ordering of Brent and Luk: every round rotates npad/2 disjoint index pairs
-// at once, so the two-sided update J^T A J splits into independent 2 x 2
-// blocks and the eigenvector update V J into independent row pairs.  Jacobi
-// returns an orthonormal eigenbasis also for exactly degenerate eigenvalues,
-// which is what the reference's LAPACK eigh gives and what the ground-state
-// selection needs when a sector holds several ground states.  The rotation
-// is the symmetric Schur decomposition of Golub and Van Loan (Matrix
-// Computations, Alg. 8.4.1).  A and V live in global memory (L2-resident for
-// the default threshold, 256 states: 1 MB per sector).
+// One CTA of kDenseThreads threads solves one sector, and the CTAs of a launch
+// take sectors from an atomic queue, largest first.  The matrix is built from
+// the context's factored hop tables (the elements ed_buildH_c inserts,
+// build_h.f90:29-53 with Himp/Hint/Hbath/Himp_bath), then:
+//   1. Householder tridiagonalisation A = Q T Q^T (the unblocked reduction of
+//      LAPACK's dsytd2: per column a reflector H = I - tau v v^T, then the
+//      trailing block updated by the rank-2 form A - v w^T - w v^T with
+//      w = p - (tau/2)(p.v) v, p = tau A v); v overwrites the column below the
+//      diagonal and tau the diagonal entry, which T has already taken;
+//   2. the lowest m eigenpairs of T by Sturm multisection and inverse
+//      iteration (tridiag.cuh), with clusters of equal eigenvalues -- a sector
+//      holding several ground states -- given an orthonormal basis of their
+//      invariant subspace;
+//   3. the back-transformation x = H_0 H_1 ... H_{n-3} y of those m vectors.
+// A lives in global memory (L2-resident: 0.5 MB at the default threshold of
+// 256 states); the reflector and the product vectors live in shared memory.
 #include <algorithm>
 #include <vector>
 
 #include "internal.cuh"
 #include "sector.cuh"
+#include "tridiag.cuh"
 
 namespace dmfted {
 
 constexpr int kDenseThreads = 1024;
-constexpr int kDenseMaxSweeps = 40;
 
 struct DenseJob {
     int nup, ndw;
-    int n, npad;      // sector dimension, padded to even
+    int n;            // sector dimension
     int m;            // eigenpairs wanted (lowest m)
-    int slot;         // output slot: evals[slot * kDenseMaxEigen + j], sweeps[slot]
-    int64_t a_off;    // work: A (npad^2) then V (npad^2)
+    int slot;         // output slot: evals[slot * kDenseMaxEigen + j]
+    int64_t a_off;    // work: A (n x n, row-major)
     int64_t out_off;  // eigenvectors: m x n FP64, vector j at out_off + j*n
 };
 
-// Player in slot j (0..npad-1) of round r of the round-robin schedule: slot 0
-// keeps player 0, the others rotate.  Slots k and npad-1-k meet.
-__device__ __forceinline__ int rr_player(int j, int r, int npad) {
-    return j == 0 ? 0 : 1 + (j - 1 + r) % (npad - 1);
+// Sum over the block of one double per thread (plain FP64), returned in every
+// thread.  red: 32 doubles of shared memory.
+__device__ __forceinline__ double dense_block_sum(double x, double *red) {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = x;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    return t;
 }
 
 __global__ void __launch_bounds__(kDenseThreads, 1)
     k_dense_eigs(const BatchTables<double> tb, const DenseJob *jobs, int njobs, unsigned *queue,
-                 double *work, double *vecs, double *evals, int *sweeps, int64_t work_cap,
-                 int64_t vec_cap) {
-    __shared__ int s_p[kDenseMaxDim / 2], s_q[kDenseMaxDim / 2];
-    __shared__ double s_c[kDenseMaxDim / 2], s_s[kDenseMaxDim / 2];
-    __shared__ double s_red[2 * 32];
-    __shared__ double s_tot[2];
+                 double *work, double *vecs, double *evals, int64_t work_cap, int64_t vec_cap,
+                 int ritz_cap) {
+    extern __shared__ double dyn[];  // T (a, b), then the Ritz work space
+    __shared__ double s_v[kDenseMaxDim], s_p[kDenseMaxDim];
+    __shared__ double s_red[32];
+    __shared__ double s_ev[kDenseMaxEigen], s_est[kDenseMaxEigen];
+    __shared__ double s_tau, s_k;
     __shared__ int s_job;
-    const int tid = threadIdx.x, bd = blockDim.x;
+    const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    const int nwarp = bd >> 5;
     const int ni = 1 << tb.norb;
     const uint32_t imask = (uint32_t)ni - 1u;
     for (;;) {
@@ -62,24 +72,20 @@ __global__ void __launch_bounds__(kDenseThreads, 1)
         __syncthreads();
         if (jid >= njobs) break;
         const DenseJob J = jobs[jid];
-        const int n = J.n, np = J.npad, h = np / 2;
-        if (!DM_IN(J.a_off + 2 * (int64_t)np * np - 1, work_cap) ||
-            !DM_IN(J.out_off + (int64_t)J.m * n - 1, vec_cap) || !DM_IN(np, kDenseMaxDim + 1) ||
-            !DM_IN(J.m, kDenseMaxEigen + 1))
+        const int n = J.n;
+        if (!DM_IN(J.a_off + (int64_t)n * n - 1, work_cap) ||
+            !DM_IN(J.out_off + (int64_t)J.m * n - 1, vec_cap) || !DM_IN(n, kDenseMaxDim + 1) ||
+            !DM_IN(J.m, kDenseMaxEigen + 1) || !DM_IN(2 * n, ritz_cap + 1))
             continue;
-        double *A = work + J.a_off, *V = A + (int64_t)np * np;
+        double *A = work + J.a_off;
         const Sec<double> s = make_sec(tb, J.nup, J.ndw);
-        for (int64_t t = tid; t < (int64_t)np * np; t += bd) {
-            const int i = (int)(t / np), j = (int)(t % np);
-            A[t] = 0.0;
-            V[t] = i == j ? 1.0 : 0.0;
-        }
+        for (int64_t t = tid; t < (int64_t)n * n; t += bd) A[t] = 0.0;
         __syncthreads();
         // row i = r + DimUp*q: diagonal, up hops (same column q), down hops
         // (same row r of the neighbouring columns)
         for (int i = tid; i < n; i += bd) {
             const uint32_t r = (uint32_t)i % s.dimup, q = (uint32_t)i / s.dimup;
-            double *row = A + (int64_t)i * np;
+            double *row = A + (int64_t)i * n;
             row[i] = s.du[r] + s.dd[q] + tb.dint[(s.wu[r] & imask) * ni + (s.wd[q] & imask)];
             for (int e = 0; e < s.cu[r]; e++) {
                 const uint32_t en = s.eu[(int64_t)e * s.dimup + r];
@@ -95,119 +101,94 @@ __global__ void __launch_bounds__(kDenseThreads, 1)
             }
         }
         __syncthreads();
-        int sweep = 0;
-        double prev = 0.0;
-        for (; sweep < kDenseMaxSweeps; sweep++) {
-            // off-diagonal and total squared norms
-            double off = 0.0, tot = 0.0;
-            for (int64_t t = tid; t < (int64_t)n * np; t += bd) {
-                const int i = (int)(t / np), j = (int)(t % np);
-                if (j >= n) continue;
-                const double a = A[t], a2 = a * a;
-                tot += a2;
-                if (i != j) off += a2;
+        double *sa = dyn, *sb = dyn + n;
+        if (tid == 0) sb[0] = 0.0;
+        // ---- 1. tridiagonalisation -------------------------------------------
+        for (int k = 0; k + 1 < n; k++) {
+            const int m = n - k - 1;  // length of the column below the diagonal
+            double part = 0.0;
+            for (int i = tid; i < m; i += bd) {
+                const double x = A[(int64_t)(k + 1 + i) * n + k];
+                s_v[i] = x;
+                if (i > 0) part += x * x;
             }
-            for (int o = 16; o > 0; o >>= 1) {
-                off += __shfl_xor_sync(0xffffffffu, off, o);
-                tot += __shfl_xor_sync(0xffffffffu, tot, o);
-            }
-            if ((tid & 31) == 0) {
-                s_red[tid >> 5] = off;
-                s_red[32 + (tid >> 5)] = tot;
-            }
-            __syncthreads();
+            const double tail = dense_block_sum(part, s_red);  // |x|^2 without x_0
             if (tid == 0) {
-                double a = 0.0, b = 0.0;
-                for (int w = 0; w < (bd >> 5); w++) {
-                    a += s_red[w];
-                    b += s_red[32 + w];
+                const double x0 = s_v[0];
+                sa[k] = A[(int64_t)k * n + k];
+                if (m == 1 || tail == 0.0) {
+                    s_tau = 0.0;  // already tridiagonal in this column
+                    sb[k + 1] = x0;
+                } else {
+                    const double nx = sqrt(x0 * x0 + tail);
+                    const double alpha = x0 >= 0.0 ? -nx : nx;
+                    const double v0 = x0 - alpha;
+                    s_v[0] = v0;
+                    s_tau = 2.0 / (v0 * v0 + tail);
+                    sb[k + 1] = alpha;
                 }
-                s_tot[0] = a;
-                s_tot[1] = b;
+                A[(int64_t)k * n + k] = s_tau;  // T holds a_k now; keep tau here
             }
             __syncthreads();
-            const double offn = s_tot[0], totn = s_tot[1];
+            const double tau = s_tau;
+            if (tau == 0.0) continue;
+            for (int i = tid; i < m; i += bd) A[(int64_t)(k + 1 + i) * n + k] = s_v[i];
+            // p = tau A_sub v, one warp per row
+            for (int i = warp; i < m; i += nwarp) {
+                const double *row = A + (int64_t)(k + 1 + i) * n + (k + 1);
+                double d = 0.0;
+                for (int j = lane; j < m; j += 32) d += row[j] * s_v[j];
+                for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+                if (lane == 0) s_p[i] = tau * d;
+            }
             __syncthreads();
-            // converged when the off-diagonal norm is below 1e-14 |A|_F, or
-            // once it is below 1e-10 |A|_F and a sweep no longer reduces it
-            // (rounding level of a large matrix)
-            if (!(offn > 1e-28 * totn)) break;
-            if (sweep > 0 && offn <= 1e-20 * totn && offn >= 0.25 * prev) break;
-            prev = offn;
-            for (int round = 0; round < np - 1; round++) {
-                for (int k = tid; k < h; k += bd) {
-                    int p = rr_player(k, round, np), q = rr_player(np - 1 - k, round, np);
-                    if (p > q) {
-                        const int t = p;
-                        p = q;
-                        q = t;
-                    }
-                    const double app = A[(int64_t)p * np + p], aqq = A[(int64_t)q * np + q];
-                    const double apq = A[(int64_t)p * np + q];
-                    double c = 1.0, sn = 0.0;
-                    if (apq != 0.0) {
-                        const double tau = (aqq - app) / (2.0 * apq);
-                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                        c = 1.0 / sqrt(1.0 + t * t);
-                        sn = t * c;
-                    }
-                    s_p[k] = p;
-                    s_q[k] = q;
-                    s_c[k] = c;
-                    s_s[k] = sn;
-                }
-                __syncthreads();
-                // A <- J^T A J on the 2 x 2 blocks (rows of pair k1, columns of pair k2)
-                for (int b = tid; b < h * h; b += bd) {
-                    const int k1 = b / h, k2 = b % h;
-                    const int p1 = s_p[k1], q1 = s_q[k1], p2 = s_p[k2], q2 = s_q[k2];
-                    const double c1 = s_c[k1], s1 = s_s[k1], c2 = s_c[k2], s2 = s_s[k2];
-                    double *r1 = A + (int64_t)p1 * np, *r2 = A + (int64_t)q1 * np;
-                    const double x11 = r1[p2], x12 = r1[q2], x21 = r2[p2], x22 = r2[q2];
-                    const double y11 = c1 * x11 - s1 * x21, y12 = c1 * x12 - s1 * x22;
-                    const double y21 = s1 * x11 + c1 * x21, y22 = s1 * x12 + c1 * x22;
-                    double z11 = c2 * y11 - s2 * y12, z12 = s2 * y11 + c2 * y12;
-                    double z21 = c2 * y21 - s2 * y22, z22 = s2 * y21 + c2 * y22;
-                    if (k1 == k2) z12 = z21 = 0.0;  // the rotated pair is annihilated
-                    r1[p2] = z11;
-                    r1[q2] = z12;
-                    r2[p2] = z21;
-                    r2[q2] = z22;
-                }
-                // V <- V J
-                for (int b = tid; b < np * h; b += bd) {
-                    const int i = b / h, k = b % h;
-                    double *vr = V + (int64_t)i * np;
-                    const int p = s_p[k], q = s_q[k];
-                    const double c = s_c[k], sn = s_s[k];
-                    const double vp = vr[p], vq = vr[q];
-                    vr[p] = c * vp - sn * vq;
-                    vr[q] = sn * vp + c * vq;
-                }
-                __syncthreads();
+            part = 0.0;
+            for (int i = tid; i < m; i += bd) part += s_p[i] * s_v[i];
+            const double kk = 0.5 * tau * dense_block_sum(part, s_red);
+            for (int i = tid; i < m; i += bd) s_p[i] -= kk * s_v[i];  // w
+            __syncthreads();
+            // A_sub -= v w^T + w v^T
+            for (int64_t t = tid; t < (int64_t)m * m; t += bd) {
+                const int i = (int)(t / m), j = (int)(t % m);
+                A[(int64_t)(k + 1 + i) * n + (k + 1 + j)] -= s_v[i] * s_p[j] + s_p[i] * s_v[j];
             }
+            __syncthreads();
         }
-        // rank of each eigenvalue (ties by index); the lowest m are written
-        for (int i = tid; i < n; i += bd) {
-            const double di = A[(int64_t)i * np + i];
-            int rk = 0;
-            for (int j = 0; j < n; j++) {
-                const double dj = A[(int64_t)j * np + j];
-                rk += (dj < di || (dj == di && j < i)) ? 1 : 0;
-            }
-            if (rk < J.m) {
-                evals[(int64_t)J.slot * kDenseMaxEigen + rk] = di;
-                s_p[rk] = i;  // column of V (the pair arrays are free now)
-            }
-        }
+        if (tid == 0) sa[n - 1] = A[(int64_t)(n - 1) * n + (n - 1)];
         __syncthreads();
-        for (int64_t t = tid; t < (int64_t)J.m * n; t += bd) {
-            const int j = (int)(t / n), row = (int)(t % n);
-            vecs[J.out_off + t] = V[(int64_t)row * np + s_p[j]];
+        // ---- 2. lowest m eigenpairs of T ---------------------------------------
+        double *Y = vecs + J.out_off;
+        ritz_multi_dev(sa, sb, n, J.m, 1.0, 0.0, s_ev, Y, s_est, dyn + 2 * n, ritz_cap - 2 * n);
+        // ---- 3. back-transformation x = H_0 ... H_{n-3} y ----------------------
+        for (int k = n - 2; k >= 0; k--) {
+            const double tau = A[(int64_t)k * n + k];
+            if (tau == 0.0) continue;  // uniform: every thread reads the same value
+            const int m = n - k - 1;
+            for (int i = tid; i < m; i += bd) s_v[i] = A[(int64_t)(k + 1 + i) * n + k];
+            __syncthreads();
+            for (int j = warp; j < J.m; j += nwarp) {
+                double *y = Y + (int64_t)j * n + (k + 1);
+                double d = 0.0;
+                for (int i = lane; i < m; i += 32) d += s_v[i] * y[i];
+                for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+                d *= tau;
+                for (int i = lane; i < m; i += 32) y[i] -= d * s_v[i];
+            }
+            __syncthreads();
         }
-        if (tid == 0) sweeps[J.slot] = sweep;
+        for (int j = tid; j < J.m; j += bd) evals[(int64_t)J.slot * kDenseMaxEigen + j] = s_ev[j];
         __syncthreads();
     }
+}
+
+// Dynamic shared memory of k_dense_eigs for sectors of up to n states and m
+// eigenpairs: T (2n) and as many inverse-iteration work spaces (up to 8) as
+// fit in 190 KB.  Returns the size in doubles.
+static int dense_ritz_doubles(int n, int m) {
+    const int per = ritz_evec_doubles(n);
+    int lanes = std::max(1, std::min(8, m));
+    while (lanes > 1 && (2 * n + lanes * per) * 8 > 190 * 1024) lanes--;
+    return 2 * n + lanes * per;
 }
 
 // Host side: the lowest want[i] eigenpairs of every sector list[i] whose
@@ -230,13 +211,11 @@ void dense_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<i
         J.nup = s.nup;
         J.ndw = s.ndw;
         J.n = (int)s.dim;
-        J.npad = (int)((s.dim + 1) / 2 * 2);
-        if (J.npad < 2) J.npad = 2;
         J.m = (int)std::min<int64_t>(want[i], s.dim);
         J.slot = (int)jobs.size();
         J.a_off = work;
         J.out_off = vec;
-        work += 2 * (int64_t)J.npad * J.npad;
+        work += ((int64_t)J.n * J.n + 31) / 32 * 32;
         vec += ((int64_t)J.m * J.n + 31) / 32 * 32;
         jobs.push_back(J);
         where.push_back((int)i);
@@ -245,40 +224,42 @@ void dense_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<i
     const int nj = (int)jobs.size();
     std::vector<DenseJob> q = jobs;
     std::stable_sort(q.begin(), q.end(), [](const DenseJob &a, const DenseJob &b) {
-        return a.npad > b.npad;
+        return a.n > b.n;
     });
+    int nmax = 1, mmax = 1;
+    for (auto &J : q) {
+        nmax = std::max(nmax, J.n);
+        mmax = std::max(mmax, J.m);
+    }
+    const int rcap = dense_ritz_doubles(nmax, mmax);
     c->dense_work.alloc((size_t)work);
     c->dense_vec.alloc((size_t)vec);
     c->dense_eval.alloc((size_t)nj * kDenseMaxEigen);
-    c->dense_int.alloc((size_t)nj + 1);
+    c->dense_int.alloc(1);
     c->dense_jobs.alloc((size_t)nj * sizeof(DenseJob));
     DM_CUDA(cudaMemcpyAsync(c->dense_jobs.p, q.data(), nj * sizeof(DenseJob),
                             cudaMemcpyHostToDevice, c->stream));
-    DM_CUDA(cudaMemsetAsync(c->dense_int.p + nj, 0, sizeof(int), c->stream));
+    DM_CUDA(cudaMemsetAsync(c->dense_int.p, 0, sizeof(int), c->stream));
     const int grid = std::min(nj, num_sms(c));
-    k_dense_eigs<<<grid, kDenseThreads, 0, c->stream>>>(
+    DM_CUDA(cudaFuncSetAttribute(k_dense_eigs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 rcap * (int)sizeof(double)));
+    k_dense_eigs<<<grid, kDenseThreads, rcap * sizeof(double), c->stream>>>(
         batch_tables<double>(c), reinterpret_cast<const DenseJob *>(c->dense_jobs.p), nj,
-        reinterpret_cast<unsigned *>(c->dense_int.p + nj), c->dense_work.p, c->dense_vec.p,
-        c->dense_eval.p, c->dense_int.p, (int64_t)c->dense_work.n, (int64_t)c->dense_vec.n);
+        reinterpret_cast<unsigned *>(c->dense_int.p), c->dense_work.p, c->dense_vec.p,
+        c->dense_eval.p, (int64_t)c->dense_work.n, (int64_t)c->dense_vec.n, rcap);
     DM_CHECK_LAUNCH();
     c->launches++;
     std::vector<double> ev((size_t)nj * kDenseMaxEigen);
-    std::vector<int> sw(nj);
     DM_CUDA(cudaMemcpyAsync(ev.data(), c->dense_eval.p, ev.size() * sizeof(double),
                             cudaMemcpyDeviceToHost, c->stream));
-    DM_CUDA(cudaMemcpyAsync(sw.data(), c->dense_int.p, nj * sizeof(int), cudaMemcpyDeviceToHost,
-                            c->stream));
     DM_CUDA(cudaStreamSynchronize(c->stream));
     for (int j = 0; j < nj; j++) {
         const DenseJob &J = jobs[j];
         DenseEig &r = res[where[j]];
         r.m = J.m;
-        r.sweeps = sw[J.slot];
         r.evals.assign(ev.begin() + (size_t)J.slot * kDenseMaxEigen,
                        ev.begin() + (size_t)J.slot * kDenseMaxEigen + J.m);
         r.vecs = c->dense_vec.p + J.out_off;
-        DM_REQUIRE(r.sweeps < kDenseMaxSweeps, DMFTED_ERR_NOTCONV,
-                   "dense sector eigensolve: Jacobi sweeps did not converge");
     }
 }
 

@@ -141,26 +141,58 @@ double *slot_ptr(dmfted_ctx *c, const SectorJob &j, int k) {
     return c->lockpool.p + j.base + (int64_t)k * j.s.dim;
 }
 
-// The largest probe eigenvalue the sector still wants (+inf: any).
-double probe_top(const dmfted_ctx *c, const SectorJob &j, bool finite_t) {
+// Zero temperature: the ground-state window above energy e0.
+double t0_window(const dmfted_ctx *c, double e0) {
+    return e0 + 11.0 * c->p.gs_threshold + 4.0 * c->p.lanc_tolerance * std::max(1.0, std::fabs(e0));
+}
+
+// The largest probe eigenvalue the sector still wants (+inf: any).  cut: an
+// energy at or above which no state can enter the list any more (the T=0
+// window of the lowest energy of all sectors, or the lanc_nstates_total-th
+// lowest energy found at finite T; +inf when unknown).
+double probe_top(const dmfted_ctx *c, const SectorJob &j, bool finite_t, double cut) {
     const int n = (int)j.e.size();
     if (!finite_t) {
         const double e0 = *std::min_element(j.e.begin(), j.e.end());
-        return e0 + 11.0 * c->p.gs_threshold +
-               4.0 * c->p.lanc_tolerance * std::max(1.0, std::fabs(e0));
+        return std::min(t0_window(c, e0), cut);
     }
-    if (n < j.neigen) return 1e300;
+    if (n < j.neigen) return cut;
     std::vector<double> srt = j.e;
     std::sort(srt.begin(), srt.end());
     const double top = srt[j.neigen - 1];
-    return top - 1e-12 * std::max(1.0, std::fabs(top));
+    return std::min(top - 1e-12 * std::max(1.0, std::fabs(top)), cut);
 }
 
 // Whether probe eigenvalue mu joins the sector's wanted set.
-bool probe_accepts(const dmfted_ctx *c, const SectorJob &j, double mu, bool finite_t) {
+bool probe_accepts(const dmfted_ctx *c, const SectorJob &j, double mu, bool finite_t,
+                   double cut) {
     const int n = (int)j.e.size();
     if (n >= j.cap || (!finite_t && n >= j.neigen)) return false;
-    return finite_t ? mu < probe_top(c, j, true) : mu <= probe_top(c, j, false);
+    return finite_t ? mu < probe_top(c, j, true, cut) : mu <= probe_top(c, j, false, cut);
+}
+
+// The energy cut of the whole diagonalisation (see probe_top): at T=0 the
+// window above the lowest energy found in any sector; at finite T with a list
+// cap, the cap-th lowest of every sector's lowest Neigen energies (a later
+// probe only adds energies, so the final list boundary can only be lower).
+double list_cut(const dmfted_ctx *c, const std::vector<SectorJob> &jobs, bool finite_t,
+                int list_cap) {
+    if (!finite_t) {
+        double emin = 1e300;
+        for (auto &j : jobs)
+            for (double e : j.e) emin = std::min(emin, e);
+        return emin < 1e300 ? t0_window(c, emin) : 1e300;
+    }
+    if (list_cap <= 0) return 1e300;
+    std::vector<double> all;
+    for (auto &j : jobs) {
+        std::vector<double> srt = j.e;
+        std::sort(srt.begin(), srt.end());
+        for (int k = 0; k < (int)srt.size() && k < j.neigen; k++) all.push_back(srt[k]);
+    }
+    if ((int)all.size() < list_cap) return 1e300;
+    std::nth_element(all.begin(), all.begin() + (list_cap - 1), all.end());
+    return all[list_cap - 1];
 }
 
 }  // namespace
@@ -170,7 +202,8 @@ bool probe_accepts(const dmfted_ctx *c, const SectorJob &j, double mu, bool fini
 // single-sector contract of dmfted_gs_lanczos (finite-T rule).  On return
 // every job holds its eigenvalues in j.e and its vectors in the lock pool (or
 // dense_vecs), in slot order.  Returns the H*v products used.
-static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool finite_t) {
+static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool finite_t,
+                              int list_cap) {
     const dmfted_params &p = c->p;
     const bool dbg = getenv("DMFTED_DEBUG_EIGS") != nullptr;
     double t_last = 0.0;
@@ -298,6 +331,12 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
         std::vector<LockSpec> locks;
         std::vector<size_t> at;
         bool any = false;
+        // sectors whose lowest energy is at or above the cut cannot put a
+        // state into the list, whatever copies a probe would find
+        const double cut = list_cut(c, jobs, finite_t, list_cap);
+        for (auto &j : jobs)
+            if (j.probing && !j.e.empty() && *std::min_element(j.e.begin(), j.e.end()) >= cut)
+                j.probing = false;
         for (size_t i = 0; i < jobs.size(); i++) {
             SectorJob &j = jobs[i];
             if (!j.probing) continue;
@@ -308,7 +347,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
                 LockSpec ls;
                 ls.off = j.base;
                 ls.n = (int)j.e.size();
-                ls.top = probe_top(c, j, finite_t);
+                ls.top = probe_top(c, j, finite_t, cut);
                 locks.push_back(ls);
                 at.push_back(i);
             }
@@ -325,7 +364,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
                 hv += br[k].steps;
                 show("batch probe", j, br[k].steps, std::max(br[k].m, 0), br[k].evals.data(),
                      (int)j.e.size());
-                if (br[k].m >= 1 && probe_accepts(c, j, br[k].evals[0], finite_t)) {
+                if (br[k].m >= 1 && probe_accepts(c, j, br[k].evals[0], finite_t, cut)) {
                     DM_CUDA(cudaMemcpyAsync(slot_ptr(c, j, (int)j.e.size()), br[k].vecs,
                                             j.s.dim * sizeof(double), cudaMemcpyDeviceToDevice,
                                             c->stream));
@@ -342,11 +381,11 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
             c->eigvecs.alloc((size_t)j.s.dim);
             const int m = lanczos_eigs(c, j.s, 1, DMFTED_FP64, p.lanc_tolerance, nit, ev.data(),
                                        c->eigvecs.p, &steps, slot_ptr(c, j, 0), (int)j.e.size(),
-                                       probe_top(c, j, finite_t));
+                                       probe_top(c, j, finite_t, cut));
             j.steps += steps;
             hv += steps;
             show("grid probe", j, steps, m, ev.data(), (int)j.e.size());
-            if (m >= 1 && probe_accepts(c, j, ev[0], finite_t)) {
+            if (m >= 1 && probe_accepts(c, j, ev[0], finite_t, cut)) {
                 DM_CUDA(cudaMemcpyAsync(slot_ptr(c, j, (int)j.e.size()), c->eigvecs.p,
                                         j.s.dim * sizeof(double), cudaMemcpyDeviceToDevice,
                                         c->stream));
@@ -390,7 +429,7 @@ int64_t ed_diag(dmfted_ctx *c, const std::vector<int> &list) {
         if (j.neigen <= 0) continue;
         jobs.push_back(j);
     }
-    const int64_t hv = sector_spectra(c, jobs, c->finite_t);
+    const int64_t hv = sector_spectra(c, jobs, c->finite_t, c->finite_t ? c->nstates_total : 0);
     if (c->finite_t) {
         // ED_DIAG.f90:196-200: i = 1..Neigen into the capped list
         for (auto &j : jobs)
@@ -427,7 +466,7 @@ int sector_eigenpairs(dmfted_ctx *c, int isector, int neigen, double *evals_h, d
     jobs[0].isector = isector;
     jobs[0].neigen = (int)std::min<int64_t>(state_dim(c, isector), neigen);
     const bool ft = neigen > 1;
-    const int64_t hv = sector_spectra(c, jobs, ft);
+    const int64_t hv = sector_spectra(c, jobs, ft, 0);
     if (steps) *steps = hv;
     const auto pr = ordered_pairs(c, jobs[0], jobs[0].neigen);
     const int64_t dim = state_dim(c, isector);

@@ -360,14 +360,14 @@ void batch_chains_gf(dmfted_ctx *c, const std::vector<ChainRec> &recs, int preci
 void fock_build_map(dmfted_ctx *c, int isector, int32_t *d_map);  // combined map
 
 // ---- dense.cu ------------------------------------------------------------
-// Dense eigensolve (Jacobi, one CTA per sector) of the sectors ed_diag_c
+// Dense eigensolve (Householder + tridiagonal, one CTA per sector) of the sectors ed_diag_c
 // hands to eigh: the lowest want[i] eigenpairs of sector list[i] (want 0:
 // skipped, m = -1).  Vectors are FP64 at vecs, dim apart, owned by the
 // context until the next call.
 constexpr int kDenseMaxDim = 1024;
 constexpr int kDenseMaxEigen = 64;
 struct DenseEig {
-    int m = -1, sweeps = 0;
+    int m = -1;
     std::vector<double> evals;
     const double *vecs = nullptr;
 };
