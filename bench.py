@@ -133,21 +133,45 @@ def seeded_bath_2orb(seed=4, norb=2, nbath=4):
     return np.concatenate([e.reshape(-1), v.reshape(-1)])
 
 
+def config_pins():
+    """Oracle fixtures of the workload configurations (tests/golden), or None."""
+    try:
+        return np.load(os.path.join(ROOT, "tests", "golden", "config_pins.npz"))
+    except OSError:
+        return None
+
+
 def finite_t_workload(dmfted, device, steps, warmup):
-    """Norb=2, Nbath=4 (Ns=10), U=3, J=0.5, Ust=U-2J, beta=50: every one of the
-    121 sectors diagonalised, lanc_nstates_total=16 lowest states kept, the
-    particle/hole chains of every kept state, spin and orbital -- all in the
-    persistent work-queue kernels."""
-    bath = seeded_bath_2orb()
+    """Norb=2, Nbath=4 (Ns=10), U=3, J=0.5, Ust=U-2J, beta=50, Nspin=2 (the
+    same bath for both spins): every one of the 121 sectors diagonalised,
+    lanc_nstates_total=16 lowest states kept, the particle/hole chains of
+    every kept state, spin and orbital -- all in the persistent work-queue
+    kernels."""
+    b1 = seeded_bath_2orb()
+    nb = b1.size // 2
+    bath = np.concatenate([b1[:nb], b1[:nb], b1[nb:], b1[nb:]])  # Nspin=2, same bath per spin
+    pins = config_pins()
     out = {}
     ref_g = None
     for prec in (dmfted.FP64, dmfted.MIXED):
-        p = dmfted.default_params(norb=2, nbath=4, uloc=[3.0, 3.0], ust=2.0, jh=0.5, beta=50.0,
-                                  lmats=LMATS, lreal=0, lanc_nstates_total=16, precision=prec,
-                                  device=device)
+        p = dmfted.default_params(norb=2, nbath=4, nspin=2, uloc=[3.0, 3.0], ust=2.0, jh=0.5,
+                                  beta=50.0, lmats=LMATS, lreal=0, lanc_nstates_total=16,
+                                  precision=prec, device=device)
         s = dmfted.EDSolver(p)
-        for _ in range(warmup):
+        oracle = None
+        for w in range(max(1, warmup)):
             s.ed_solve(bath)
+            if w == 0 and pins is not None and "cfg4_gmats" in pins:
+                # the first solve (lanc_nstates_total = 16, Neigen = 6) against
+                # the oracle fixture; later solves adapt the state counts
+                e, _, z = s.eigenspace()
+                g0 = s.ed_get_gimp_matsubara()
+                oracle = dict(
+                    fixture="tests/golden/config_pins.npz cfg4 (first solve)",
+                    dE0_rel=abs(e[0] - float(pins["cfg4_e"][0])) / abs(float(pins["cfg4_e"][0])),
+                    dZ_rel=abs(z - float(pins["cfg4_zeta"])) / float(pins["cfg4_zeta"]),
+                    max_dG=max(float(np.abs(g0[i, i, a, a] - pins["cfg4_gmats"][i, a]).max())
+                               for i in range(2) for a in range(2)))
         ms, launches = [], 0
         for _ in range(steps):
             s.launch_count(reset=True)
@@ -163,7 +187,7 @@ def finite_t_workload(dmfted, device, steps, warmup):
             ms_per_solve=statistics.median(ms), launches_per_solve=launches,
             states_kept=len(e), gf_chains=tm["hv_gf"] // NGF, diag_ms=tm["diag_ms"],
             gf_ms=tm["gf_ms"], max_dG_vs_fp64=float(np.abs(g - ref_g).max()),
-            autotune=s.autotune_log())
+            vs_oracle=oracle, autotune=s.autotune_log())
         s.close()
     return out
 
@@ -312,7 +336,12 @@ def run_ours(args, rank, world, local_rank):
         s.hxv_timing(False)
         launches = s.launch_count(reset=True)
         dist_barrier(world)
-        e2e = [e2e_step(s) for _ in range(max(1, min(args.steps, 3)))]
+        # the same K steps through the public API, L2 flushed between them
+        # (outside each step's own interval)
+        e2e = []
+        for _ in range(args.steps):
+            e2e.append(e2e_step(s))
+            l2_flush(dev)
         res[prec] = dict(ms=ms, clocks=clk.summary(), launches=launches, e2e_ms=[x[0] for x in e2e],
                          g=e2e[-1][1], e0=s.egs(), obs=e2e[-1][3], tm=s.timings(), hvt=hvt)
     # H*v of the sector alone, both precisions (device events on the library stream)
@@ -386,6 +415,91 @@ def cpu_step_seconds(t_map, t_hv, hv_per_step):
     return 3 * t_map + t_hv * hv_per_step
 
 
+def reference_hv_per_step():
+    """H*v products of one DMFT step of the reference on the 7/7 sector: the
+    plain Lanczos ground state (its step count, taken from the oracle's own
+    run in the cfg3 fixture), the second pass that rebuilds the vector
+    (PLAIN_LANCZOS.f90:286-385: one product fewer), and the particle and hole
+    chains (2 x lanc_ngfiter)."""
+    pins = config_pins()
+    nl = int(pins["cfg3_nlanc"]) if pins is not None and "cfg3_nlanc" in pins else 170
+    return 2 * nl - 1 + 2 * NGF, nl
+
+
+def small_solve_check(nthreads):
+    """The model behind the extrapolation (3 map builds + per-product time x
+    products) against a complete oracle solve, measured end to end, on the
+    small configuration (Ns=8, sector 4/4, dim 4900, U=2, Lmats=4096): plain
+    Lanczos ground state with its second pass, observables, two 200-step
+    chains, G and Sigma."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    m = O.seeded_model(SEED, nbath=7, u=2.0, beta=BETA)
+    out = {}
+    for nt in (1, nthreads):
+        t0 = time.perf_counter()
+        r = O.solve_t0(m, sectors=[(4, 4)], nstates_sector=1, lmats=LMATS, nthreads=nt)
+        t_full = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        hm = O.build_sector(m.ns, 4, 4)
+        t_map = time.perf_counter() - t0
+        v = O.start_vector(hm.size)
+        reps = 50
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            v = O.hxv(m, hm, v, nthreads=nt)
+            v /= np.linalg.norm(v)
+        t_hv = (time.perf_counter() - t0) / reps
+        hv = 2 * r["nlanc"] - 1 + 2 * NGF
+        out[f"threads_{nt}"] = dict(measured_s=t_full, model_s=cpu_step_seconds(t_map, t_hv, hv),
+                                    hv_per_step=hv)
+    return out
+
+
+def reference_arm(args, nthreads):
+    """--impl reference: the reference's algorithm (the oracle restatement of
+    directMatVec_cc with the combined map and binary search, complex128, and
+    the plain Lanczos) timed on the host cores.  A complete Ns=14 step takes
+    about a quarter of an hour on 16 threads, so each timed step is a bounded
+    sample -- the map build and one product on the same sector -- scaled to
+    the products of one DMFT step (kind port-extrapolated).  Once per run: a
+    single-thread product (the reference runs one thread per MPI rank), and
+    the extrapolation model against complete oracle solves of the small
+    configuration, single-thread and on every core."""
+    hv_per_step, nl = reference_hv_per_step()
+    samples = []
+    t_wall0 = time.perf_counter()
+    for i in range(args.warmup + args.steps):
+        t_map, t_hv = cpu_sample(nthreads, 1)
+        if i >= args.warmup:
+            samples.append(cpu_step_seconds(t_map, t_hv, hv_per_step))
+    t_sampled = time.perf_counter() - t_wall0
+    sec = statistics.mean(samples)
+    val = 1.0 / sec
+    t_map1, t_hv1 = cpu_sample(1, 1)
+    single = 1.0 / cpu_step_seconds(t_map1, t_hv1, hv_per_step)
+    check = small_solve_check(nthreads)
+    return dict(
+        metric=METRIC, value=val, unit=UNIT, n_gpus=args.gpus, steps=args.steps,
+        warmup=args.warmup, ms_per_step=sec * 1e3, higher_is_better=True, scaling="weak",
+        vs_baseline=None, dtype="c128", data="synthetic", impl="reference",
+        config={"workload": "impurity solve Ns=14 (Nbath=13, U=3, beta=100) sector 7/7 "
+                            "dim 11778624: Lanczos GS + observables + particle/hole chains "
+                            "(200 steps) + G, Sigma on Lmats=4096",
+                "lanc_nstates_sector": 1, "parallelism": f"{nthreads} host threads"},
+        cpu_baseline=dict(
+            value=val, unit=UNIT, cores=nthreads, kind="port-extrapolated",
+            sample=(f"per step: the map build and 1 oracle directMatVec_cc (complex128, "
+                    f"binary-search map) on the 7/7 sector with {nthreads} threads, scaled to "
+                    f"{hv_per_step} H*v per DMFT step (plain Lanczos: {nl} steps, the second "
+                    f"pass, 2 x {NGF} chain steps) + 3 map builds"),
+            single_thread=dict(value=single, unit=UNIT, cores=1,
+                               sample="the map build and 1 product on one thread, same scaling"),
+            model_check_small_config=check,
+            sampled_wall_s=t_sampled),
+        e2e=dict(value=val, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -407,30 +521,7 @@ def main():
         # Fortran reference cannot be built here), rank 0 only
         if rank != 0:
             return
-        # one DMFT step of the reference = the H*v products of the GPU run's
-        # step (GS iterations, the eigenvector replay pass, 2 x 200 chain steps)
-        hv_per_step = 2 * 170 + 2 * NGF
-        samples = []
-        for i in range(args.warmup + args.steps):
-            t_map, t_hv = cpu_sample(nthreads, 1)
-            if i >= args.warmup:
-                samples.append(cpu_step_seconds(t_map, t_hv, hv_per_step))
-        sec = statistics.mean(samples)
-        val = 1.0 / sec
-        line = dict(metric=METRIC, value=val, unit=UNIT, n_gpus=args.gpus, steps=args.steps,
-                    warmup=args.warmup, ms_per_step=sec * 1e3, higher_is_better=True,
-                    scaling="weak", vs_baseline=None, dtype="c128", data="synthetic",
-                    impl="reference",
-                    config={"workload": "impurity solve Ns=14 (Nbath=13) sector 7/7 dim 11778624, "
-                                        "GS + G(iwn) Lmats=4096, 200-step chains",
-                            "parallelism": "host threads"},
-                    cpu_baseline=dict(value=val, unit=UNIT, cores=nthreads, kind="port",
-                                      sample=f"per step: 1 oracle directMatVec_cc (complex128, "
-                                             f"binary-search map) on the 7/7 sector with {nthreads} "
-                                             f"threads + the map build, scaled to {hv_per_step} "
-                                             f"H*v per DMFT step"),
-                    e2e=dict(value=val, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
-        print(json.dumps(line))
+        print(json.dumps(reference_arm(args, nthreads)))
         return
 
     if world > 1:
@@ -473,6 +564,18 @@ def main():
     traffic = prof * per_launch / (3 * dim * 4) if prof else None
     g_err = float(np.abs(mixed["g"] - fp64["g"]).max())
     e_err = abs(mixed["e0"] - fp64["e0"]) / abs(fp64["e0"])
+    pins = config_pins()
+    vs_oracle = None
+    if pins is not None and "cfg3_gmats" in pins:
+        e_ref = float(pins["cfg3_e0"])
+        vs_oracle = dict(fixture="tests/golden/config_pins.npz cfg3 (oracle solve of the same "
+                                 "sector and bath)")
+        for name, r in (("mixed", mixed), ("fp64", fp64)):
+            vs_oracle[name] = dict(dE0_rel=abs(r["e0"] - e_ref) / abs(e_ref),
+                                   max_dG=float(np.abs(r["g"][0, 0, 0, 0] -
+                                                       pins["cfg3_gmats"]).max()),
+                                   max_d_docc=float(np.abs(r["obs"]["docc"] -
+                                                           pins["cfg3_docc"]).max()))
     if world > 1:
         dist_barrier(world)
     if rank != 0:
@@ -497,6 +600,7 @@ def main():
         fp64_dropin=dict(ms_per_step=t_fp64 / args.steps * 1e3,
                          speedup_mixed_vs_fp64=t_fp64 / t_mixed,
                          mixed_vs_fp64_dE0_rel=e_err, mixed_vs_fp64_max_dG=g_err),
+        vs_oracle=vs_oracle,
         hv=dict(dim=dim, fp32_us=hv32 * 1e3, fp64_us=hv64 * 1e3,
                 fp32_gbs=hv_bytes32 / (hv32 * 1e-3) / 1e9,
                 fp64_gbs=2 * dim * 8 / (hv64 * 1e-3) / 1e9,
@@ -520,14 +624,15 @@ def main():
         chi2_host = extra["differentiation"].pop("chi2_host")
         line.update(extra)
     if not args.no_cpu_baseline and world == 1:
-        hv_per_step = 2 * 170 + 2 * NGF
+        hv_per_step, nl = reference_hv_per_step()
         t_map, t_hv = cpu_sample(nthreads, 2)
         sec = cpu_step_seconds(t_map, t_hv, hv_per_step)
         line["cpu_baseline"] = dict(
-            value=1.0 / sec, unit=UNIT, cores=nthreads, kind="port",
+            value=1.0 / sec, unit=UNIT, cores=nthreads, kind="port-extrapolated",
             sample=f"2 oracle directMatVec_cc products (complex128, binary-search map, "
                    f"{nthreads} threads) on the 7/7 sector + the map build, scaled to "
-                   f"{hv_per_step} H*v per DMFT step; {t_hv:.2f} s per H*v")
+                   f"{hv_per_step} H*v per DMFT step ({nl} plain-Lanczos steps, the second "
+                   f"pass, 2 x {NGF} chain steps); {t_hv:.2f} s per H*v")
         if chi2_host is not None:
             line["differentiation"]["chi2"]["cpu_baseline"] = chi2_cpu(chi2_host)
     print(json.dumps(line))

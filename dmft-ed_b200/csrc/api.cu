@@ -764,6 +764,24 @@ int dmfted_gs_lanczos(dmfted_ctx *c, int32_t isector, int32_t neigen, int32_t ni
     API_END
 }
 
+int dmfted_add_to_lanczos_gf(dmfted_ctx *c, double vnorm2, double ei, double egs, double zeta,
+                             int32_t nlanc, const double *alanc, const double *blanc,
+                             int32_t isign, double *gmats, double *greal) {
+    API_BEGIN
+    DM_REQUIRE(c && alanc && blanc && gmats, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(zeta > 0.0, DMFTED_ERR_ARG, "add_to_lanczos_gf: zeta <= 0");
+    DM_REQUIRE(isign == 1 || isign == -1, DMFTED_ERR_ARG, "add_to_lanczos_gf: isign not +-1");
+    DM_CUDA(cudaSetDevice(c->device));
+    // pesoBZ of build_gf_normal.f90:457-464
+    const bool finite_t = c->p.lanc_nstates_total != 1;
+    double weight;
+    if (finite_t && c->p.beta * (ei - egs) < 200.0) weight = std::exp(-c->p.beta * (ei - egs)) / zeta;
+    else if (!finite_t) weight = 1.0 / zeta;
+    else weight = 0.0;
+    gf_add_chain(c, nlanc, alanc, blanc, weight, vnorm2, ei, isign, gmats, greal);
+    API_END
+}
+
 int dmfted_lanc_tridiag(dmfted_ctx *c, int32_t isector, const double *vvinit, int32_t nlanc,
                         double *alanc, double *blanc, int32_t *nused) {
     API_BEGIN

@@ -810,6 +810,50 @@ __global__ void k_cf_sum(const ChainCF *cfs, int ncf, int nso, const int *nsteps
 // ------------------------------------------------------------------ host --
 static size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// One chain's continued fraction on the context's grids, added to host arrays
+// gm[lmats], gr[lreal] (complex, gr may be null): the device evaluation every
+// solve uses, for a chain given by its coefficients.
+void gf_add_chain(dmfted_ctx *c, int nlanc, const double *alanc, const double *blanc,
+                  double weight, double norm2, double ei, int isign, double *gm, double *gr) {
+    DM_REQUIRE(nlanc >= 1 && nlanc <= kChainStride - 1, DMFTED_ERR_ARG,
+               "add_to_lanczos_gf: nlanc out of range");
+    const dmfted_params &p = c->p;
+    const int L = p.lmats + p.lreal;
+    std::vector<double> buf(2 * (size_t)kChainStride + 2, 0.0);
+    std::copy(alanc, alanc + nlanc, buf.begin());
+    for (int k = 1; k < nlanc; k++) buf[kChainStride + k] = blanc[k];
+    buf[2 * kChainStride] = norm2;
+    ChainCF cf{0, 0, isign > 0 ? 1 : -1, weight, ei};
+    c->eig_aux.alloc(buf.size() + 2 * (size_t)L + 8);
+    double *d = c->eig_aux.p, *d_terms = d + buf.size() + 4;
+    c->bjobs.alloc(sizeof(ChainCF) + 16);
+    c->bint.alloc(4);
+    const int n = nlanc;
+    DM_CUDA(cudaMemcpyAsync(d, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+    DM_CUDA(cudaMemcpyAsync(c->bjobs.p, &cf, sizeof(cf), cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(c->bint.p, &n, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    k_cf_terms<<<div_up(L, 128), 128, 0, c->stream>>>(
+        reinterpret_cast<const ChainCF *>(c->bjobs.p), 1, d, d + kChainStride, c->bint.p,
+        d + 2 * kChainStride, c->d_wm.p, p.lmats, c->d_wr.p, p.lreal, p.eps,
+        reinterpret_cast<double2 *>(d_terms));
+    DM_CHECK_LAUNCH();
+    c->launches++;
+    std::vector<double> t(2 * (size_t)L);
+    DM_CUDA(cudaMemcpyAsync(t.data(), d_terms, t.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    for (int f = 0; f < p.lmats; f++) {
+        gm[2 * f] += t[2 * f];
+        gm[2 * f + 1] += t[2 * f + 1];
+    }
+    if (gr)
+        for (int f = 0; f < p.lreal; f++) {
+            gr[2 * f] += t[2 * (p.lmats + f)];
+            gr[2 * f + 1] += t[2 * (p.lmats + f) + 1];
+        }
+}
+
 // Persistent launch: as many CTAs (CL == 1) or clusters as can be resident,
 // at most one per job.
 template <typename... KArgs, typename... Args>

@@ -75,10 +75,11 @@ void chi2_batch_device(dmfted_ctx *c, int nbatch, int nbath, int L, const double
     auto bytes = [&](int t) { return (size_t)(2 * nbath + (1 + 2 * nbath) * t + 2 * nbath * t) * 8; };
     while (nt > 32 && bytes(nt) > 160 * 1024) nt /= 2;
     DM_REQUIRE(bytes(nt) <= 200 * 1024, DMFTED_ERR_UNSUPPORTED, "chi2: too many bath levels");
-    static bool attr = false;
-    if (!attr) {
+    // the attribute belongs to the device current when it is set: once per device
+    static bool attr[64] = {false};
+    if (!attr[c->device & 63]) {
         DM_CUDA(cudaFuncSetAttribute(k_chi2, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr = true;
+        attr[c->device & 63] = true;
     }
     k_chi2<<<nbatch, nt, bytes(nt), c->stream>>>(nbath, L, a, x, (const double2 *)g, w, chi2, grad);
     DM_CHECK_LAUNCH();

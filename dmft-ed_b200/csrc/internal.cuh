@@ -358,6 +358,10 @@ struct ChainRec {
 // path above it) and adds all of them to the Matsubara / real-axis G.
 void batch_chains_gf(dmfted_ctx *c, const std::vector<ChainRec> &recs, int precision);
 void fock_build_map(dmfted_ctx *c, int isector, int32_t *d_map);  // combined map
+// One chain's continued fraction (coefficients on the host) added to host
+// arrays gm[lmats], gr[lreal] (complex; gr may be null).
+void gf_add_chain(dmfted_ctx *c, int nlanc, const double *alanc, const double *blanc,
+                  double weight, double norm2, double ei, int isign, double *gm, double *gr);
 
 // ---- dense.cu ------------------------------------------------------------
 // Dense eigensolve (Householder + tridiagonal, one CTA per sector) of the sectors ed_diag_c

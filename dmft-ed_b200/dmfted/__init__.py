@@ -22,7 +22,7 @@ _LIB = os.environ.get("DMFTED_LIB") or os.path.join(os.path.dirname(_HERE), "lib
 _lib = None
 
 OK = 0
-ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_STATE, ERR_NOTCONV, ERR_NORM, ERR_TIMEOUT = range(1, 9)
+ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_STATE, ERR_NOTCONV, ERR_NORM = range(1, 8)
 FP64 = 0
 MIXED = 1
 
@@ -82,6 +82,8 @@ EXPORTS = {
                                     _ip]),
     "dmfted_lanc_tridiag": (C.c_int, [_vp, C.c_int32, _dp, C.c_int32, _dp, _dp, _ip]),
     "dmfted_lanc_tridiag_noalloc": (C.c_int, [_vp, C.c_int32, _vp, C.c_int32, _vp, _vp, _vp, _vp]),
+    "dmfted_add_to_lanczos_gf": (C.c_int, [_vp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                           C.c_int32, _dp, _dp, C.c_int32, _dp, _dp]),
     "dmfted_ed_solve": (C.c_int, [_vp, _dp, C.c_int32, _ip, C.c_int32]),
     "dmfted_get_gimp_matsubara": (C.c_int, [_vp, _dp]),
     "dmfted_get_gimp_real": (C.c_int, [_vp, _dp]),
@@ -295,6 +297,17 @@ class EDSolver:
         _ck(lib().dmfted_lanc_tridiag(self.ctx, isector, _p(v.view(np.float64)), nlanc, _p(a),
                                       _p(b), C.byref(used)))
         return a, b, used.value
+
+    def add_to_lanczos_gf(self, vnorm2, ei, egs, zeta, alanc, blanc, isign, lmats, lreal):
+        """add_to_lanczos_gf_normal (build_gf_normal.f90:442-488) for one chain on
+        the context's frequency grids; returns (gmats[lmats], greal[lreal])."""
+        a = np.ascontiguousarray(alanc, np.float64)
+        b = np.ascontiguousarray(blanc, np.float64)
+        gm = np.zeros(2 * max(lmats, 1))
+        gr = np.zeros(2 * max(lreal, 1))
+        _ck(lib().dmfted_add_to_lanczos_gf(self.ctx, vnorm2, ei, egs, zeta, a.size, _p(a), _p(b),
+                                           isign, _p(gm), _p(gr) if lreal > 0 else None))
+        return gm.view(np.complex128)[:lmats], gr.view(np.complex128)[:lreal]
 
     def ed_solve(self, bath, sectors=None):
         """ed_solve_single (ED_MAIN.f90:251-289); sectors restricts the scan."""

@@ -43,7 +43,6 @@ extern "C" {
 #define DMFTED_ERR_STATE 5       /* call out of order (no sector / no bath)  */
 #define DMFTED_ERR_NOTCONV 6     /* iteration limit hit before convergence   */
 #define DMFTED_ERR_NORM 7        /* state not normalised                     */
-#define DMFTED_ERR_TIMEOUT 8     /* a bounded device wait gave up            */
 
 /* ---- precision of the Lanczos vectors ------------------------------- */
 #define DMFTED_FP64 0  /* plain FP64: the drop-in path                       */
@@ -197,6 +196,19 @@ int dmfted_lanc_tridiag(dmfted_ctx *ctx, int32_t isector, const double *vvinit, 
 int dmfted_lanc_tridiag_noalloc(dmfted_ctx *ctx, int32_t isector, const double *d_v0,
                                 int32_t nlanc, double *d_work, double *d_alanc, double *d_blanc,
                                 int32_t *d_nused);
+
+/* add_to_lanczos_gf_normal (build_gf_normal.f90:442-488) for one chain: adds
+ * pesoBZ * sum_j Z(1,j)^2 / (z - isign (E_j - Ei)) over the Matsubara grid
+ * (gmats, complex128[Lmats]) and the real axis z = w + i eps (greal,
+ * complex128[Lreal], may be NULL) of the context's parameters, with
+ * pesoBZ = vnorm2 exp(-beta (Ei - Egs)) / zeta at finite temperature (0 when
+ * beta (Ei - Egs) >= 200) and vnorm2 / zeta at T=0 (lanc_nstates_total == 1).
+ * alanc[nlanc], blanc[nlanc] in the dmfted_lanc_tridiag convention (blanc[0]
+ * unused).  The pole sum is the chain's continued fraction, evaluated on the
+ * device in FP64, as every solve does. */
+int dmfted_add_to_lanczos_gf(dmfted_ctx *ctx, double vnorm2, double ei, double egs, double zeta,
+                             int32_t nlanc, const double *alanc, const double *blanc,
+                             int32_t isign, double *gmats, double *greal);
 
 /* ---- the solve ------------------------------------------------------------
  * ed_solve_single (ED_MAIN.f90:251-289) for the normal mode:

@@ -4,13 +4,18 @@ owned by their own pool, or the call sits in a loop where cudaMalloc must not
 run).  The caller passes every vector as a device pointer; the library uses a
 fixed scratch array of its own.
 
-Checks, through the C-ABI: two calls in a row reproduce the allocating entry
-point dmfted_lanc_tridiag on the same start vector within the tolerances of
-tests/test_gpu_parity.py (first 20 alpha/beta to 1e-10, the continued fraction
-G(iwn) to 1e-8), the two calls agree with each other, and an nlanc beyond the
-fixed scratch is refused with DMFTED_ERR_ARG."""
-import ctypes as C
-
+Checks, through the C-ABI:
+  - the entry point is the first work on a fresh context (only the tables of
+    set_bath exist), so no buffer an earlier call allocated can hide an
+    allocation of its own;
+  - the device's free memory is the same before and after a call (the first
+    call may also load the library's kernel code under lazy module loading,
+    which is the driver's memory, so the check runs on the later calls);
+  - two calls in a row reproduce the allocating entry point dmfted_lanc_tridiag
+    on the same start vector within the tolerances of tests/test_gpu_parity.py
+    (first 20 alpha/beta to 1e-10, the continued fraction G(iwn) to 1e-8) and
+    agree with each other bit for bit;
+  - an nlanc beyond the fixed scratch is refused with DMFTED_ERR_ARG."""
 import numpy as np
 import pytest
 
@@ -23,18 +28,12 @@ pytestmark = pytest.mark.gpu
 def test_no_alloc_tridiag_matches_allocating_entry_point():
     import torch
     m = O.seeded_model(3, nbath=7, u=2.0, beta=100.0)
-    p = dmfted.default_params(nbath=7, uloc=[2.0], beta=100.0, lmats=16, lreal=0)
-    s = dmfted.EDSolver(p)
-    s.set_bath(m.bath_array())
     hi = O.build_sector(m.ns, 4, 4)
     hj = O.build_sector(m.ns, 5, 4)
     e0, psi, _ = O.lanczos_gs(m, hi)
     n2, vv = O.gf_vvinit(True, 1, hi, hj, psi)
     v = np.ascontiguousarray(vv.real)
     nlanc = 200
-    isec = s.sector_index(5, 4)
-    a_ref, b_ref, n_ref = s.lanc_tridiag(isec, v, nlanc)
-
     dim = v.size
     dev = torch.device("cuda", 0)
     d_v = torch.tensor(v, dtype=torch.float64, device=dev)
@@ -43,7 +42,28 @@ def test_no_alloc_tridiag_matches_allocating_entry_point():
     d_b = torch.zeros(nlanc, dtype=torch.float64, device=dev)
     d_n = torch.zeros(1, dtype=torch.int32, device=dev)
     torch.cuda.synchronize()
+
+    p = dmfted.default_params(nbath=7, uloc=[2.0], beta=100.0, lmats=16, lreal=0)
+    s = dmfted.EDSolver(p)
+    s.set_bath(m.bath_array())
+    isec = s.sector_index(5, 4)
     L = dmfted.lib()
+
+    def call():
+        dmfted._ck(L.dmfted_lanc_tridiag_noalloc(s.ctx, isec, d_v.data_ptr(), nlanc,
+                                                 d_work.data_ptr(), d_a.data_ptr(),
+                                                 d_b.data_ptr(), d_n.data_ptr()))
+        torch.cuda.synchronize()
+        return d_a.cpu().numpy().copy(), d_b.cpu().numpy().copy(), int(d_n.item())
+
+    outs = [call()]
+    for _ in range(2):
+        free0 = torch.cuda.mem_get_info(dev)[0]
+        outs.append(call())
+        assert torch.cuda.mem_get_info(dev)[0] == free0
+
+    # the allocating entry point on the same start vector
+    a_ref, b_ref, n_ref = s.lanc_tridiag(isec, v, nlanc)
     wm = O.matsubara(100.0, 1024)
 
     def cf(a, b):
@@ -53,22 +73,15 @@ def test_no_alloc_tridiag_matches_allocating_entry_point():
         return g
 
     g_ref = cf(a_ref, b_ref)
-    outs = []
-    for call in range(2):
-        dmfted._ck(L.dmfted_lanc_tridiag_noalloc(s.ctx, isec, d_v.data_ptr(), nlanc,
-                                                 d_work.data_ptr(), d_a.data_ptr(),
-                                                 d_b.data_ptr(), d_n.data_ptr()))
-        torch.cuda.synchronize()
-        a = d_a.cpu().numpy()
-        b = d_b.cpu().numpy()
-        assert int(d_n.item()) == n_ref
+    for a, b, n in outs:
+        assert n == n_ref
         assert np.allclose(a[:20], a_ref[:20], rtol=0, atol=1e-10)
         assert np.allclose(b[:20], b_ref[:20], rtol=0, atol=1e-10)
         assert np.abs(cf(a, b) - g_ref).max() <= 1e-8
-        outs.append((a.copy(), b.copy()))
     # the fixed scratch keeps the previous call's contents; results do not
     # depend on them
-    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    for a, b, _ in outs[1:]:
+        assert np.array_equal(outs[0][0], a) and np.array_equal(outs[0][1], b)
 
     with pytest.raises(dmfted.DmftedError) as err:
         dmfted._ck(L.dmfted_lanc_tridiag_noalloc(s.ctx, isec, d_v.data_ptr(), 5000,
