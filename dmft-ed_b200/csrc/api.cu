@@ -252,17 +252,19 @@ static void ed_analysis_finite_t(dmfted_ctx *c) {
 // Thermal average of the raw accumulators over the kept states, with the
 // Boltzmann weights of ED_OBSERVABLES.f90:128-129 (T=0: 1/Z over the ground
 // states); hops: include the hop terms of the Hellmann-Feynman gradient.
+// The pair terms (obs_pair_count entries after the weighted ones) are summed
+// over the states without weights, as local_energy_impurity sums them.
 static std::vector<double> thermal_observables(dmfted_ctx *c, bool hops) {
     // every state's accumulators into its own slot, then one copy and one wait
-    const int na = obs_count(c);
+    const int na = obs_count(c), np = obs_pair_count(c), nt = na + np;
     const size_t ns = c->states.size();
-    c->obs_d.alloc(std::max<size_t>(ns, 1) * na);
+    c->obs_d.alloc(std::max<size_t>(ns, 1) * nt);
     for (size_t i = 0; i < ns; i++) {
         const auto &st = c->states[i];
         observables_raw(c, sector_view(c, st.isector), c->states64.p + st.off,
-                        c->obs_d.p + i * na, hops);
+                        c->obs_d.p + i * nt, hops);
     }
-    std::vector<double> all(ns * na), acc(na, 0.0);
+    std::vector<double> all(ns * nt), acc(nt, 0.0);
     DM_CUDA(cudaMemcpyAsync(all.data(), c->obs_d.p, all.size() * sizeof(double),
                             cudaMemcpyDeviceToHost, c->stream));
     DM_CUDA(cudaStreamSynchronize(c->stream));
@@ -270,9 +272,73 @@ static std::vector<double> thermal_observables(dmfted_ctx *c, bool hops) {
         const auto &st = c->states[i];
         const double peso =
             (c->finite_t ? std::exp(-c->p.beta * (st.e - c->egs)) : 1.0) / c->zeta;
-        for (int q = 0; q < na; q++) acc[q] += peso * all[i * na + q];
+        for (int q = 0; q < na; q++) acc[q] += peso * all[i * nt + q];
+        for (int q = na; q < nt; q++) acc[q] += all[i * nt + q];
     }
     return acc;
+}
+
+// local_energy_impurity (ED_OBSERVABLES.f90:454-635) from the thermal
+// accumulators: the diagonal terms from the weighted impurity-configuration
+// histogram, the inter-orbital Hloc hopping of Eknot and the spin-exchange /
+// pair-hopping terms from the unweighted pair sums (the reference adds those
+// three without the state weight).  c->eloc = {Epot, Eint, Ehartree, Eknot,
+// Dust, Dund, Dse, Dph}; Epot includes Ehartree, and Eint, which the
+// reference declares but never assigns, is 0.
+static void local_energies(dmfted_ctx *c, const std::vector<double> &acc) {
+    const dmfted_params &p = c->p;
+    const int no = c->norb, ni = 1 << no, ns = c->nspin;
+    const int na = obs_count(c);
+    const double *P = acc.data() + na - ni * ni;
+    auto hl = [&](int is, int a, int b) {
+        const int64_t idx = is + ns * (is + ns * (a + (int64_t)no * b));
+        return c->hloc[2 * idx];
+    };
+    double eknot = 0.0, epot = 0.0, ehart = 0.0, dust = 0.0, dund = 0.0, dse = 0.0, dph = 0.0;
+    for (int iu = 0; iu < ni; iu++)
+        for (int id = 0; id < ni; id++) {
+            const double w = P[iu * ni + id];
+            double nu[kMaxNorb], nd[kMaxNorb];
+            for (int a = 0; a < no; a++) {
+                nu[a] = (iu >> a) & 1;
+                nd[a] = (id >> a) & 1;
+            }
+            for (int a = 0; a < no; a++) eknot += (hl(0, a, a) * nu[a] + hl(ns - 1, a, a) * nd[a]) * w;
+            for (int a = 0; a < no; a++) epot += p.uloc[a] * nu[a] * nd[a] * w;
+            for (int a = 0; a < no; a++)
+                for (int b = a + 1; b < no; b++) {
+                    const double ud = nu[a] * nd[b] + nu[b] * nd[a];
+                    const double uu = nu[a] * nu[b] + nd[a] * nd[b];
+                    epot += p.ust * ud * w + (p.ust - p.jh) * uu * w;
+                    dust += ud * w;
+                    dund += uu * w;
+                }
+            if (p.hfmode) {
+                for (int a = 0; a < no; a++)
+                    ehart += -0.5 * p.uloc[a] * (nu[a] + nd[a]) * w + 0.25 * p.uloc[a] * w;
+                for (int a = 0; a < no; a++)
+                    for (int b = a + 1; b < no; b++) {
+                        const double nn = nu[a] + nd[a] + nu[b] + nd[b];
+                        ehart += -0.5 * p.ust * nn * w + 0.25 * p.ust * w;
+                        ehart += -0.5 * (p.ust - p.jh) * nn * w + 0.25 * (p.ust - p.jh) * w;
+                    }
+            }
+        }
+    if (no > 1) {
+        const double *pr = acc.data() + na;
+        for (int a = 0; a < no; a++)
+            for (int b = 0; b < no; b++) {
+                if (a == b) continue;
+                eknot += hl(0, a, b) * pr[a * no + b] + hl(ns - 1, a, b) * pr[no * no + a * no + b];
+            }
+        if (p.jhflag) {
+            dse = pr[2 * no * no];
+            dph = pr[2 * no * no + 1];
+            epot += p.jx * dse + p.jp * dph;
+        }
+    }
+    epot += ehart;
+    c->eloc = {epot, 0.0, ehart, eknot, dust, dund, dse, dph};
 }
 
 static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list) {
@@ -317,8 +383,9 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
         c->obs[3 * no + a] = acc[2 * no + a];  // docc
         c->obs[4 * no + a] = nu - nd;  // magz
     }
-    c->hf_terms.assign(acc.begin() + 3 * no, acc.end());
+    c->hf_terms.assign(acc.begin() + 3 * no, acc.begin() + 3 * no + 4 * no * c->nbath);
     c->hf_hops = false;  // the hop terms are computed when the gradient is asked for
+    local_energies(c, acc);
     DM_CUDA(cudaEventRecord(ev[2], c->stream));
     // ---- Green's functions ---------------------------------------------------
     const size_t gsz = (size_t)c->nspin * no;
@@ -913,6 +980,22 @@ int dmfted_get_eigenspace(dmfted_ctx *c, int32_t cap, double *energies, int32_t 
     API_END
 }
 
+int dmfted_get_eimp(dmfted_ctx *c, double *eimp) {
+    API_BEGIN
+    DM_REQUIRE(c && eimp, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(c->solved, DMFTED_ERR_STATE, "no solve has run on this context");
+    for (int k = 0; k < 4; k++) eimp[k] = c->eloc[k];
+    API_END
+}
+
+int dmfted_get_doubles(dmfted_ctx *c, double *doubles) {
+    API_BEGIN
+    DM_REQUIRE(c && doubles, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(c->solved, DMFTED_ERR_STATE, "no solve has run on this context");
+    for (int k = 0; k < 4; k++) doubles[k] = c->eloc[4 + k];
+    API_END
+}
+
 int dmfted_get_egs(dmfted_ctx *c, double *egs) {
     API_BEGIN
     DM_REQUIRE(c && egs, DMFTED_ERR_ARG, "null argument");
@@ -931,7 +1014,7 @@ int dmfted_hf_gradient(dmfted_ctx *c, double *grad, int32_t nb) {
     if (!c->hf_hops) {
         DM_CUDA(cudaSetDevice(c->device));
         const std::vector<double> acc = thermal_observables(c, true);
-        c->hf_terms.assign(acc.begin() + 3 * no, acc.end());
+        c->hf_terms.assign(acc.begin() + 3 * no, acc.begin() + 3 * no + 4 * no * c->nbath);
         c->hf_hops = true;
     }
     const double *nk = c->hf_terms.data();           // [2][norb][nbath]

@@ -296,6 +296,7 @@ struct dmfted_ctx {
     dmfted::DBuf<double> gm, gr, g0m, sm, sr;  // complex (nspin,norb,L) blocks
     std::vector<double> obs;                   // dens, up, dw, docc, magz (norb each)
     std::vector<double> hf_terms;              // nk[2][norb][nbath], hop[2][norb][nbath]
+    std::vector<double> eloc = std::vector<double>(8, 0.0);  // Epot Eint Ehartree Eknot Dust Dund Dse Dph
     dmfted::SolveStats stats;
     bool solved = false;
 };
@@ -452,6 +453,7 @@ void gf_sigma(dmfted_ctx *c);  // impSmats/impSreal/impG0mats from impG*
 
 // ---- observables.cu --------------------------------------------------------
 int obs_count(const dmfted_ctx *c);
+int obs_pair_count(const dmfted_ctx *c);
 void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, double *d_out,
                      bool hops);
 

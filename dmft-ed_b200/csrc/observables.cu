@@ -7,7 +7,15 @@
 // with the normal bath stride Norb+(iorb-1)*Nbath+k (ED_SETUP.f90:445-462).
 //
 // Accumulator layout: [0,norb) n_up, [norb,2norb) n_dw, [2norb,3norb) docc,
-// then nk[s][a][k] (2*norb*nbath), then hop[s][a][k] (2*norb*nbath).
+// then nk[s][a][k] (2*norb*nbath), then hop[s][a][k] (2*norb*nbath), then the
+// impurity-configuration histogram P[iu][id] (2^norb x 2^norb: the weight of
+// the states whose impurity orbitals hold the up bits iu and down bits id),
+// from which local_energy_impurity's diagonal terms follow.
+//
+// Pair terms (k_obs_pairs, Norb > 1 only): <psi|c^+_{a s} c_{b s}|psi> for
+// a != b (the inter-orbital Hloc hopping of Eknot) and the spin-exchange and
+// pair-hopping expectations (Dse, Dph) of ED_OBSERVABLES.f90:504-538,585-621,
+// layout hl[s][a][b] (2*norb*norb), then se, ph.
 //
 // Occupations (k_obs_occ, every solve): the state is the DimUp x DimDw matrix
 // psi[r, c], and every occupation is diagonal in one spin, so with
@@ -50,14 +58,16 @@ __global__ void __launch_bounds__(kOccThreads) k_obs_occ(HxvArgs<double> a, int 
     extern __shared__ double occ_sm[];
     __shared__ double red[kOccThreads / 32];
     const int tid = threadIdx.x, bd = blockDim.x;
-    const int norb = a.norb, pv = norb * nbath;
+    const int norb = a.norb, pv = norb * nbath, ni = 1 << norb;
+    const int nacc = nocc + ni * ni;  // occupations, then the histogram
     const int64_t dimup = a.dimup;
     double *R = occ_sm, *ca = occ_sm + dimup;
     for (int64_t r = tid; r < dimup; r += bd) R[r] = 0.0;
-    for (int q = tid; q < nocc; q += bd) ca[q] = 0.0;
+    for (int q = tid; q < nacc; q += bd) ca[q] = 0.0;
     __syncthreads();
     for (int64_t c = blockIdx.x; c < a.dimdw; c += gridDim.x) {
         double sw = 0.0, sd[kMaxNorb] = {0.0, 0.0, 0.0};
+        double sh[1 << kMaxNorb] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (int64_t r = tid; r < dimup; r += bd) {
             const double x = psi[r + dimup * c];
             const double w = x * x;
@@ -67,13 +77,22 @@ __global__ void __launch_bounds__(kOccThreads) k_obs_occ(HxvArgs<double> a, int 
 #pragma unroll
             for (int o = 0; o < kMaxNorb; o++)
                 if (o < norb) sd[o] += (wu >> o) & 1u ? w : 0.0;
+            const uint32_t iu = wu & (uint32_t)(ni - 1);
+#pragma unroll
+            for (int h = 0; h < (1 << kMaxNorb); h++)
+                if (h < ni) sh[h] += iu == (uint32_t)h ? w : 0.0;
         }
         const double csum = block_sum_occ(sw, red);
         double dsum[kMaxNorb];
 #pragma unroll
         for (int o = 0; o < kMaxNorb; o++) dsum[o] = o < norb ? block_sum_occ(sd[o], red) : 0.0;
+        double hsum[1 << kMaxNorb];
+#pragma unroll
+        for (int h = 0; h < (1 << kMaxNorb); h++) hsum[h] = h < ni ? block_sum_occ(sh[h], red) : 0.0;
         if (tid == 0) {
             const uint32_t wd = a.wd[c];
+            const uint32_t id = wd & (uint32_t)(ni - 1);
+            for (int h = 0; h < ni; h++) ca[nocc + h * ni + (int)id] += hsum[h];
             for (int o = 0; o < norb; o++) {
                 const bool nd = (wd >> o) & 1u;
                 if (nd) {
@@ -96,9 +115,75 @@ __global__ void __launch_bounds__(kOccThreads) k_obs_occ(HxvArgs<double> a, int 
         if (tid == 0) ca[q < norb ? q : 3 * norb + (q - norb)] += v;
     }
     __syncthreads();
-    for (int q = tid; q < nocc; q += bd) {
+    for (int q = tid; q < nacc; q += bd) {
         partials[((int64_t)q * gridDim.x + blockIdx.x) * 2 + 0] = ca[q];
         partials[((int64_t)q * gridDim.x + blockIdx.x) * 2 + 1] = 0.0;
+    }
+}
+
+// Pair terms of one state (Norb > 1): per-thread slots in shared memory,
+// targets through the rank table.  Signs: a hop b -> a of one spin is
+// (-1)^(occupied levels of that spin's word between a and b), the other
+// spin's word contributing pairs that cancel; the spin-exchange term moves
+// up b -> a and down a -> b, the pair hopping both spins b -> a, and their
+// signs are the products of the two one-spin signs (ED_OBSERVABLES.f90:
+// 585-621 with c/cdg of ED_SETUP.f90:1055-1081).
+__device__ __forceinline__ double hop_sign(uint32_t w, int b, int a) {
+    // c_b then c^+_a on word w (bit b set, bit a clear)
+    const uint32_t w1 = w & ~(1u << b);
+    const int p = __popc(w & ((1u << b) - 1u)) + __popc(w1 & ((1u << a) - 1u));
+    return (p & 1) ? -1.0 : 1.0;
+}
+
+__global__ void __launch_bounds__(kObsThreads) k_obs_pairs(HxvArgs<double> a, const int32_t *rank,
+                                                           const double *psi, int npair,
+                                                           int jhflag, double *partials) {
+    extern __shared__ double pslot[];  // [npair][kObsThreads]
+    const int tid = threadIdx.x;
+    const int norb = a.norb;
+    for (int q = 0; q < npair; q++) pslot[q * kObsThreads + tid] = 0.0;
+    const int64_t dimup = a.dimup;
+    for (int64_t cidx = blockIdx.x; cidx < a.dimdw; cidx += gridDim.x) {
+        const uint32_t wd = a.wd[cidx];
+        for (int64_t r = tid; r < dimup; r += kObsThreads) {
+            const double x = psi[r + dimup * cidx];
+            const uint32_t wu = a.wu[r];
+            for (int ai = 0; ai < norb; ai++)
+                for (int bi = 0; bi < norb; bi++) {
+                    if (ai == bi) continue;
+                    const uint32_t ma = 1u << ai, mb = 1u << bi;
+                    const bool ua = wu & ma, ub = wu & mb, da = wd & ma, db = wd & mb;
+                    if (!ua && ub) {  // up hop b -> a, same column
+                        const int64_t rt = rank[(wu ^ mb) | ma];
+                        pslot[(ai * norb + bi) * kObsThreads + tid] +=
+                            hop_sign(wu, bi, ai) * x * psi[rt + dimup * cidx];
+                    }
+                    if (!da && db) {  // down hop b -> a, same row
+                        const int64_t qt = rank[(wd ^ mb) | ma];
+                        pslot[(norb * norb + ai * norb + bi) * kObsThreads + tid] +=
+                            hop_sign(wd, bi, ai) * x * psi[r + dimup * qt];
+                    }
+                    if (!jhflag) continue;
+                    if (ub && da && !db && !ua) {  // spin exchange
+                        const int64_t rt = rank[(wu ^ mb) | ma], qt = rank[(wd ^ ma) | mb];
+                        pslot[(2 * norb * norb) * kObsThreads + tid] +=
+                            hop_sign(wu, bi, ai) * hop_sign(wd, ai, bi) * x * psi[rt + dimup * qt];
+                    }
+                    if (ub && db && !da && !ua) {  // pair hopping
+                        const int64_t rt = rank[(wu ^ mb) | ma], qt = rank[(wd ^ mb) | ma];
+                        pslot[(2 * norb * norb + 1) * kObsThreads + tid] +=
+                            hop_sign(wu, bi, ai) * hop_sign(wd, bi, ai) * x * psi[rt + dimup * qt];
+                    }
+                }
+        }
+    }
+    __syncthreads();
+    for (int q = tid; q < npair; q += kObsThreads) {
+        CSum s;
+        s.zero();
+        for (int t = 0; t < kObsThreads; t++) s.add(pslot[q * kObsThreads + t]);
+        partials[((int64_t)q * gridDim.x + blockIdx.x) * 2 + 0] = s.hi;
+        partials[((int64_t)q * gridDim.x + blockIdx.x) * 2 + 1] = s.lo;
     }
 }
 
@@ -160,16 +245,23 @@ __global__ void __launch_bounds__(32 * kFoldWarps) k_obs_fold(const double *part
     if (lane == 0) out[q] = s.value();
 }
 
-int obs_count(const dmfted_ctx *c) { return 3 * c->norb + 4 * c->norb * c->nbath; }
+int obs_count(const dmfted_ctx *c) {
+    return 3 * c->norb + 4 * c->norb * c->nbath + (1 << c->norb) * (1 << c->norb);
+}
+
+int obs_pair_count(const dmfted_ctx *c) { return c->norb > 1 ? 2 * c->norb * c->norb + 2 : 0; }
 
 // Raw accumulators of one state (weight 1) into d_out[obs_count] (device):
-// the occupations, and the hop terms when hops is set (else zero).
+// the occupations and the impurity histogram, and the hop terms when hops is
+// set (else zero); then the pair terms into d_out[obs_count ...
+// + obs_pair_count] when Norb > 1.
 void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, double *d_out,
                      bool hops) {
     HxvArgs<double> a = make_hxv_args<double>(c, s);
     const int na = obs_count(c);
     const int pv = c->norb * c->nbath, nocc = 3 * c->norb + 2 * pv;
-    const size_t smem = ((size_t)a.dimup + nocc) * sizeof(double);
+    const int nh = (1 << c->norb) * (1 << c->norb);
+    const size_t smem = ((size_t)a.dimup + nocc + nh) * sizeof(double);
     DM_REQUIRE(smem <= 200 * 1024, DMFTED_ERR_UNSUPPORTED, "sector rows too long for k_obs_occ");
     static bool attr[64] = {false};
     if (!attr[c->device & 63]) {
@@ -186,10 +278,27 @@ void observables_raw(dmfted_ctx *c, const SectorView &s, const double *psi, doub
     DM_CHECK_LAUNCH();
     k_obs_fold<<<div_up(nocc, kFoldWarps), 32 * kFoldWarps, 0, c->stream>>>(c->red_partials.p,
                                                                            grid, nocc, d_out);
+    // the histogram's partials follow the occupations' (rows nocc .. nocc+nh)
+    k_obs_fold<<<div_up(nh, kFoldWarps), 32 * kFoldWarps, 0, c->stream>>>(
+        c->red_partials.p + (size_t)nocc * grid * 2, grid, nh, d_out + na - nh);
     DM_CHECK_LAUNCH();
-    c->launches += 2;
+    c->launches += 3;
+    const int npair = obs_pair_count(c);
+    if (npair > 0) {
+        const size_t psmem = (size_t)npair * kObsThreads * sizeof(double);
+        const int pgrid = (int)std::min<int64_t>(s.dimdw, (int64_t)num_sms(c) * 4);
+        DM_REQUIRE((int64_t)npair * pgrid * 2 <= (int64_t)c->red_partials.n,
+                   DMFTED_ERR_UNSUPPORTED, "reduction scratch too small for the pair terms");
+        k_obs_pairs<<<pgrid, kObsThreads, psmem, c->stream>>>(a, c->rank.p + 0, psi, npair,
+                                                              c->p.jhflag, c->red_partials.p);
+        DM_CHECK_LAUNCH();
+        k_obs_fold<<<div_up(npair, kFoldWarps), 32 * kFoldWarps, 0, c->stream>>>(
+            c->red_partials.p, pgrid, npair, d_out + na);
+        DM_CHECK_LAUNCH();
+        c->launches += 2;
+    }
     if (!hops) {
-        DM_CUDA(cudaMemsetAsync(d_out + nocc, 0, (size_t)(na - nocc) * sizeof(double), c->stream));
+        DM_CUDA(cudaMemsetAsync(d_out + nocc, 0, (size_t)(2 * pv) * sizeof(double), c->stream));
         return;
     }
     const size_t hsmem = (size_t)2 * pv * kObsThreads * sizeof(double);

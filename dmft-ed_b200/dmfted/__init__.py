@@ -93,6 +93,8 @@ EXPORTS = {
     "dmfted_get_observables": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "dmfted_get_eigenspace": (C.c_int, [_vp, C.c_int32, _dp, _ip, _ip, _dp]),
     "dmfted_get_egs": (C.c_int, [_vp, _dp]),
+    "dmfted_get_eimp": (C.c_int, [_vp, _dp]),
+    "dmfted_get_doubles": (C.c_int, [_vp, _dp]),
     "dmfted_hf_gradient": (C.c_int, [_vp, _dp, C.c_int32]),
     "dmfted_chi2_delta_batch": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _dp,
                                           _dp, _dp, _dp]),
@@ -373,6 +375,18 @@ class EDSolver:
         _ck(lib().dmfted_get_eigenspace(self.ctx, cap, _p(e), _p(s, C.c_int32), C.byref(n),
                                         C.byref(z)))
         return e[:n.value], s[:n.value], z.value
+
+    def ed_get_eimp(self):
+        """[Epot, Eint, Ehartree, Eknot] (ed_get_eimp, ED_IO/get_eimp.f90:1-4)."""
+        out = np.zeros(4)
+        _ck(lib().dmfted_get_eimp(self.ctx, _p(out)))
+        return out
+
+    def ed_get_doubles(self):
+        """[Dust, Dund, Dse, Dph] (ed_get_doubles, ED_IO/get_doubles.f90:1-4)."""
+        out = np.zeros(4)
+        _ck(lib().dmfted_get_doubles(self.ctx, _p(out)))
+        return out
 
     def egs(self):
         e = C.c_double()

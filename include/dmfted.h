@@ -236,6 +236,17 @@ int dmfted_get_observables(dmfted_ctx *ctx, double *dens, double *dens_up, doubl
  * ED_EIGENSPACE.f90:157-213), count, partition function Z. */
 int dmfted_get_eigenspace(dmfted_ctx *ctx, int32_t cap, double *energies, int32_t *sectors,
                           int32_t *nstates, double *zeta);
+/* Local energies of the last solve (local_energy_impurity,
+ * ED_OBSERVABLES.f90:454-635): ed_get_eimp (ED_IO/get_eimp.f90:1-4),
+ * eimp[4] = {Epot, Eint, Ehartree, Eknot}, and ed_get_doubles
+ * (ED_IO/get_doubles.f90:1-4), doubles[4] = {Dust, Dund, Dse, Dph}.  As in the
+ * reference: Epot includes Ehartree; Eint is never assigned there and is 0;
+ * the inter-orbital Hloc hopping part of Eknot and the spin-exchange /
+ * pair-hopping parts (Dse, Dph and their Jx, Jp terms in Epot, with Jhflag)
+ * are summed over the kept states without the Boltzmann weight. */
+int dmfted_get_eimp(dmfted_ctx *ctx, double *eimp);
+int dmfted_get_doubles(dmfted_ctx *ctx, double *doubles);
+
 /* Ground-state energy of the last solve. */
 int dmfted_get_egs(dmfted_ctx *ctx, double *egs);
 

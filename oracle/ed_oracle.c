@@ -776,6 +776,118 @@ void or_observables_state(const or_model *M, const int32_t *map, int64_t dim, co
             }
 }
 
+/* local_energy_impurity, ED_OBSERVABLES.f90:454-633, the body for one kept
+ * state (weight peso = exp(-beta(Ei-Egs))/Z or 1/Z), accumulated into
+ * e[8] = {Eknot, Epot (without the Hartree part), Ehartree, Dust, Dund, Dse,
+ * Dph, unused}.  As in the reference, the inter-orbital Hloc hopping terms
+ * of Eknot and the spin-exchange / pair-hopping terms of Epot, Dse and Dph
+ * are summed without the state's weight (ED_OBSERVABLES.f90:531,538,594-595,
+ * 619-620), and only their real parts enter (the energies are real(8)). */
+void or_local_energy_state(const or_model *M, const int32_t *map, int64_t dim, const double *psi_,
+                           double peso, double *e) {
+    const zc *psi = (const zc *)psi_;
+    const int Ns = M->ns, Norb = M->norb, Nspin = M->nspin;
+    const double Ust = M->ust, Jh = M->jh;
+    double eloc[2][3];
+    for (int is = 0; is < Nspin; is++)
+        for (int a = 0; a < Norb; a++) eloc[is][a] = creal(hloc_at(M, is, is, a, a));
+    for (int64_t i = 0; i < dim; i++) {
+        const int32_t m = map[i];
+        const double gsw = peso * (creal(psi[i]) * creal(psi[i]) + cimag(psi[i]) * cimag(psi[i]));
+        double nup[3], ndw[3];
+        for (int a = 0; a < Norb; a++) {
+            nup[a] = IB(m, a + 1);
+            ndw[a] = IB(m, a + 1 + Ns);
+        }
+        /* LOCAL ENERGY */
+        for (int a = 0; a < Norb; a++) e[0] += eloc[0][a] * nup[a] * gsw + eloc[Nspin - 1][a] * ndw[a] * gsw;
+        /* HYBRIDIZATION TERMS I: same spin */
+        for (int a = 1; a <= Norb; a++)
+            for (int b = 1; b <= Norb; b++) {
+                if (IB(m, a) == 0 && IB(m, b) == 1) {
+                    int32_t k1 = 0, k2 = 0;
+                    double sg1 = 1.0, sg2 = 1.0;
+                    op_c(b, m, &k1, &sg1);
+                    op_cdg(a, k1, &k2, &sg2);
+                    const int64_t j = or_binary_search(map, dim, k2);
+                    if (j > 0) e[0] += creal(hloc_at(M, 0, 0, a - 1, b - 1) * sg1 * sg2 * psi[i] * conj(psi[j - 1]));
+                }
+                if (IB(m, a + Ns) == 0 && IB(m, b + Ns) == 1) {
+                    int32_t k1 = 0, k2 = 0;
+                    double sg1 = 1.0, sg2 = 1.0;
+                    op_c(b + Ns, m, &k1, &sg1);
+                    op_cdg(a + Ns, k1, &k2, &sg2);
+                    const int64_t j = or_binary_search(map, dim, k2);
+                    if (j > 0)
+                        e[0] += creal(hloc_at(M, Nspin - 1, Nspin - 1, a - 1, b - 1) * sg1 * sg2 * psi[i] *
+                                      conj(psi[j - 1]));
+                }
+            }
+        /* DENSITY-DENSITY */
+        for (int a = 0; a < Norb; a++) e[1] += M->uloc[a] * nup[a] * ndw[a] * gsw;
+        if (Norb > 1) {
+            for (int a = 0; a < Norb; a++)
+                for (int b = a + 1; b < Norb; b++) {
+                    e[1] += Ust * (nup[a] * ndw[b] + nup[b] * ndw[a]) * gsw;
+                    e[3] += (nup[a] * ndw[b] + nup[b] * ndw[a]) * gsw;
+                }
+            for (int a = 0; a < Norb; a++)
+                for (int b = a + 1; b < Norb; b++) {
+                    e[1] += (Ust - Jh) * (nup[a] * nup[b] + ndw[a] * ndw[b]) * gsw;
+                    e[4] += (nup[a] * nup[b] + ndw[a] * ndw[b]) * gsw;
+                }
+        }
+        /* SPIN-EXCHANGE and PAIR-HOPPING */
+        if (Norb > 1 && M->jhflag) {
+            for (int a = 1; a <= Norb; a++)
+                for (int b = 1; b <= Norb; b++) {
+                    if (a != b && IB(m, b) == 1 && IB(m, a + Ns) == 1 && IB(m, b + Ns) == 0 &&
+                        IB(m, a) == 0) {
+                        int32_t k1 = 0, k2 = 0, k3 = 0, k4 = 0;
+                        double s1 = 1.0, s2 = 1.0, s3 = 1.0, s4 = 1.0;
+                        op_c(b, m, &k1, &s1);
+                        op_c(a + Ns, k1, &k2, &s2);
+                        op_cdg(b + Ns, k2, &k3, &s3);
+                        op_cdg(a, k3, &k4, &s4);
+                        const int64_t j = or_binary_search(map, dim, k4);
+                        if (j > 0) {
+                            const double t = creal(s1 * s2 * s3 * s4 * psi[i] * conj(psi[j - 1]));
+                            e[1] += M->jx * t;
+                            e[5] += t;
+                        }
+                    }
+                    if (a != b && IB(m, b) == 1 && IB(m, b + Ns) == 1 && IB(m, a + Ns) == 0 &&
+                        IB(m, a) == 0) {
+                        int32_t k1 = 0, k2 = 0, k3 = 0, k4 = 0;
+                        double s1 = 1.0, s2 = 1.0, s3 = 1.0, s4 = 1.0;
+                        op_c(b, m, &k1, &s1);
+                        op_c(b + Ns, k1, &k2, &s2);
+                        op_cdg(a + Ns, k2, &k3, &s3);
+                        op_cdg(a, k3, &k4, &s4);
+                        const int64_t j = or_binary_search(map, dim, k4);
+                        if (j > 0) {
+                            const double t = creal(s1 * s2 * s3 * s4 * psi[i] * conj(psi[j - 1]));
+                            e[1] += M->jp * t;
+                            e[6] += t;
+                        }
+                    }
+                }
+        }
+        /* HARTREE TERMS */
+        if (M->hfmode) {
+            for (int a = 0; a < Norb; a++)
+                e[2] += -0.5 * M->uloc[a] * (nup[a] + ndw[a]) * gsw + 0.25 * M->uloc[a] * gsw;
+            if (Norb > 1)
+                for (int a = 0; a < Norb; a++)
+                    for (int b = a + 1; b < Norb; b++) {
+                        const double nn = nup[a] + ndw[a] + nup[b] + ndw[b];
+                        e[2] += -0.5 * Ust * nn * gsw + 0.25 * Ust * gsw;
+                        e[2] += -0.5 * (Ust - Jh) * nn * gsw + 0.25 * (Ust - Jh) * gsw;
+                    }
+        }
+    }
+}
+
 /* <psi| c^+_{a s} c_{k s} + h.c. |psi> and <psi|n_{k s}|psi> with the normal
  * bath stride (ED_SETUP.f90:445-462), the derivatives of the sector energy
  * with respect to V_{s,a,k} and e_{s,a,k} (Hellmann-Feynman; the operators

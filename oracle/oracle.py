@@ -93,6 +93,7 @@ def _declare(L):
     L.or_observables_state.argtypes = [C.POINTER(_Model), _ip, C.c_int64, _dp, C.c_double,
                                        _dp, _dp, _dp, _dp, _dp, _dp]
     L.or_hf_terms_state.argtypes = [C.POINTER(_Model), _ip, C.c_int64, _dp, C.c_double, _dp, _dp]
+    L.or_local_energy_state.argtypes = [C.POINTER(_Model), _ip, C.c_int64, _dp, C.c_double, _dp]
     L.or_delta_bath.argtypes = [_dp, _dp, C.c_int32, _dp, C.c_int32, _dp]
     L.or_sigma_normal.argtypes = [_dp, _dp, C.c_int32, C.c_double, C.c_double, _dp, C.c_int32,
                                   _dp, _dp]
@@ -330,6 +331,29 @@ def observables_state(model, hmap, psi, peso):
     return out
 
 
+def local_energy_state(model, hmap, psi, peso, acc=None):
+    """local_energy_impurity's body for one state, ED_OBSERVABLES.f90:454-633:
+    adds into acc[8] = [Eknot, Epot without Ehartree, Ehartree, Dust, Dund,
+    Dse, Dph, 0]."""
+    acc = np.zeros(8) if acc is None else acc
+    psi = np.ascontiguousarray(psi, np.complex128)
+    ms = model._struct()
+    lib().or_local_energy_state(C.byref(ms), _p(hmap, C.c_int32), hmap.size,
+                                _p(psi.view(np.float64)), peso, _p(acc))
+    return acc
+
+
+def local_energies(acc):
+    """The reference's module variables after local_energy_impurity
+    (ED_OBSERVABLES.f90:635): Epot includes Ehartree; ed_Eint is never
+    assigned there and stays 0.  Returns eimp = [Epot, Eint, Ehartree, Eknot]
+    (ed_get_eimp_, ED_IO/get_eimp.f90:1-4) and doubles = [Dust, Dund, Dse,
+    Dph] (ed_get_doubles_, ED_IO/get_doubles.f90:1-4)."""
+    eimp = np.array([acc[1] + acc[2], 0.0, acc[2], acc[0]])
+    doubles = np.array([acc[3], acc[4], acc[5], acc[6]])
+    return eimp, doubles
+
+
 def hf_terms_state(model, hmap, psi, peso=1.0):
     """<c+_a c_k + h.c.> and <n_k> per physical spin (Hellmann-Feynman operators)."""
     no, nb = model.norb, model.nbath
@@ -470,6 +494,7 @@ def _gf_and_obs(model, states, egs, zeta, finite_t, lmats, lreal, wini, wfin, ep
     (:442-488), followed by get_sigma_normal.  states: [(e, nup, ndw, psi)]."""
     ns, no = model.ns, model.norb
     obs = {k: np.zeros(no) for k in ["dens", "dens_up", "dens_dw", "docc", "magz"]}
+    eacc = np.zeros(8)
     wm = matsubara(model.beta, lmats)
     wr = realaxis(wini, wfin, lreal)
     gm = np.zeros((model.nspin, no, lmats), np.complex128)
@@ -482,6 +507,7 @@ def _gf_and_obs(model, states, egs, zeta, finite_t, lmats, lreal, wini, wfin, ep
         o = observables_state(model, hm, psi, peso)
         for k in obs:
             obs[k] += o[k]
+        local_energy_state(model, hm, psi, peso, eacc)
         for ispin in range(model.nspin):
             for iorb in range(no):
                 isite = (iorb + 1) + ispin * ns
@@ -508,6 +534,7 @@ def _gf_and_obs(model, states, egs, zeta, finite_t, lmats, lreal, wini, wfin, ep
             sm[ispin, iorb] = sigma_normal(model.e[ispin, iorb], model.v[ispin, iorb], model.xmu,
                                            model.hloc[ispin, ispin, iorb, iorb].real, 1j * wm,
                                            gm[ispin, iorb])
+    obs["eimp"], obs["doubles"] = local_energies(eacc)
     return obs, gm, gr, sm, chains, wm
 
 
@@ -619,36 +646,8 @@ def solve_finite_t(model, lmats=256, lreal=0, wini=-5.0, wfin=5.0, eps=0.01, ngf
         while len(states) > 1 and np.exp(-model.beta * (states[-1][0] - egs)) <= cutoff:
             states.pop()
         new_total = max(len(states), nstates_step) + nstates_step
-    no = model.norb
-    obs = {k: np.zeros(no) for k in ["dens", "dens_up", "dens_dw", "docc", "magz"]}
-    wm = matsubara(model.beta, lmats)
-    wr = realaxis(wini, wfin, lreal)
-    gm = np.zeros((model.nspin, no, lmats), np.complex128)
-    gr = np.zeros((model.nspin, no, lreal), np.complex128)
-    for e, isec, psi in states:
-        a, b = secs[isec - 1]
-        hm = build_sector(ns, a, b)
-        peso = np.exp(-model.beta * (e - egs)) / zeta
-        o = observables_state(model, hm, psi.astype(np.complex128), peso)
-        for k in obs:
-            obs[k] += o[k]
-        for ispin in range(model.nspin):
-            for iorb in range(no):
-                isite = (iorb + 1) + ispin * ns
-                for particle, dn in ((True, 1), (False, -1)):
-                    jn = (a + dn, b) if ispin == 0 else (a, b + dn)
-                    if not (0 <= jn[0] <= ns and 0 <= jn[1] <= ns):
-                        continue
-                    jmap = build_sector(ns, *jn)
-                    n2, vv = gf_vvinit(particle, isite, hm, jmap, psi.astype(np.complex128))
-                    vv = vv / np.sqrt(n2)
-                    nlanc = min(jmap.size, ngfiter)
-                    al, bl, _ = lanczos_tridiag(model, jmap, vv, nlanc, nthreads=nthreads)
-                    gmt = np.zeros(lmats, np.complex128)
-                    grt = np.zeros(lreal, np.complex128)
-                    add_to_lanczos_gf(n2, e, egs, zeta, True, model.beta, al, bl,
-                                      1 if particle else -1, wm, wr, eps, gmt, grt)
-                    gm[ispin, iorb] += gmt
-                    gr[ispin, iorb] += grt
+    st4 = [(e, secs[isec - 1][0], secs[isec - 1][1], psi) for e, isec, psi in states]
+    obs, gm, gr, sm, chains, wm = _gf_and_obs(model, st4, egs, zeta, True, lmats, lreal, wini,
+                                              wfin, eps, ngfiter, nthreads)
     return dict(states=[(s[0], s[1]) for s in states], egs=egs, zeta=zeta, obs=obs, gmats=gm,
-                greal=gr, neigen=new_neigen, nstates_total=new_total)
+                greal=gr, smats=sm, neigen=new_neigen, nstates_total=new_total)
