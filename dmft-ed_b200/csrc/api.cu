@@ -550,15 +550,13 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         DM_REQUIRE(p->lanc_niter >= 1, DMFTED_ERR_ARG, "lanc_niter < 1");
         DM_REQUIRE(p->precision == DMFTED_FP64 || p->precision == DMFTED_MIXED, DMFTED_ERR_ARG,
                    "unknown precision mode");
-        DM_REQUIRE(!(p->jhflag && p->norb > 1 && (p->jx != 0.0 || p->jp != 0.0)),
-                   DMFTED_ERR_UNSUPPORTED,
-                   "Jhflag spin-exchange/pair-hopping is not available in this build");
         c = new dmfted_ctx();
         c->p = *p;
         if (c->p.lanc_ncheck <= 0) c->p.lanc_ncheck = 10;
         if (c->p.lanc_gf_threshold <= 0) c->p.lanc_gf_threshold = 1e-13;
         c->norb = p->norb;
         c->nbath = p->nbath;
+        c->jterms = p->jhflag && p->norb > 1 && (p->jx != 0.0 || p->jp != 0.0);
         c->nspin = p->nspin;
         c->ns = ns;
         c->device = p->device;

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "jterms.cuh"
 #include "reduce.cuh"
 #include "sector.cuh"
 #include "tridiag.cuh"
@@ -87,6 +88,18 @@ __device__ __forceinline__ T hx_elem(const Sec<T> &s, const BatchSmem<T> &sm, in
         h += (ell_neg(en) ? -v : v) * x[s.dimup * ell_col(en) + r];
     }
     return h;
+}
+
+// The Jhflag terms of (H x)_i, i = r + DimUp*q (zero without Jhflag).
+template <typename T>
+__device__ __forceinline__ T hx_jterms(const BatchTables<T> &tb, const Sec<T> &s, const T *x,
+                                       uint32_t r, uint32_t q) {
+    double h = 0.0;
+    for_jterms(s.wu[r], s.wd[q], tb.norb, tb.jx, tb.jp, [&](uint32_t tu, uint32_t td, double cf) {
+        const int64_t j = tb.rank[tu] + (int64_t)s.dimup * tb.rank[td];
+        if (DM_IN(j, s.dim)) h += cf * (double)x[j];
+    });
+    return (T)h;
 }
 
 template <int CL>
@@ -192,6 +205,7 @@ __device__ void chain_job(const BatchTables<T> &tb, BatchSmem<T> &sm, const Chai
     const bool lead = rank == 0 && tid == 0;  // writes the job's outputs
     const uint32_t i0 = (uint32_t)(rank * bd + tid), st = (uint32_t)(CL * bd);
     const Sec<T> s = make_sec(tb, J.tnup, J.tndw);
+    const bool jflag = tb.jx != 0.0 || tb.jp != 0.0;
     const uint32_t dim = s.dim;
     const uint32_t ld = (dim + 31u) & ~31u;
     if (!DM_IN(J.work_off + 2 * (int64_t)ld - 1, cap.work) || !DM_IN(J.slot, cap.slots) ||
@@ -247,7 +261,8 @@ __device__ void chain_job(const BatchTables<T> &tb, BatchSmem<T> &sm, const Chai
         a[0].zero();
         for (uint32_t i = i0; i < dim; i += st) {
             const uint32_t r = i % s.dimup, q = i / s.dimup;
-            const T h = hx_elem(s, sm, ni, tb.W, tb.P, Q, r, q);
+            T h = hx_elem(s, sm, ni, tb.W, tb.P, Q, r, q);
+            if (jflag) h += hx_jterms(tb, s, Q, r, q);
             const T u = (T)(sc * (double)h - cprev * (double)P[i]);
             P[i] = u;
             a[0].add((double)Q[i] * (double)u);
@@ -513,6 +528,7 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
     const bool lead = rank == 0 && tid == 0;  // writes the job's outputs
     const uint32_t i0 = (uint32_t)(rank * bd + tid), st = (uint32_t)(CL * bd);
     const Sec<T> s = make_sec(tb, J.nup, J.ndw);
+    const bool jflag = tb.jx != 0.0 || tb.jp != 0.0;
     const uint32_t dim = s.dim;
     const uint32_t ld = (dim + 31u) & ~31u;
     if (!DM_IN(J.basis_off + (int64_t)(J.kmax + 1) * ld - 1, cap.work) ||
@@ -562,7 +578,8 @@ __device__ void eigs_job(const BatchTables<T> &tb, BatchSmem<T> &sm, double *dyn
         a1[0].zero();
         for (uint32_t i = i0; i < dim; i += st) {
             const uint32_t r = i % s.dimup, q = i / s.dimup;
-            const T h = hx_elem(s, sm, ni, tb.W, tb.P, x, r, q);
+            T h = hx_elem(s, sm, ni, tb.W, tb.P, x, r, q);
+            if (jflag) h += hx_jterms(tb, s, x, r, q);
             const T u = (T)(sc * (double)h - cprev * (double)xp[i]);
             y[i] = u;
             a1[0].add((double)x[i] * (double)u);
@@ -1200,6 +1217,7 @@ struct SecondLane {
         c->red_partials.swap(c->red_partials2);
         c->red_counter.swap(c->red_counter2);
         c->chainbuf.swap(c->chainbuf2);
+        c->jscratch.swap(c->jscratch2);
     }
 };
 

@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "jterms.cuh"
 #include "sector.cuh"
 #include "tridiag.cuh"
 
@@ -99,6 +100,12 @@ __global__ void __launch_bounds__(kDenseThreads, 1)
                 const double v = tb.sp[1].par[ell_par(en)];
                 row[s.dimup * ell_col(en) + r] += ell_neg(en) ? -v : v;
             }
+            if (tb.jx != 0.0 || tb.jp != 0.0)
+                for_jterms(s.wu[r], s.wd[q], tb.norb, tb.jx, tb.jp,
+                           [&](uint32_t tu, uint32_t td, double cf) {
+                               const int64_t j = tb.rank[tu] + (int64_t)s.dimup * tb.rank[td];
+                               if (DM_IN(j, n)) row[j] += cf;
+                           });
         }
         __syncthreads();
         double *sa = dyn, *sb = dyn + n;

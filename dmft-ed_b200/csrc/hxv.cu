@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "hxv.cuh"
+#include "jterms.cuh"
 
 namespace dmfted {
 
@@ -1078,6 +1079,97 @@ static void launch_hxv(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int 
     hv_timer_end(c, bytes);
 }
 
+// y += H_J x for the Jhflag spin-exchange / pair-hopping terms (jterms.cuh),
+// on nvec vectors vstride apart, each nstack stacked halves of the sector
+// (dim apart), in the view's storage order.  One thread per element gathers
+// the targets through the rank table.
+template <typename T>
+__global__ void k_hxv_jadd(const uint32_t *__restrict__ wup, const uint32_t *__restrict__ wdw,
+                           const int32_t *__restrict__ rank, uint32_t dimup, uint32_t dimdw,
+                           int swapped, int norb, double jx, double jp, const T *x, T *y,
+                           int nstack, int nvec, int64_t vstride) {
+    const int64_t dim = (int64_t)dimup * dimdw;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < dim;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = swapped ? (uint32_t)(e / dimdw) : (uint32_t)(e % dimup);
+        const uint32_t q = swapped ? (uint32_t)(e % dimdw) : (uint32_t)(e / dimup);
+        for (int v = 0; v < nvec; v++)
+            for (int h = 0; h < nstack; h++) {
+                const int64_t base = v * vstride + h * dim;
+                double acc = 0.0;
+                for_jterms(wup[r], wdw[q], norb, jx, jp, [&](uint32_t tu, uint32_t td, double cf) {
+                    const int64_t rt = rank[tu], qt = rank[td];
+                    const int64_t j = swapped ? qt + (int64_t)dimdw * rt : rt + (int64_t)dimup * qt;
+                    if (DM_IN(j, dim)) acc += cf * (double)x[base + j];
+                });
+                if (acc != 0.0) y[base + e] = (T)((double)y[base + e] + acc);
+            }
+    }
+}
+
+template <typename T>
+static void hxv_jadd(dmfted_ctx *c, const SectorView &s, const T *x, T *y, int nstack, int nvec,
+                     int64_t vstride) {
+    const int grid = (int)std::min<int64_t>(std::max<int64_t>(div_up(s.dim, 256), 1),
+                                            (int64_t)num_sms(c) * 8);
+    k_hxv_jadd<T><<<grid, 256, 0, c->stream>>>(c->words.p + s.offup, c->words.p + s.offdw,
+                                                c->rank.p, (uint32_t)s.dimup, (uint32_t)s.dimdw,
+                                                s.swapped ? 1 : 0, c->norb, c->p.jx, c->p.jp, x, y,
+                                                nstack, nvec, vstride);
+    DM_CHECK_LAUNCH();
+    c->launches++;
+}
+
+// The Lanczos combination of the fused step, for products computed in parts
+// (Jhflag): u = sc hx - cprev x_prev into y (y may be x_prev: each element is
+// read before it is written, by the same thread), alpha_k = sc <x, u>.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_lz_combine(T *y, const T *hx, const T *x,
+                                                            const T *xprev, int64_t n,
+                                                            LanczosScalars lz, int k,
+                                                            double *partials, unsigned *counter) {
+    if (lz.status[0]) return;  // the recurrence has ended
+    const double sc = lz.scale[k], cprev = k > 0 ? lz.beta[k] * lz.scale[k - 1] : 0.0;
+    CSum d;
+    d.zero();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const T u = (T)(sc * (double)hx[i] - cprev * (double)xprev[i]);
+        y[i] = u;
+        d.add((double)x[i] * (double)u);
+    }
+    CSum arr[1] = {d};
+    double tot[1];
+    if (grid_reduce<1>(arr, partials, counter, tot)) {
+        if (threadIdx.x == 0) lz.alpha[k] = sc * tot[0];
+    }
+}
+
+// Lanczos step k in parts: the plain product into the context's scratch, the
+// Jhflag terms, then the combination and alpha (the fused kernels hold no
+// Jhflag terms; y may alias x_prev, as the in-place chains have it).
+template <typename T>
+static void lanczos_step_parts(dmfted_ctx *c, const SectorView &s, const T *x, const T *xprev,
+                               T *y, const LanczosScalars &lz, int k, int nstack,
+                               double *partials, unsigned *counter) {
+    const int64_t n = s.dim * nstack;
+    c->jscratch.alloc((size_t)n * sizeof(T) + 256);
+    T *hx = reinterpret_cast<T *>(c->jscratch.p);
+    HxvArgs<T> a = make_hxv_args<T>(c, s);
+    a.nstack = nstack;
+    a.x = x;
+    a.y = hx;
+    HxvCfg g = hxv_config<T>(c, s, a, nstack);
+    launch_hxv<T, false>(c, a, g, 1);
+    hxv_jadd<T>(c, s, x, hx, nstack, 1, 0);
+    const int grid = (int)std::min<int64_t>(std::max<int64_t>(div_up(n, kRedThreads), 1),
+                                            std::min<int64_t>(kMaxRedBlocks, (int64_t)num_sms(c) * 8));
+    k_lz_combine<T><<<grid, kRedThreads, 0, c->stream>>>(y, hx, x, xprev, n, lz, k, partials,
+                                                        counter);
+    DM_CHECK_LAUNCH();
+    c->launches++;
+}
+
 template <typename T>
 static void hxv_plain(dmfted_ctx *c, const SectorView &s, const T *x, T *y, int nvec) {
     HxvArgs<T> a = make_hxv_args<T>(c, s);
@@ -1085,6 +1177,7 @@ static void hxv_plain(dmfted_ctx *c, const SectorView &s, const T *x, T *y, int 
     a.y = y;
     HxvCfg g = hxv_config<T>(c, s, a);
     launch_hxv<T, false>(c, a, g, nvec);
+    if (c->jterms) hxv_jadd<T>(c, s, x, y, 1, nvec, a.vstride);
 }
 
 void hxv_f64(dmfted_ctx *c, const SectorView &s, const double *x, double *y, int nvec) {
@@ -1098,6 +1191,11 @@ void hxv_f32(dmfted_ctx *c, const SectorView &s, const float *x, float *y, int n
 template <typename T>
 void hxv_lanczos_step(dmfted_ctx *c, const SectorView &s, const T *x, const T *xprev, T *y,
                       const LanczosScalars &lz, int k, int nstack) {
+    if (c->jterms) {
+        lanczos_step_parts<T>(c, s, x, xprev, y, lz, k, nstack, c->red_partials.p,
+                              c->red_counter.p);
+        return;
+    }
     HxvArgs<T> a = make_hxv_args<T>(c, s);
     a.nstack = nstack;
     a.x = x;
@@ -1128,6 +1226,9 @@ template <typename T>
 void hxv_lanczos_step_scratch(dmfted_ctx *c, const SectorView &s, const T *x, const T *xprev, T *y,
                               const LanczosScalars &lz, int k, double *partials,
                               unsigned *counter) {
+    DM_REQUIRE(!c->jterms, DMFTED_ERR_UNSUPPORTED,
+               "the Jhflag terms need scratch memory of the size of a vector: "
+               "use dmfted_lanc_tridiag for this model");
     HxvArgs<T> a = make_hxv_args<T>(c, s);
     a.x = x;
     a.y = y;

@@ -194,6 +194,7 @@ struct dmfted_ctx {
     std::vector<double> bath_e, bath_v;  // [nspin][norb][nbath]
     std::vector<double> hloc;            // complex (re,im), Fortran order
     bool bath_set = false;
+    bool jterms = false;  // Jhflag spin-exchange / pair-hopping terms present (Norb > 1)
     int device = 0;
     cudaStream_t stream = nullptr;
     // device Fock tables
@@ -273,6 +274,8 @@ struct dmfted_ctx {
     // locked vectors it keeps its Krylov space orthogonal to
     dmfted::DBuf<double> lockpool;
     dmfted::DBuf<double> gsvec;  // eigenvectors returned by dmfted_gs_lanczos
+    dmfted::DBuf<uint8_t> jscratch;  // H*x of a Lanczos step computed in parts (Jhflag)
+    dmfted::DBuf<uint8_t> jscratch2; // the same for the second chain lane
     int64_t launches = 0;
     // live timing of the H*v launches (dmfted_hxv_timing)
     bool hv_timing = false;

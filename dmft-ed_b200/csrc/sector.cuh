@@ -30,6 +30,7 @@ struct BatchTables {
     int64_t binom[kMaxNs + 1];  // class sizes
     int64_t nrank;              // entries of the rank table (2^Ns)
     int norb, P, W;
+    double jx, jp;              // Jhflag spin-exchange / pair hopping (0: none)
 };
 
 template <typename T>
@@ -59,6 +60,8 @@ inline BatchTables<T> batch_tables(const dmfted_ctx *c) {
     b.norb = c->norb;
     b.P = c->P;
     b.W = std::max(c->W, 1);
+    b.jx = c->jterms ? c->p.jx : 0.0;
+    b.jp = c->jterms ? c->p.jp : 0.0;
     return b;
 }
 

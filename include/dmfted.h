@@ -188,7 +188,9 @@ int dmfted_lanc_tridiag(dmfted_ctx *ctx, int32_t isector, const double *vvinit, 
  * convention as dmfted_lanc_tridiag) and d_nused, all device pointers.  The
  * reduction scratch is a fixed array inside the library (about 90 KB per GPU,
  * held until the process exits); the call allocates and frees nothing.
- * Limit: 1 <= nlanc <= 1022, else DMFTED_ERR_ARG.  Calls on one device share
+ * Limit: 1 <= nlanc <= 1022, else DMFTED_ERR_ARG; a context whose model has
+ * the Jhflag spin-exchange / pair-hopping terms is refused with
+ * DMFTED_ERR_UNSUPPORTED (its Lanczos step needs a vector of scratch).  Calls on one device share
  * the array and must not overlap on the GPU.  The first call on a device
  * looks up the array's device address; make it before any stream capture.
  * Returns after the results are written (the context's stream is

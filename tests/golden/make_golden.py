@@ -36,9 +36,12 @@ def jw_ops(nlev):
     return ops
 
 
-def hamiltonian(norb, nbath, e, v, uloc, ust, jh, xmu, hfmode, hloc_diag, hloc_off=None):
+def hamiltonian(norb, nbath, e, v, uloc, ust, jh, xmu, hfmode, hloc_diag, hloc_off=None,
+                jx=0.0, jp=0.0):
     """Full Fock-space H of the normal-bath impurity model, normal ed_mode.
-    e, v: [2 spins][norb][nbath]; hloc_diag: [2][norb]; hloc_off: [2][norb][norb]."""
+    e, v: [2 spins][norb][nbath]; hloc_diag: [2][norb]; hloc_off: [2][norb][norb];
+    jx, jp: spin-exchange J c+_{a up} c+_{b dw} c_{a dw} c_{b up} and pair hopping
+    J c+_{a up} c+_{a dw} c_{b dw} c_{b up} over a != b (the Jhflag terms)."""
     ns = (nbath + 1) * norb
     c = jw_ops(2 * ns)
     cd = [m.T for m in c]
@@ -72,6 +75,14 @@ def hamiltonian(norb, nbath, e, v, uloc, ust, jh, xmu, hfmode, hloc_diag, hloc_o
                 eye = np.eye(H.shape[0])
                 H += -0.5 * ust * nab + 0.25 * ust * eye
                 H += -0.5 * (ust - jh) * nab + 0.25 * (ust - jh) * eye
+    for a in range(norb):
+        for b in range(norb):
+            if a == b:
+                continue
+            if jx != 0.0:
+                H += jx * cd[lev(0, a)] @ cd[lev(1, b)] @ c[lev(1, a)] @ c[lev(0, b)]
+            if jp != 0.0:
+                H += jp * cd[lev(0, a)] @ cd[lev(1, a)] @ c[lev(1, b)] @ c[lev(0, b)]
     return H, ns
 
 
@@ -149,6 +160,39 @@ def main():
     h1[1:, 0] = v
     out["u0_e"], out["u0_v"] = e, v
     out["u0_levels"] = np.linalg.eigvalsh(h1)
+    # a Jhflag case (spin exchange and pair hopping), from its own generator so
+    # that the cases above keep their values
+    rng2 = np.random.default_rng(20251203)
+    for norb, nbath, jx, jp, split in ((2, 2, 0.4, 0.3, False), (3, 1, 0.3, 0.25, True)):
+        ic = len(cases)
+        e1 = rng2.uniform(-1, 1, (norb, nbath))
+        v1 = 0.5 + rng2.uniform(-0.1, 0.1, (norb, nbath))
+        e2 = e1 + rng2.uniform(-0.2, 0.2, (norb, nbath)) if split else e1.copy()
+        v2 = v1 + rng2.uniform(-0.05, 0.05, (norb, nbath)) if split else v1.copy()
+        uloc3 = [3.0] * norb + [0.0] * (3 - norb)
+        hd = np.zeros((2, norb))
+        H, ns = hamiltonian(norb, nbath, [e1, e2], [v1, v2], uloc3, 2.0, 0.5, 0.0, True, hd,
+                            None, jx, jp)
+        spec = {}
+        for nup in range(ns + 1):
+            for ndw in range(ns + 1):
+                spec[(nup, ndw)] = sector_spectrum(H, ns, nup, ndw, 4)
+        sectors = np.array(sorted(spec.keys()), np.int32)
+        low = np.full((len(sectors), 4), np.nan)
+        for i, sec in enumerate(sectors):
+            lv = spec[tuple(sec)]
+            low[i, :len(lv)] = lv
+        pre = f"c{ic}_"
+        out[pre + "norb"], out[pre + "nbath"] = norb, nbath
+        out[pre + "nspin"] = 2 if split else 1
+        out[pre + "uloc"] = np.array(uloc3)
+        out[pre + "ust"], out[pre + "jh"], out[pre + "xmu"], out[pre + "hfmode"] = 2.0, 0.5, 0.0, 1
+        out[pre + "jx"], out[pre + "jp"] = jx, jp
+        out[pre + "e"], out[pre + "v"] = np.stack([e1, e2]), np.stack([v1, v2])
+        out[pre + "hloc_diag"], out[pre + "hloc_off"] = hd, np.zeros((2, norb, norb))
+        out[pre + "sectors"], out[pre + "low"] = sectors, low
+        cases.append(ic)
+    out["ncases"] = len(cases)
     np.savez_compressed(os.path.join(HERE, "pins.npz"), **out)
     print("wrote", os.path.join(HERE, "pins.npz"), len(cases), "cases")
 

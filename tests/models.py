@@ -19,9 +19,11 @@ def golden_models():
         hl = np.zeros((nspin, nspin, norb, norb), complex)
         for s in range(nspin):
             hl[s, s] = np.diag(g("hloc_diag")[s]) + g("hloc_off")[s]
+        jx = float(g("jx")) if f"c{ic}_jx" in z else 0.0
+        jp = float(g("jp")) if f"c{ic}_jp" in z else 0.0
         m = O.Model(norb=norb, nbath=nbath, nspin=nspin, uloc=tuple(g("uloc")), ust=float(g("ust")),
-                    jh=float(g("jh")), xmu=float(g("xmu")), hfmode=bool(g("hfmode")), e=e, v=v,
-                    hloc=hl)
+                    jh=float(g("jh")), jx=jx, jp=jp, jhflag=(jx != 0.0 or jp != 0.0),
+                    xmu=float(g("xmu")), hfmode=bool(g("hfmode")), e=e, v=v, hloc=hl)
         out.append((m, g("sectors"), g("low")))
     return out
 

@@ -157,3 +157,34 @@ def test_grid_chains_on_two_lanes_equal_in_turn(precision):
     assert np.array_equal(one["e"], two["e"])
     for k in ("dens", "docc", "magz"):
         assert np.array_equal(one["obs"][k], two["obs"][k]), k
+
+
+@pytest.mark.parametrize("batch_dim", [str(1 << 17), "0"])
+def test_jhflag_finite_t_batch_and_grid_match_oracle(batch_dim):
+    # spin exchange and pair hopping (HxVint.f90:45-97) in the batched
+    # eigensolve and chains (and, with batching off, the grid-wide product)
+    m = split_model(23, 2, 2, beta=30.0, ust=2.0, jh=0.5)
+    m.jx, m.jp, m.jhflag = 0.4, 0.3, True
+    p = dict(norb=2, nbath=2, nspin=2, uloc=list(m.uloc), ust=m.ust, jh=m.jh, jx=m.jx, jp=m.jp,
+             jhflag=1, beta=m.beta, lmats=128, lreal=0, lanc_nstates_total=12)
+    old = os.environ.get("DMFTED_BATCH_MAX_DIM")
+    os.environ["DMFTED_BATCH_MAX_DIM"] = batch_dim
+    try:
+        s = dmfted.EDSolver(dmfted.default_params(**p))
+    finally:
+        if old is None:
+            os.environ.pop("DMFTED_BATCH_MAX_DIM", None)
+        else:
+            os.environ["DMFTED_BATCH_MAX_DIM"] = old
+    s.ed_solve(m.bath_array())
+    e, secs, z = s.eigenspace()
+    ref = O.solve_finite_t(m, lmats=128, nstates_total=12, nthreads=4)
+    re = np.array([x[0] for x in ref["states"]])
+    assert np.allclose(e, re, rtol=0, atol=1e-10 * max(1.0, np.abs(re).max()))
+    assert np.array_equal(secs, np.array([x[1] for x in ref["states"]]))
+    g = s.ed_get_gimp_matsubara()
+    for ispin in range(2):
+        for a in range(2):
+            assert np.abs(g[ispin, ispin, a, a] - ref["gmats"][ispin, a]).max() <= 1e-8
+    assert np.allclose(s.ed_get_doubles(), ref["obs"]["doubles"], atol=1e-9)
+    s.close()

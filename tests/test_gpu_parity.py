@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
 def solver_for(model, **kw):
     ul = list(model.uloc) + [0.0] * (3 - len(model.uloc))
     args = dict(norb=model.norb, nbath=model.nbath, nspin=model.nspin, uloc=ul, ust=model.ust,
-                jh=model.jh, xmu=model.xmu, beta=model.beta, hfmode=int(model.hfmode))
+                jh=model.jh, jx=model.jx, jp=model.jp, jhflag=int(model.jhflag), xmu=model.xmu,
+                beta=model.beta, hfmode=int(model.hfmode))
     args.update(kw)
     p = dmfted.default_params(**args)
     s = dmfted.EDSolver(p, hloc=model.hloc)
@@ -254,8 +255,9 @@ def test_ed_solve_cfg1_fp64():
     _compare_solve(cfg1(), 4, 4, dmfted.FP64, 1e-8)
 
 
-@pytest.mark.parametrize("ic", [3, 4, 5])
+@pytest.mark.parametrize("ic", [3, 4, 5, 6, 7])
 def test_ed_solve_multiorbital_fp64(ic):
+    # 6, 7: Jhflag spin exchange and pair hopping
     m, sectors, _ = golden_models()[ic]
     ns = m.ns
     _compare_solve(m, ns // 2, ns - ns // 2, dmfted.FP64, 1e-8, lmats=256)

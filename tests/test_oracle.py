@@ -68,8 +68,9 @@ def test_sector_tables():
     assert list(O.sector_tables(2, 3)["getbathstride"]) == [3, 6, 4, 7, 5, 8]
 
 
-@pytest.mark.parametrize("case", range(6))
+@pytest.mark.parametrize("case", range(8))
 def test_sector_spectra_against_jordan_wigner(case):
+    # cases 6 and 7 carry the Jhflag spin-exchange and pair-hopping terms
     model, sectors, low = golden_models()[case]
     ns = model.ns
     for (nup, ndw), ref in zip(sectors, low):
