@@ -235,7 +235,7 @@ static void ed_analysis_finite_t(dmfted_ctx *c) {
     } else {
         while (c->states.size() > 1 &&
                std::exp(-p.beta * (c->states.back().e - c->egs)) <= p.cutoff)
-            c->states.pop_back();
+            states_pop_last(c);
         c->nstates_total =
             std::max<int>((int)c->states.size(), p.lanc_nstates_step) + p.lanc_nstates_step;
     }
@@ -345,7 +345,6 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "ed_solve: bath not set");
     const dmfted_params &p = c->p;
     c->finite_t = p.lanc_nstates_total != 1;  // ED_SETUP.f90:242-246
-    DM_REQUIRE(!p.ed_twin, DMFTED_ERR_UNSUPPORTED, "ed_twin is not available in this build");
     std::vector<int> list;
     if (sectors && nsect_list > 0) {
         for (int i = 0; i < nsect_list; i++) {

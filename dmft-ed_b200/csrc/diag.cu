@@ -53,7 +53,7 @@ static int64_t state_dim(const dmfted_ctx *c, int isector) {
 static int64_t states_used(const dmfted_ctx *c) {
     int64_t u = 0;
     for (auto &s : c->states)
-        if (!s.src) u = std::max<int64_t>(u, s.off + state_dim(c, s.isector));
+        if (!s.src && s.off >= 0) u = std::max<int64_t>(u, s.off + state_dim(c, s.isector));
     return u;
 }
 
@@ -75,26 +75,73 @@ static void states_reserve(dmfted_ctx *c, int64_t used, int64_t need) {
     }
 }
 
-// Energy-ordered insertion after equal energies (es_insert_state_c,
-// ED_EIGENSPACE.f90:157-213: traverse until e <= next).
-static void states_insert(dmfted_ctx *c, const dmfted_ctx::State &st) {
-    auto it = c->states.begin();
-    while (it != c->states.end() && !(st.e <= it->e)) ++it;
-    c->states.insert(it, st);
+// The twin sector (ndw, nup) of a sector (get_twin_sector).
+static int twin_sector(const dmfted_ctx *c, int isector) {
+    const int nup = c->getnup[isector - 1], ndw = c->getndw[isector - 1];
+    return c->getsector[ndw * (c->ns + 1) + nup];
 }
 
-// Copies every state whose vector is still held elsewhere into the store.
+// Energy-ordered insertion after equal energies (es_insert_state_c,
+// ED_EIGENSPACE.f90:157-213: traverse until e <= next); with twin, the twin
+// entry follows the state directly.
+static void states_insert(dmfted_ctx *c, const dmfted_ctx::State &st, bool twin = false) {
+    auto it = c->states.begin();
+    while (it != c->states.end() && !(st.e <= it->e)) ++it;
+    it = c->states.insert(it, st);
+    if (twin) {
+        dmfted_ctx::State tw{st.e, twin_sector(c, st.isector), -1, nullptr};
+        tw.itwin = true;
+        c->states.insert(it + 1, tw);
+    }
+}
+
+// es_pop_state on the last entry (ED_EIGENSPACE.f90:219-299): a twin entry
+// goes together with its state.
+void states_pop_last(dmfted_ctx *c) {
+    if (c->states.empty()) return;
+    const bool tw = c->states.back().itwin;
+    c->states.pop_back();
+    if (tw && !c->states.empty()) c->states.pop_back();
+}
+
+// B[q + DimDw*r] = A[r + DimUp*q]: the twin vector of a state of sector A
+// (DimUp x DimDw) in the twin sector B, whose up words are A's down words.
+__global__ void k_twin_transpose(const double *A, double *B, int64_t dimup, int64_t dimdw) {
+    const int64_t n = dimup * dimdw;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = k % dimup, q = k / dimup;
+        B[q + dimdw * r] = A[k];
+    }
+}
+
+// Copies every state whose vector is still held elsewhere into the store and
+// builds the twin entries' vectors from their states'.
 static void states_materialize(dmfted_ctx *c) {
     int64_t used = states_used(c), need = (used + 31) / 32 * 32;
     for (auto &s : c->states)
-        if (s.src) need = (need + state_dim(c, s.isector) + 31) / 32 * 32;
+        if (s.src || s.itwin) need = (need + state_dim(c, s.isector) + 31) / 32 * 32;
     states_reserve(c, used, need);
     int64_t off = (used + 31) / 32 * 32;
-    for (auto &s : c->states) {
-        if (!s.src) continue;
+    for (size_t i = 0; i < c->states.size(); i++) {
+        auto &s = c->states[i];
         const int64_t dim = state_dim(c, s.isector);
-        DM_CUDA(cudaMemcpyAsync(c->states64.p + off, s.src, dim * sizeof(double),
-                                cudaMemcpyDeviceToDevice, c->stream));
+        if (s.src) {
+            DM_CUDA(cudaMemcpyAsync(c->states64.p + off, s.src, dim * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+        } else if (s.itwin && s.off < 0) {
+            DM_REQUIRE(i > 0 && !c->states[i - 1].itwin, DMFTED_ERR_STATE,
+                       "eigenspace: a twin entry without its state");
+            const auto &a = c->states[i - 1];
+            const int64_t du = c->binom[c->getnup[a.isector - 1]];
+            const int64_t dd = c->binom[c->getndw[a.isector - 1]];
+            k_twin_transpose<<<(int)std::min<int64_t>(div_up(dim, 256), 4 * num_sms(c)), 256, 0,
+                               c->stream>>>(c->states64.p + a.off, c->states64.p + off, du, dd);
+            DM_CHECK_LAUNCH();
+            c->launches++;
+        } else {
+            continue;
+        }
         s.off = off;
         s.src = nullptr;
         off = (off + dim + 31) / 32 * 32;
@@ -106,11 +153,12 @@ static void states_materialize(dmfted_ctx *c) {
 // limit insert; at the limit insert only below the highest energy, which is
 // popped first (es_pop_state, :219-299).  The vector stays where it is until
 // states_materialize.
-static void states_add_capped(dmfted_ctx *c, double e, int isector, const double *psi, int size) {
+static void states_add_capped(dmfted_ctx *c, double e, int isector, const double *psi, int size,
+                              bool twin) {
     const bool take = (int)c->states.size() < size;
     if (!take && !(!c->states.empty() && e < c->states.back().e)) return;
-    if (!take) c->states.pop_back();
-    states_insert(c, dmfted_ctx::State{e, isector, -1, psi});
+    if (!take) states_pop_last(c);
+    states_insert(c, dmfted_ctx::State{e, isector, -1, psi}, twin);
 }
 
 // ---------------------------------------------------------------------------
@@ -430,11 +478,18 @@ int64_t ed_diag(dmfted_ctx *c, const std::vector<int> &list) {
         jobs.push_back(j);
     }
     const int64_t hv = sector_spectra(c, jobs, c->finite_t, c->finite_t ? c->nstates_total : 0);
+    // Tflag of ED_DIAG.f90:120-123: twin entries for the states of a sector
+    // with nup != ndw when ed_twin is on
+    auto tflag = [&](int isector) {
+        return p.ed_twin && c->twin_mask[isector - 1] &&
+               c->getnup[isector - 1] != c->getndw[isector - 1];
+    };
     if (c->finite_t) {
         // ED_DIAG.f90:196-200: i = 1..Neigen into the capped list
         for (auto &j : jobs)
             for (auto &pr : ordered_pairs(c, j, j.neigen))
-                states_add_capped(c, pr.first, j.isector, pr.second, c->nstates_total);
+                states_add_capped(c, pr.first, j.isector, pr.second, c->nstates_total,
+                                  tflag(j.isector));
     } else {
         // ED_DIAG.f90:202-214
         double oldzero = 1000.0;
@@ -445,10 +500,12 @@ int64_t ed_diag(dmfted_ctx *c, const std::vector<int> &list) {
                 if (enemin < oldzero - 10.0 * gsth) {
                     oldzero = enemin;
                     states_reset(c);
-                    states_insert(c, dmfted_ctx::State{enemin, j.isector, -1, pr.second});
+                    states_insert(c, dmfted_ctx::State{enemin, j.isector, -1, pr.second},
+                                  tflag(j.isector));
                 } else if (std::fabs(enemin - oldzero) <= gsth) {
                     oldzero = std::min(oldzero, enemin);
-                    states_insert(c, dmfted_ctx::State{enemin, j.isector, -1, pr.second});
+                    states_insert(c, dmfted_ctx::State{enemin, j.isector, -1, pr.second},
+                                  tflag(j.isector));
                 }
             }
     }

@@ -290,6 +290,12 @@ struct dmfted_ctx {
         int isector;
         int64_t off;                  // offset (elements) of the vector in states64
         const double *src = nullptr;  // not yet copied: the vector is still here
+        // twin entry of ed_twin (es_insert_state_c, ED_EIGENSPACE.f90:185-195):
+        // the spin-flipped copy of the state just before it in the list,
+        // sector (ndw, nup); its vector is the transpose of that state's
+        // DimUp x DimDw matrix (es_return_cvector with twin_sector_order,
+        // ED_EIGENSPACE.f90:399-430, ED_SETUP.f90:1098-1126)
+        bool itwin = false;
     };
     std::vector<State> states;  // energy-ordered eigenspace
     dmfted::DBuf<double> states64;
@@ -394,6 +400,8 @@ int64_t ed_diag(dmfted_ctx *c, const std::vector<int> &list);
 int sector_eigenpairs(dmfted_ctx *c, int isector, int neigen, double *evals_h, double *vecs,
                       int64_t *steps);
 void states_reset(dmfted_ctx *c);
+// es_pop_state on the last entry: a twin entry goes together with its state.
+void states_pop_last(dmfted_ctx *c);
 
 // ---- hxv.cu --------------------------------------------------------------
 // y = H x for nvec vectors of sector s (plain product).

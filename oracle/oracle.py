@@ -540,7 +540,7 @@ def _gf_and_obs(model, states, egs, zeta, finite_t, lmats, lreal, wini, wfin, ep
 
 def solve_t0(model, sectors=None, nstates_sector=6, gs_threshold=1e-9, dim_threshold=256,
              lmats=4096, lreal=0, wini=-5.0, wfin=5.0, eps=0.01, ngfiter=200, nitermax=512,
-             tol=1e-12, nthreads=1):
+             tol=1e-12, nthreads=1, twin=False):
     """Zero-temperature impurity solve (lanc_nstates_total = 1) over the given
     sectors [(nup, ndw)] in the reference's order (default: all of them):
     ed_diag_c's T=0 branch (ED_DIAG.f90:93-228).  Every sector yields
@@ -557,8 +557,11 @@ def solve_t0(model, sectors=None, nstates_sector=6, gs_threshold=1e-9, dim_thres
     ns = model.ns
     if sectors is None:
         sectors = [(a, b) for a in range(ns + 1) for b in range(ns + 1)]
+    if twin:
+        sectors = [(a, b) for a, b in sectors if a >= b]
     from math import comb
-    states = []  # [e, nup, ndw, psi]
+    allsecs = [(a, b) for a in range(ns + 1) for b in range(ns + 1)]
+    lst = _StateList()
     oldzero = 1000.0
     nl_total = 0
     for a, b in sectors:
@@ -572,21 +575,18 @@ def solve_t0(model, sectors=None, nstates_sector=6, gs_threshold=1e-9, dim_thres
             w, V = [e0], psi[:, None]
         else:
             w, V = _sector_eigs(model, hm, neigen)
+        isec = a * (ns + 1) + b + 1
+        tsec = b * (ns + 1) + a + 1 if (twin and a != b) else None
         for i in range(neigen):
             en = float(w[i])
             if en < oldzero - 10.0 * gs_threshold:
                 oldzero = en
-                states = [[en, a, b, V[:, i]]]
+                lst = _StateList()
+                lst.add(en, isec, V[:, i], tsec)
             elif abs(en - oldzero) <= gs_threshold:
                 oldzero = min(oldzero, en)
-                states.append([en, a, b, V[:, i]])
-    # es_add_state keeps the list energy-ordered, after equal energies
-    ordered = []
-    for st in states:
-        i = 0
-        while i < len(ordered) and not (st[0] <= ordered[i][0]):
-            i += 1
-        ordered.insert(i, st)
+                lst.add(en, isec, V[:, i], tsec)
+    ordered = [list(x) for x in _materialize(ns, allsecs, lst)]
     egs = min(s[0] for s in ordered)
     zeta = float(len(ordered))
     obs, gm, gr, sm, chains, wm = _gf_and_obs(model, ordered, egs, zeta, False, lmats, lreal,
@@ -596,13 +596,72 @@ def solve_t0(model, sectors=None, nstates_sector=6, gs_threshold=1e-9, dim_thres
                 wm=wm, nlanc=nl_total)
 
 
+def twin_vector(ns, nup, ndw, vec):
+    """es_return_cvector for a twin entry (ED_EIGENSPACE.f90:399-430): the
+    vector in the twin sector (ndw, nup) rebuilt from the state's vector of
+    sector (nup, ndw) through twin_sector_order (ED_SETUP.f90:1098-1126):
+    Order = the permutation that sorts flip_state(map(i)) (up and down words
+    exchanged, :1136-1161), vector(i) = cvec(Order(i))."""
+    hm = build_sector(ns, nup, ndw).astype(np.int64)
+    mask = (1 << ns) - 1
+    flipped = ((hm >> ns) & mask) | ((hm & mask) << ns)
+    order = np.argsort(flipped, kind="stable")
+    return np.asarray(vec)[order]
+
+
+class _StateList:
+    """state_list with es_insert_state / es_add_state / es_pop_state
+    (ED_EIGENSPACE.f90:126-299): entries [e, isector, vec, itwin]; a twin
+    entry follows its state, carries no vector and leaves with it."""
+
+    def __init__(self):
+        self.s = []
+
+    def insert(self, e, isec, v, twin_sec=None):
+        i = 0
+        while i < len(self.s) and not (e <= self.s[i][0]):
+            i += 1
+        self.s.insert(i, [e, isec, v, False])
+        if twin_sec is not None:
+            self.s.insert(i + 1, [e, twin_sec, None, True])
+
+    def pop(self):
+        tw = self.s[-1][3]
+        self.s.pop()
+        if tw and self.s:
+            self.s.pop()
+
+    def add(self, e, isec, v, twin_sec=None, size=None):
+        if size is None or len(self.s) < size:
+            self.insert(e, isec, v, twin_sec)
+        elif e < self.s[-1][0]:
+            self.pop()
+            self.insert(e, isec, v, twin_sec)
+
+
+def _materialize(ns, secs, lst):
+    """(e, nup, ndw, vector) of every entry; twin entries get their vector
+    from the state before them."""
+    out = []
+    for i, (e, isec, v, tw) in enumerate(lst.s):
+        a, b = secs[isec - 1]
+        if tw:
+            pa, pb = secs[lst.s[i - 1][1] - 1]
+            v = twin_vector(ns, pa, pb, lst.s[i - 1][2])
+        out.append((e, a, b, v))
+    return out
+
+
 def solve_finite_t(model, lmats=256, lreal=0, wini=-5.0, wfin=5.0, eps=0.01, ngfiter=200,
-                   nstates_sector=6, nstates_total=16, nstates_step=2, cutoff=1e-9, nthreads=1):
+                   nstates_sector=6, nstates_total=16, nstates_step=2, cutoff=1e-9, nthreads=1,
+                   twin=False):
     """Finite-temperature solve over every sector: ed_diag_c (ED_DIAG.f90:93-228,
     finite-T branch with es_add_state's size cap, ED_EIGENSPACE.f90:126-151),
     ed_analysis (ED_DIAG.f90:248-398: Z before trimming, Neigen adaptation,
     cutoff trimming), observables with Boltzmann weights and the GF chains of
-    every kept state (build_gf_normal.f90:71-180,442-488)."""
+    every kept state (build_gf_normal.f90:71-180,442-488).  twin: ed_twin
+    (sectors with nup < ndw skipped, twin entries for nup != ndw,
+    ED_SETUP.f90:429-438, ED_DIAG.f90:111-123)."""
     ns = model.ns
     if nstates_total != 1:
         nstates_sector += nstates_sector % 2
@@ -610,26 +669,19 @@ def solve_finite_t(model, lmats=256, lreal=0, wini=-5.0, wfin=5.0, eps=0.01, ngf
     secs = [(a, b) for a in range(ns + 1) for b in range(ns + 1)]
     from math import comb
     neigen = [min(comb(ns, a) * comb(ns, b), nstates_sector) for a, b in secs]
-    states = []  # [e, isector(1-based), psi]
-
-    def insert(e, isec, v):
-        i = 0
-        while i < len(states) and not (e <= states[i][0]):
-            i += 1
-        states.insert(i, [e, isec, v])
+    lst = _StateList()
 
     for isec0, (a, b) in enumerate(secs):
+        if twin and a < b:
+            continue
+        tsec = b * (ns + 1) + a + 1 if (twin and a != b) else None
         hm = build_sector(ns, a, b)
         k = min(hm.size, neigen[isec0])
         w, V = _sector_eigs(model, hm, k)
         for i in range(k):
-            e = float(w[i])
-            if len(states) < nstates_total:
-                insert(e, isec0 + 1, V[:, i])
-            elif e < states[-1][0]:
-                states.pop()
-                insert(e, isec0 + 1, V[:, i])
-    egs = states[0][0]
+            lst.add(float(w[i]), isec0 + 1, V[:, i], tsec, nstates_total)
+    states = lst.s
+    egs = min(s[0] for s in states)
     zeta = sum(np.exp(-model.beta * (s[0] - egs)) for s in states)
     count = np.zeros(len(secs), int)
     for s in states:
@@ -644,10 +696,10 @@ def solve_finite_t(model, lmats=256, lreal=0, wini=-5.0, wfin=5.0, eps=0.01, ngf
         new_total = nstates_total + nstates_step
     else:
         while len(states) > 1 and np.exp(-model.beta * (states[-1][0] - egs)) <= cutoff:
-            states.pop()
+            lst.pop()
         new_total = max(len(states), nstates_step) + nstates_step
-    st4 = [(e, secs[isec - 1][0], secs[isec - 1][1], psi) for e, isec, psi in states]
+    st4 = _materialize(ns, secs, lst)
     obs, gm, gr, sm, chains, wm = _gf_and_obs(model, st4, egs, zeta, True, lmats, lreal, wini,
                                               wfin, eps, ngfiter, nthreads)
-    return dict(states=[(s[0], s[1]) for s in states], egs=egs, zeta=zeta, obs=obs, gmats=gm,
+    return dict(states=[(s[0], s[1]) for s in lst.s], egs=egs, zeta=zeta, obs=obs, gmats=gm,
                 greal=gr, smats=sm, neigen=new_neigen, nstates_total=new_total)

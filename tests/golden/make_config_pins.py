@@ -17,11 +17,12 @@ solver with the CPU restatement of the reference at the full sizes.
         (e ~ U[-1.5,1.5], V = 0.4 + U[-0.1,0.1]): every one of the 121
         sectors diagonalised, lanc_nstates_total=16, Neigen=6 per sector,
         the Boltzmann-weighted observables and G(iwn) on Lmats=4096.
+  cfg4t the cfg4 solve with ed_twin on.
 
 The oracle is the restatement in oracle/ (test infrastructure); every number
 here is what it computes.  Run once on a CPU host:
 
-    python tests/golden/make_config_pins.py [cfg2] [cfg3] [cfg4]
+    python tests/golden/make_config_pins.py [cfg2] [cfg3] [cfg4] [cfg4t]
 
 (cfg3 takes tens of minutes on 8 cores; the others a minute or two).  An
 existing npz is updated in place for the configurations named.
@@ -108,8 +109,21 @@ def main(which):
         out["cfg4_gmats"] = r["gmats"]
         print(f"cfg4: {len(r['states'])} states, Z={r['zeta']:.12f} ({time.time() - t0:.0f} s)",
               flush=True)
+    if "cfg4t" in which:
+        # the same solve with ed_twin (twin entries for the nup != ndw sectors)
+        t0 = time.time()
+        r = O.solve_finite_t(cfg4_model(), lmats=LMATS, nstates_total=16, nthreads=nthreads,
+                             twin=True)
+        out["cfg4t_e"] = np.array([s[0] for s in r["states"]])
+        out["cfg4t_sector"] = np.array([s[1] for s in r["states"]], np.int32)
+        out["cfg4t_zeta"] = np.array(r["zeta"])
+        for k in ("dens", "dens_up", "dens_dw", "docc", "magz"):
+            out["cfg4t_" + k] = r["obs"][k]
+        out["cfg4t_gmats"] = r["gmats"]
+        print(f"cfg4t: {len(r['states'])} states, Z={r['zeta']:.12f} ({time.time() - t0:.0f} s)",
+              flush=True)
     np.savez_compressed(OUT, **out)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["cfg2", "cfg4", "cfg3"])
+    main(sys.argv[1:] or ["cfg2", "cfg4", "cfg4t", "cfg3"])
