@@ -265,6 +265,66 @@ def differentiation_workload(dmfted, device, steps, warmup, solver64, isec, bath
         chi2_host=(a, wm, delta, w, dc.cpu().numpy(), dgr.cpu().numpy().reshape(nbatch, n2)))
 
 
+def dmft_workload(dmfted, device, steps, warmup):
+    """The self-consistency around the solve.  (a) The bath-fit minimiser on
+    4096 start points at once (the chi^2 workload's target and parameter sets,
+    delta scheme, cg_weight as 1/wn there, one CTA per fit).  (b) Whole
+    iterations of the Bethe-lattice DMFT loop at the small configuration (Ns=8,
+    Nbath=7, U=2, beta=100, Lmats=4096, T=0 with every sector scanned as
+    ed_solve does, Weiss-field fit on Lfit=1000 points, 500-point semicircle):
+    solve, Sigma, G_loc, Weiss field, fit and mixing, all on the device."""
+    from dmfted import bethe
+    a, wm, delta, w = chi2_inputs()
+    p = dmfted.default_params(nbath=9, beta=100.0, lmats=1000, lreal=0, device=device)
+    with dmfted.EDSolver(p) as s:
+        s.cg_fit_batch(a[:64], wm, delta, w, scheme=dmfted.CG_DELTA)  # warm-up
+        t0 = time.perf_counter()
+        am, c2, it = s.cg_fit_batch(a, wm, delta, w, scheme=dmfted.CG_DELTA)
+        fit_s = time.perf_counter() - t0
+    fits = dict(nbatch=a.shape[0], nbath=a.shape[1] // 2, lfit=wm.size, seconds=fit_s,
+                fits_per_s=a.shape[0] / fit_s, mean_iterations=float(np.mean(it)),
+                max_iterations=int(np.max(it)), median_chi2=float(np.median(c2)),
+                timing="wall clock around the synchronous call (host copies included)")
+    p = dmfted.default_params(norb=1, nbath=7, uloc=[2.0], beta=100.0, lmats=LMATS, lreal=0,
+                              device=device)
+    rng = np.random.default_rng(SEED)
+    bath = np.concatenate([rng.uniform(-1.0, 1.0, 7), 0.5 + rng.uniform(-0.1, 0.1, 7)])
+    he, wt = bethe.bethe_dos(500, 1.0)
+    ms = []
+    with dmfted.EDSolver(p) as s:
+        prev = None
+        for i in range(warmup + steps):
+            t0 = time.perf_counter()
+            new, weiss, chi2 = bethe.dmft_step(s, bath, he, wt)
+            bath = new if prev is None else 0.5 * new + 0.5 * prev
+            prev = bath.copy()
+            if i >= warmup:
+                ms.append((time.perf_counter() - t0) * 1e3)
+    loop = dict(workload="Bethe DMFT iteration, Ns=8 (Nbath=7, U=2, beta=100), every sector "
+                         "at T=0, Lmats=4096, Weiss fit on Lfit=1000",
+                ms_per_iteration=statistics.median(ms), iterations_timed=len(ms),
+                last_chi2=float(chi2[0][0]),
+                timing="wall clock of the public calls (host arrays in and out)")
+    return dict(fit_batch=fits, bethe_iteration=loop,
+                fit_host=(a[:8].copy(), wm, delta, w, am[:8].copy(), c2[:8].copy()))
+
+
+def fit_cpu(host):
+    """The oracle's conjugate-gradient fit (one thread) on the first start
+    points of the batch: fits per second and the largest chi^2 difference."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    a, wm, delta, w, am, c2 = host
+    t0 = time.perf_counter()
+    err = 0.0
+    for b in range(a.shape[0]):
+        ar, fr, _, _ = O.cg_fit(a[b], wm, delta, w, weiss=False)
+        err = max(err, abs(c2[b] - fr) / fr)
+    sec = time.perf_counter() - t0
+    return dict(fits_per_s=a.shape[0] / sec, cores=1, kind="port", sample=f"{a.shape[0]} fits",
+                max_rel_chi2_diff_gpu_vs_oracle=err)
+
+
 def make_solver(dmfted, precision, device):
     # LANC_NSTATES_SECTOR = 1: the workload is the sector's ground state (the
     # reference then asks sp_eigh for one eigenpair and keeps one state per
@@ -355,6 +415,7 @@ def run_ours(args, rank, world, local_rank):
         extra["finite_t_batched"] = finite_t_workload(dmfted, local_rank, args.steps, args.warmup)
         extra["differentiation"] = differentiation_workload(
             dmfted, local_rank, args.steps, args.warmup, solvers[dmfted.FP64], isec, bath)
+        extra["self_consistency"] = dmft_workload(dmfted, local_rank, args.steps, args.warmup)
     for sv in solvers.values():
         sv.close()
     return res, dim, hv32, hv64, extra
@@ -508,7 +569,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", default="all",
-                    choices=["all", "headline", "finite_t", "differentiation"],
+                    choices=["all", "headline", "finite_t", "differentiation",
+                             "self_consistency"],
                     help="run one workload (profiling); the default prints the full line")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -530,12 +592,15 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     import dmfted
-    if args.only in ("finite_t", "differentiation"):
+    if args.only in ("finite_t", "differentiation", "self_consistency"):
         # one secondary workload alone, for profiling; rank 0 prints it
         import torch
         torch.cuda.set_device(local_rank)
         if args.only == "finite_t":
             out = finite_t_workload(dmfted, local_rank, args.steps, args.warmup)
+        elif args.only == "self_consistency":
+            out = dmft_workload(dmfted, local_rank, args.steps, args.warmup)
+            out.pop("fit_host")
         else:
             s64 = make_solver(dmfted, dmfted.FP64, local_rank)
             out = differentiation_workload(dmfted, local_rank, args.steps, args.warmup, s64,
@@ -619,9 +684,10 @@ def main():
         gpu_launches=int(mixed["launches"]),
         clocks=mixed["clocks"],
     )
-    chi2_host = None
+    chi2_host = fit_host = None
     if extra:
         chi2_host = extra["differentiation"].pop("chi2_host")
+        fit_host = extra["self_consistency"].pop("fit_host")
         line.update(extra)
     if not args.no_cpu_baseline and world == 1:
         hv_per_step, nl = reference_hv_per_step()
@@ -635,6 +701,8 @@ def main():
                    f"pass, 2 x {NGF} chain steps); {t_hv:.2f} s per H*v")
         if chi2_host is not None:
             line["differentiation"]["chi2"]["cpu_baseline"] = chi2_cpu(chi2_host)
+        if fit_host is not None:
+            line["self_consistency"]["fit_batch"]["cpu_baseline"] = fit_cpu(fit_host)
     print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -518,6 +518,11 @@ void dmfted_default_params(dmfted_params *p) {
     p->lanc_ncheck = 10;
     p->device = 0;
     p->lanc_gf_threshold = 1e-13;
+    p->cg_niter = 500;
+    p->cg_scheme = DMFTED_CG_WEISS;
+    p->cg_ftol = 1e-5;
+    p->cg_stop = 0;
+    p->cg_eps = 1e-6;
 }
 
 const char *dmfted_last_error(void) { return last_error(); }
@@ -1064,6 +1069,189 @@ int dmfted_chi2_delta_batch(dmfted_ctx *c, int32_t nbatch, int32_t nbath, int32_
     chi2_batch_device(c, nbatch, nbath, L, da, dx, dg, dw, dc, grad ? dgr : nullptr);
     DM_CUDA(cudaMemcpyAsync(chi2, dc, nbatch * 8, cudaMemcpyDeviceToHost, c->stream));
     if (grad) DM_CUDA(cudaMemcpyAsync(grad, dgr, na * 8, cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    API_END
+}
+
+// ---- the self-consistency around the solve (fit.cu) -------------------------
+
+// Wdelta of chi2_fitgf_normal_normal (ED_CHI2FIT/fitgf_normal_normal.f90:44-53):
+// cg_weight 0 -> Ldelta, 1 -> 1, 2 -> n, 3 -> Xdelta(n).
+static std::vector<double> fit_weights(int cg_weight, const std::vector<double> &xd) {
+    const int L = (int)xd.size();
+    std::vector<double> w(L);
+    for (int n = 0; n < L; n++) {
+        switch (cg_weight) {
+            case 1: w[n] = 1.0; break;
+            case 2: w[n] = (double)(n + 1); break;
+            case 3: w[n] = xd[n]; break;
+            default: w[n] = (double)L; break;
+        }
+    }
+    return w;
+}
+
+static void check_cg_params(const dmfted_ctx *c, int scheme) {
+    DM_REQUIRE(scheme == DMFTED_CG_DELTA || scheme == DMFTED_CG_WEISS, DMFTED_ERR_ARG,
+               "chi2_fitgf_normal_normal error: cg_scheme != [weiss,delta]");
+    DM_REQUIRE(c->p.cg_niter >= 1, DMFTED_ERR_ARG, "cg fit: cg_niter < 1");
+    DM_REQUIRE(c->p.cg_stop >= 0 && c->p.cg_stop <= 2, DMFTED_ERR_ARG, "cg fit: cg_stop not in 0..2");
+}
+
+int dmfted_chi2_fitgf(dmfted_ctx *c, const double *fg, int32_t ispin, double *bath, int32_t nb,
+                      int32_t *iter, double *chi2) {
+    API_BEGIN
+    DM_REQUIRE(c && fg && bath, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(ispin >= 1 && ispin <= c->nspin, DMFTED_ERR_ARG, "chi2_fitgf: ispin out of range");
+    DM_REQUIRE(nb == 2 * c->nspin * c->norb * c->nbath, DMFTED_ERR_ARG,
+               "chi2_fitgf_normal_normal error: wrong bath dimensions");
+    DM_REQUIRE(c->nbath >= 1, DMFTED_ERR_ARG, "chi2_fitgf: no bath levels to fit");
+    check_cg_params(c, c->p.cg_scheme);
+    DM_CUDA(cudaSetDevice(c->device));
+    const int ns = c->nspin, no = c->norb, nbth = c->nbath, is = ispin - 1;
+    const int L = std::min(c->p.lfit, c->p.lmats);
+    DM_REQUIRE(L >= 1, DMFTED_ERR_ARG, "chi2_fitgf: Lfit < 1");
+    std::vector<double> xd(L);
+    for (int n = 0; n < L; n++) xd[n] = M_PI / c->p.beta * (2.0 * (n + 1) - 1.0);
+    const std::vector<double> w = fit_weights(c->p.cg_weight, xd);
+    // one fit per orbital: target fg(is,is,a,a,1:L), parameters of (is, a)
+    std::vector<double> a((size_t)no * 2 * nbth), g((size_t)no * 2 * L), zc(no);
+    const int64_t half = (int64_t)ns * no * nbth;
+    for (int o = 0; o < no; o++) {
+        for (int k = 0; k < nbth; k++) {
+            const int64_t io = k + (int64_t)o * nbth + (int64_t)is * nbth * no;
+            a[(size_t)o * 2 * nbth + k] = bath[io];
+            a[(size_t)o * 2 * nbth + nbth + k] = bath[half + io];
+        }
+        for (int n = 0; n < L; n++) {
+            const int64_t idx = is + ns * (is + ns * (o + (int64_t)no * (o + (int64_t)no * n)));
+            g[((size_t)o * L + n) * 2] = fg[2 * idx];
+            g[((size_t)o * L + n) * 2 + 1] = fg[2 * idx + 1];
+        }
+        const int64_t h = is + ns * (is + ns * (o + (int64_t)no * o));
+        zc[o] = c->p.xmu - c->hloc[2 * h];
+    }
+    DBuf<double> buf;
+    const size_t na = a.size();
+    buf.alloc(na + g.size() + 2 * (size_t)L + no + no);
+    double *da = buf.p, *dg = da + na, *dx = dg + g.size(), *dw = dx + L, *dz = dw + L,
+           *dc = dz + no;
+    DBuf<int> ibuf;
+    ibuf.alloc(2 * (size_t)no);
+    DM_CUDA(cudaMemcpyAsync(da, a.data(), na * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dg, g.data(), g.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dx, xd.data(), (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dw, w.data(), (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dz, zc.data(), (size_t)no * 8, cudaMemcpyHostToDevice, c->stream));
+    cg_fit_device(c, no, nbth, L, da, dx, dg, no, dw, dz, c->p.cg_scheme == DMFTED_CG_WEISS,
+                  c->p.cg_niter, c->p.cg_stop, c->p.cg_ftol, c->p.cg_eps, ibuf.p, dc, ibuf.p + no);
+    std::vector<double> c2(no);
+    std::vector<int> it(2 * (size_t)no);
+    DM_CUDA(cudaMemcpyAsync(a.data(), da, na * 8, cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaMemcpyAsync(c2.data(), dc, (size_t)no * 8, cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaMemcpyAsync(it.data(), ibuf.p, 2 * (size_t)no * sizeof(int), cudaMemcpyDeviceToHost,
+                            c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    for (int o = 0; o < no; o++) {
+        for (int k = 0; k < nbth; k++) {
+            const int64_t io = k + (int64_t)o * nbth + (int64_t)is * nbth * no;
+            bath[io] = a[(size_t)o * 2 * nbth + k];
+            bath[half + io] = a[(size_t)o * 2 * nbth + nbth + k];
+        }
+        if (iter) iter[o] = it[o];
+        if (chi2) chi2[o] = c2[o];
+    }
+    API_END
+}
+
+int dmfted_cg_fit_batch_device(dmfted_ctx *c, int32_t nbatch, int32_t nbath, int32_t L,
+                               double *d_a, const double *d_xdelta, const double *d_g,
+                               const double *d_w, int32_t scheme, double zc, int32_t *d_iter,
+                               double *d_chi2, int32_t *d_status) {
+    API_BEGIN
+    DM_REQUIRE(c && d_a && d_xdelta && d_g && d_w && d_iter && d_chi2 && d_status, DMFTED_ERR_ARG,
+               "null argument");
+    check_cg_params(c, scheme);
+    DM_CUDA(cudaSetDevice(c->device));
+    DBuf<double> z;
+    z.alloc(1);
+    DM_CUDA(cudaMemcpyAsync(z.p, &zc, 8, cudaMemcpyHostToDevice, c->stream));
+    cg_fit_device(c, nbatch, nbath, L, d_a, d_xdelta, d_g, 1, d_w, z.p,
+                  scheme == DMFTED_CG_WEISS, c->p.cg_niter, c->p.cg_stop, c->p.cg_ftol,
+                  c->p.cg_eps, d_iter, d_chi2, d_status);
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    API_END
+}
+
+int dmfted_cg_fit_batch(dmfted_ctx *c, int32_t nbatch, int32_t nbath, int32_t L, double *a,
+                        const double *xdelta, const double *g, const double *w, int32_t scheme,
+                        double zc, int32_t *iter, double *chi2) {
+    API_BEGIN
+    DM_REQUIRE(c && a && xdelta && g && w, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(nbatch > 0 && nbath > 0 && L > 0, DMFTED_ERR_ARG, "cg fit: empty batch or grid");
+    check_cg_params(c, scheme);
+    DM_CUDA(cudaSetDevice(c->device));
+    const size_t na = (size_t)nbatch * 2 * nbath;
+    DBuf<double> buf;
+    buf.alloc(na + 4 * (size_t)L + 1 + nbatch);
+    double *da = buf.p, *dx = da + na, *dg = dx + L, *dw = dg + 2 * (size_t)L, *dz = dw + L,
+           *dc = dz + 1;
+    DBuf<int> ibuf;
+    ibuf.alloc(2 * (size_t)nbatch);
+    DM_CUDA(cudaMemcpyAsync(da, a, na * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dx, xdelta, (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dg, g, 2 * (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dw, w, (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dz, &zc, 8, cudaMemcpyHostToDevice, c->stream));
+    cg_fit_device(c, nbatch, nbath, L, da, dx, dg, 1, dw, dz, scheme == DMFTED_CG_WEISS,
+                  c->p.cg_niter, c->p.cg_stop, c->p.cg_ftol, c->p.cg_eps, ibuf.p, dc,
+                  ibuf.p + nbatch);
+    std::vector<int> it(2 * (size_t)nbatch);
+    DM_CUDA(cudaMemcpyAsync(a, da, na * 8, cudaMemcpyDeviceToHost, c->stream));
+    if (chi2) DM_CUDA(cudaMemcpyAsync(chi2, dc, (size_t)nbatch * 8, cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaMemcpyAsync(it.data(), ibuf.p, it.size() * sizeof(int), cudaMemcpyDeviceToHost,
+                            c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    if (iter) std::copy(it.begin(), it.begin() + nbatch, iter);
+    API_END
+}
+
+int dmfted_gloc_matsubara_diag(dmfted_ctx *c, int32_t le, const double *he, const double *wt,
+                               const double *sigma, double *gloc) {
+    API_BEGIN
+    DM_REQUIRE(c && he && wt && sigma && gloc, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(le >= 1, DMFTED_ERR_ARG, "gloc: empty density-of-states grid");
+    DM_CUDA(cudaSetDevice(c->device));
+    const int L = c->p.lmats, no = c->norb, ns = c->nspin;
+    const size_t ng = (size_t)ns * ns * no * no * L * 2;
+    DBuf<double> buf;
+    buf.alloc((size_t)no * le + le + 2 * ng);
+    double *dh = buf.p, *dwt = dh + (size_t)no * le, *ds = dwt + le, *dgl = ds + ng;
+    DM_CUDA(cudaMemcpyAsync(dh, he, (size_t)no * le * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(dwt, wt, (size_t)le * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(ds, sigma, ng * 8, cudaMemcpyHostToDevice, c->stream));
+    gloc_diag_device(c, L, le, dh, dwt, c->d_wm.p, ds, dgl);
+    DM_CUDA(cudaMemcpyAsync(gloc, dgl, ng * 8, cudaMemcpyDeviceToHost, c->stream));
+    DM_CUDA(cudaStreamSynchronize(c->stream));
+    API_END
+}
+
+int dmfted_get_weiss(dmfted_ctx *c, const double *gloc, const double *sigma, int32_t scheme,
+                     double *out) {
+    API_BEGIN
+    DM_REQUIRE(c && gloc && sigma && out, DMFTED_ERR_ARG, "null argument");
+    DM_REQUIRE(scheme == DMFTED_CG_DELTA || scheme == DMFTED_CG_WEISS, DMFTED_ERR_ARG,
+               "get_weiss: scheme != [weiss,delta]");
+    DM_CUDA(cudaSetDevice(c->device));
+    const int L = c->p.lmats, no = c->norb, ns = c->nspin;
+    const size_t ng = (size_t)ns * ns * no * no * L * 2;
+    DBuf<double> buf;
+    buf.alloc(3 * ng);
+    double *dgl = buf.p, *ds = dgl + ng, *dout = ds + ng;
+    DM_CUDA(cudaMemcpyAsync(dgl, gloc, ng * 8, cudaMemcpyHostToDevice, c->stream));
+    DM_CUDA(cudaMemcpyAsync(ds, sigma, ng * 8, cudaMemcpyHostToDevice, c->stream));
+    weiss_diag_device(c, L, scheme, c->d_hloc_aa.p, c->d_wm.p, dgl, ds, dout);
+    DM_CUDA(cudaMemcpyAsync(out, dout, ng * 8, cudaMemcpyDeviceToHost, c->stream));
     DM_CUDA(cudaStreamSynchronize(c->stream));
     API_END
 }

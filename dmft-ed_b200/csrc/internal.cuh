@@ -473,6 +473,16 @@ void chi2_batch_device(dmfted_ctx *c, int nbatch, int nbath, int L, const double
                        const double *x, const double *g, const double *w, double *chi2,
                        double *grad);
 
+// ---- fit.cu ----------------------------------------------------------------
+void cg_fit_device(dmfted_ctx *c, int nbatch, int nbath, int L, double *a, const double *x,
+                   const double *g, int ng, const double *w, const double *zc, int weiss,
+                   int itmax, int istop, double ftol, double eps, int *iter, double *chi2,
+                   int *status);
+void gloc_diag_device(dmfted_ctx *c, int L, int le, const double *he, const double *wt,
+                      const double *wm, const double *sig, double *gl);
+void weiss_diag_device(dmfted_ctx *c, int L, int scheme, const double *hloc_aa, const double *wm,
+                       const double *gl, const double *sig, double *out);
+
 // ---- small helpers ------------------------------------------------------------
 inline int div_up(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 int num_sms(dmfted_ctx *c);

@@ -25,6 +25,8 @@ OK = 0
 ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_UNSUPPORTED, ERR_STATE, ERR_NOTCONV, ERR_NORM = range(1, 8)
 FP64 = 0
 MIXED = 1
+CG_DELTA = 0  # cg_scheme: fit the hybridisation Delta(iw_n)
+CG_WEISS = 1  # cg_scheme: fit the Weiss field G0(iw_n) (the reference default)
 
 
 class DmftedError(RuntimeError):
@@ -53,6 +55,8 @@ class Params(C.Structure):
         ("ed_twin", C.c_int32), ("lfit", C.c_int32), ("cg_weight", C.c_int32),
         ("precision", C.c_int32), ("lanc_ncheck", C.c_int32), ("device", C.c_int32),
         ("lanc_gf_threshold", C.c_double),
+        ("cg_niter", C.c_int32), ("cg_scheme", C.c_int32), ("cg_ftol", C.c_double),
+        ("cg_stop", C.c_int32), ("cg_eps", C.c_double),
     ]
 
 
@@ -100,6 +104,13 @@ EXPORTS = {
                                           _dp, _dp, _dp]),
     "dmfted_chi2_delta_batch_device": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, _vp,
                                                  _vp, _vp, _vp, _vp]),
+    "dmfted_chi2_fitgf": (C.c_int, [_vp, _dp, C.c_int32, _dp, C.c_int32, _ip, _dp]),
+    "dmfted_cg_fit_batch": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp,
+                                      C.c_int32, C.c_double, _ip, _dp]),
+    "dmfted_cg_fit_batch_device": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, _vp, _vp,
+                                             _vp, C.c_int32, C.c_double, _vp, _vp, _vp]),
+    "dmfted_gloc_matsubara_diag": (C.c_int, [_vp, C.c_int32, _dp, _dp, _dp, _dp]),
+    "dmfted_get_weiss": (C.c_int, [_vp, _dp, _dp, C.c_int32, _dp]),
     "dmfted_time_hxv": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp]),
     "dmfted_hxv_timing": (C.c_int, [_vp, C.c_int32]),
     "dmfted_autotune_log": (C.c_int, [_vp, C.c_char_p, C.c_int32, C.POINTER(C.c_int32)]),
@@ -412,6 +423,63 @@ class EDSolver:
                                           _p(xdelta), _p(g.view(np.float64)), _p(w), _p(chi2),
                                           _p(gr)))
         return (chi2, gr) if grad else chi2
+
+    # ---- the self-consistency around the solve ----------------------------
+    def ed_chi2_fitgf(self, fg, bath, ispin=1):
+        """ed_chi2_fitgf (ED_CHI2FIT.f90:86-138), normal bath: the conjugate-gradient
+        fit of every orbital's levels and hybridisations of spin ispin to
+        fg(ispin,ispin,a,a,:), on the device.  Returns (new bath, iterations[Norb],
+        chi2[Norb]); the input bath array is not modified."""
+        p = self.params
+        fg = np.asarray(fg, np.complex128)
+        assert fg.shape[:4] == (p.nspin, p.nspin, p.norb, p.norb), fg.shape
+        flat = np.ascontiguousarray(fg.reshape(-1, order="F"))
+        b = np.array(bath, np.float64, copy=True)
+        it = np.zeros(p.norb, np.int32)
+        c2 = np.zeros(p.norb)
+        _ck(lib().dmfted_chi2_fitgf(self.ctx, _p(flat.view(np.float64)), int(ispin), _p(b), b.size,
+                                    _p(it, C.c_int32), _p(c2)))
+        return b, it, c2
+
+    def cg_fit_batch(self, a, xdelta, g, w, scheme=None, zc=0.0):
+        """The bath-fit minimiser on a batch of start points (one CTA each), all
+        fitting the target g.  Returns (minima, chi2, iterations)."""
+        a = np.array(np.atleast_2d(a), np.float64, copy=True, order="C")
+        nbatch, n2 = a.shape
+        xdelta = np.ascontiguousarray(xdelta, np.float64)
+        g = _c128(g)
+        w = np.ascontiguousarray(w, np.float64)
+        sch = self.params.cg_scheme if scheme is None else scheme
+        it = np.zeros(nbatch, np.int32)
+        c2 = np.zeros(nbatch)
+        _ck(lib().dmfted_cg_fit_batch(self.ctx, nbatch, n2 // 2, xdelta.size, _p(a), _p(xdelta),
+                                      _p(g.view(np.float64)), _p(w), int(sch), float(zc),
+                                      _p(it, C.c_int32), _p(c2)))
+        return a, c2, it
+
+    def gloc_matsubara_diag(self, he, wt, sigma):
+        """dmft_gloc_matsubara for a lattice Hamiltonian diagonal in spin and
+        orbital: he[Norb, Le] (or [Le] for every orbital), wt[Le], sigma as
+        ed_get_sigma_matsubara returns it."""
+        p = self.params
+        wt = np.ascontiguousarray(wt, np.float64)
+        he = np.ascontiguousarray(np.broadcast_to(np.asarray(he, np.float64), (p.norb, wt.size)))
+        sig = np.ascontiguousarray(np.asarray(sigma, np.complex128).reshape(-1, order="F"))
+        out = np.zeros(sig.size, np.complex128)
+        _ck(lib().dmfted_gloc_matsubara_diag(self.ctx, wt.size, _p(he), _p(wt),
+                                             _p(sig.view(np.float64)), _p(out.view(np.float64))))
+        return out.reshape((p.nspin, p.nspin, p.norb, p.norb, p.lmats), order="F")
+
+    def get_weiss(self, gloc, sigma, scheme=None):
+        """dmft_weiss (scheme CG_WEISS) or dmft_delta (CG_DELTA) on the diagonal."""
+        p = self.params
+        sch = p.cg_scheme if scheme is None else scheme
+        gl = np.ascontiguousarray(np.asarray(gloc, np.complex128).reshape(-1, order="F"))
+        sig = np.ascontiguousarray(np.asarray(sigma, np.complex128).reshape(-1, order="F"))
+        out = np.zeros(gl.size, np.complex128)
+        _ck(lib().dmfted_get_weiss(self.ctx, _p(gl.view(np.float64)), _p(sig.view(np.float64)),
+                                   int(sch), _p(out.view(np.float64))))
+        return out.reshape((p.nspin, p.nspin, p.norb, p.norb, p.lmats), order="F")
 
     def timings(self):
         t = np.zeros(4)

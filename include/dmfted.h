@@ -79,7 +79,18 @@ typedef struct dmfted_params {
     int32_t lanc_ncheck;          /* Ritz-value check interval (10)         */
     int32_t device;               /* CUDA device ordinal (0)                */
     double lanc_gf_threshold;     /* |b| that ends a GF chain (1e-13)       */
+    /* the bath fit (ED_INPUT_VARS.f90:158-164) */
+    int32_t cg_niter;             /* CG_NITER (500)                :158     */
+    int32_t cg_scheme;            /* CG_SCHEME: DMFTED_CG_WEISS (default) or
+                                     DMFTED_CG_DELTA               :159     */
+    double cg_ftol;               /* CG_FTOL (1e-5)                :160     */
+    int32_t cg_stop;              /* CG_STOP (0)                   :162     */
+    double cg_eps;                /* CG_EPS (1e-6)                 :163     */
 } dmfted_params;
+
+/* cg_scheme: what the bath fit matches (fitgf_normal_normal.f90:72-82) */
+#define DMFTED_CG_DELTA 0 /* the hybridisation Delta(iw_n)                  */
+#define DMFTED_CG_WEISS 1 /* the Weiss field G0(iw_n) = 1/(iw_n+xmu-Hloc-Delta) */
 
 typedef struct dmfted_ctx dmfted_ctx;
 
@@ -286,6 +297,57 @@ int dmfted_chi2_delta_batch(dmfted_ctx *ctx, int32_t nbatch, int32_t nbath, int3
 int dmfted_chi2_delta_batch_device(dmfted_ctx *ctx, int32_t nbatch, int32_t nbath, int32_t L,
                                    const double *d_a, const double *d_xdelta, const double *d_g,
                                    const double *d_w, double *d_chi2, double *d_grad);
+
+/* ---- the self-consistency around the solve --------------------------------
+ * ed_chi2_fitgf (ED_CHI2FIT.f90:86-138) for the normal bath: for every
+ * orbital a, the fit of the levels and hybridisations of spin ispin (1-based)
+ * to fg(ispin,ispin,a,a,1:Ldelta), Ldelta = min(lfit, lmats), by
+ * chi2_fitgf_normal_normal (ED_CHI2FIT/fitgf_normal_normal.f90:18-178): the
+ * chi^2 of cg_scheme (delta or weiss) with the cg_weight weights, minimised by
+ * the Polak-Ribiere conjugate gradient with Brent line searches (fmin_cg,
+ * cg_niter, cg_ftol, cg_stop, cg_eps).  All orbitals run at once, one CTA
+ * each.  fg: (Nspin,Nspin,Norb,Norb,Lmats) complex128, host; bath: the
+ * set_dmft_bath layout, updated in place for spin ispin; iter[Norb] and
+ * chi2[Norb] receive each fit's steps and final chi^2 (either may be NULL).
+ * The solver's own bath is not changed (the next ed_solve passes it). */
+int dmfted_chi2_fitgf(dmfted_ctx *ctx, const double *fg, int32_t ispin, double *bath,
+                      int32_t nb, int32_t *iter, double *chi2);
+
+/* The same minimiser on nbatch independent parameter sets at once (one CTA
+ * each), all fitting one target: a[nbatch*2*nbath] start values in, minima
+ * out ([e_1..e_Nbath, V_1..V_Nbath] per set); xdelta[L], g[L] complex128,
+ * w[L] as dmfted_chi2_delta_batch; scheme DMFTED_CG_DELTA or
+ * DMFTED_CG_WEISS with zc = xmu - Hloc_aa; the stopping controls are the
+ * context's cg_* parameters.  iter[nbatch], chi2[nbatch] (may be NULL).
+ * Host pointers. */
+int dmfted_cg_fit_batch(dmfted_ctx *ctx, int32_t nbatch, int32_t nbath, int32_t L, double *a,
+                        const double *xdelta, const double *g, const double *w, int32_t scheme,
+                        double zc, int32_t *iter, double *chi2);
+
+/* Same on device pointers, on the context's stream.  d_status[nbatch]:
+ * bit 0 a line search found no bracket, bit 1 a Brent search hit its step
+ * limit (the fit still returns its best point). */
+int dmfted_cg_fit_batch_device(dmfted_ctx *ctx, int32_t nbatch, int32_t nbath, int32_t L,
+                               double *d_a, const double *d_xdelta, const double *d_g,
+                               const double *d_w, int32_t scheme, double zc, int32_t *d_iter,
+                               double *d_chi2, int32_t *d_status);
+
+/* dmft_gloc_matsubara of DMFT_Tools (drivers/ed_hm_bethe.f90:70; the legacy
+ * in-tree .repo/ED_GLOC.f90:54-126,257-298) for a lattice Hamiltonian diagonal
+ * in spin and orbital, on a density-of-states grid of le points:
+ *   G_loc(s,s,a,a,iw_n) = sum_k wt[k] / (iw_n + xmu - Sigma(s,s,a,a,iw_n) - he[a*le+k])
+ * sigma, gloc: (Nspin,Nspin,Norb,Norb,Lmats) complex128, host (off-diagonal
+ * entries of gloc are zero).  For the Bethe lattice of half-bandwidth D:
+ * he = linspace(-D, D, le), wt = 2 sqrt(D^2 - he^2) / (pi D^2) * de. */
+int dmfted_gloc_matsubara_diag(dmfted_ctx *ctx, int32_t le, const double *he, const double *wt,
+                               const double *sigma, double *gloc);
+
+/* dmft_weiss / dmft_delta (drivers/ed_hm_bethe.f90:73-77; .repo/ED_WEISS.f90:
+ * 55-118) on the diagonal: scheme DMFTED_CG_WEISS gives 1/(1/G_loc + Sigma),
+ * DMFTED_CG_DELTA gives iw_n + xmu - Hloc_aa - Sigma - 1/G_loc.  Same array
+ * layout as dmfted_gloc_matsubara_diag; host pointers. */
+int dmfted_get_weiss(dmfted_ctx *ctx, const double *gloc, const double *sigma, int32_t scheme,
+                     double *out);
 
 /* ---- timing helpers (device time on the context's stream) ------------ */
 /* Average device milliseconds of one H*v on the current sector over reps

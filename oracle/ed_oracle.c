@@ -999,6 +999,272 @@ double or_chi2_delta(const double *a, int32_t nbath, const double *xdelta, const
     return chi2;
 }
 
+/* chi^2 of the bath fit for either scheme, chi2_delta_normal_normal and
+ * chi2_weiss_normal_normal (ED_CHI2FIT/fitgf_normal_normal.f90:193-202,
+ * 235-246) with g0and_normal_normal (:349-362): M_n = Delta_n (weiss = 0) or
+ * G0_n = 1/(i x_n + zc - Delta_n), zc = xmu - Hloc_aa (weiss = 1).  The
+ * gradient: the reference's grad_chi2_delta_normal_normal (:208-226) for the
+ * delta scheme; for the weiss scheme the same formula with dM = G0^2 dDelta
+ * (the reference differentiates this chi^2 numerically inside fmin_cg).
+ * Sums run over the frequencies in order. */
+double or_chi2_model(const double *a, int32_t nbath, const double *xdelta, const double *g_,
+                     const double *w, int32_t L, int32_t weiss, double zcv, double *grad) {
+    const zc *g = (const zc *)g_;
+    double chi2 = 0.0;
+    zc *m = (zc *)malloc(sizeof(zc) * L);
+    zc *g02 = (zc *)malloc(sizeof(zc) * L);
+    for (int i = 0; i < L; i++) {
+        zc d = 0.0;
+        for (int k = 0; k < nbath; k++) d += a[nbath + k] * a[nbath + k] / (I * xdelta[i] - a[k]);
+        if (weiss) {
+            zc g0 = 1.0 / (I * xdelta[i] + zcv - d);
+            m[i] = g0;
+            g02[i] = g0 * g0;
+        } else {
+            m[i] = d;
+            g02[i] = 1.0;
+        }
+    }
+    for (int i = 0; i < L; i++) {
+        double re = creal(g[i] - m[i]), im = cimag(g[i] - m[i]);
+        chi2 += (re * re + im * im) / w[i];
+    }
+    if (grad) {
+        for (int j = 0; j < 2 * nbath; j++) {
+            double s1 = 0.0, s2 = 0.0;
+            for (int i = 0; i < L; i++) {
+                zc dd;
+                if (j < nbath) {
+                    zc den = I * xdelta[i] - a[j];
+                    dd = a[nbath + j] * a[nbath + j] / (den * den);
+                } else {
+                    int k = j - nbath;
+                    dd = 2.0 * a[nbath + k] / (I * xdelta[i] - a[k]);
+                }
+                dd *= g02[i];
+                s1 += creal(g[i] - m[i]) * creal(dd) / w[i];
+                s2 += cimag(g[i] - m[i]) * cimag(dd) / w[i];
+            }
+            grad[j] = -2.0 * (s1 + s2);
+        }
+    }
+    free(m);
+    free(g02);
+    return chi2;
+}
+
+/* fmin_cg (SciFortran SF_OPTIMIZE, absent from the tree, version unpinned),
+ * called by chi2_fitgf_normal_normal (fitgf_normal_normal.f90:82-119), restated
+ * from the published algorithm it implements: the Polak-Ribiere conjugate
+ * gradient with line minimisation by bracketing and Brent's method with
+ * derivatives (Press et al., Numerical Recipes, 2nd ed., sections 10.1, 10.3,
+ * 10.6: frprmn, dlinmin, mnbrak, dbrent; the book's constants; line
+ * tolerance 1e-4).  Stopping test: cg_stop 0 the book's 2|fret - fp| <= ftol
+ * (|fret| + |fp| + eps); 1 |fret - fp| <= ftol; 2 fret <= ftol.
+ * a (2*nbath) in/out.  Returns the final chi^2; *iter the steps taken;
+ * *status bit 0 a bracket search failed, bit 1 a Brent search hit its limit. */
+typedef struct {
+    const double *p, *xi;
+    double *q, *gr;
+    int32_t na, nbath, L, weiss;
+    const double *xdelta, *g, *w;
+    double zc;
+} cg_line;
+
+static double cg_f1dim(const cg_line *c, double x) {
+    for (int j = 0; j < c->na; j++) c->q[j] = c->p[j] + x * c->xi[j];
+    return or_chi2_model(c->q, c->nbath, c->xdelta, c->g, c->w, c->L, c->weiss, c->zc, NULL);
+}
+
+static double cg_fdf1dim(const cg_line *c, double x, double *df) {
+    for (int j = 0; j < c->na; j++) c->q[j] = c->p[j] + x * c->xi[j];
+    double f = or_chi2_model(c->q, c->nbath, c->xdelta, c->g, c->w, c->L, c->weiss, c->zc, c->gr);
+    double d = 0.0;
+    for (int j = 0; j < c->na; j++) d += c->gr[j] * c->xi[j];
+    *df = d;
+    return f;
+}
+
+static int cg_mnbrak(const cg_line *c, double *ax, double *bx, double *cx, double *fa, double *fb,
+                     double *fc) {
+    const double GOLD = 1.618034, GLIMIT = 100.0, TINY = 1.0e-20;
+    double t;
+    *fa = cg_f1dim(c, *ax);
+    *fb = cg_f1dim(c, *bx);
+    if (*fb > *fa) {
+        t = *ax; *ax = *bx; *bx = t;
+        t = *fa; *fa = *fb; *fb = t;
+    }
+    *cx = *bx + GOLD * (*bx - *ax);
+    *fc = cg_f1dim(c, *cx);
+    for (int it = 0; *fb >= *fc; it++) {
+        if (it >= 200) return 0;
+        double r = (*bx - *ax) * (*fb - *fc);
+        double q = (*bx - *cx) * (*fb - *fa);
+        double u = *bx - ((*bx - *cx) * q - (*bx - *ax) * r) /
+                             (2.0 * copysign(fmax(fabs(q - r), TINY), q - r));
+        double ulim = *bx + GLIMIT * (*cx - *bx);
+        double fu;
+        if ((*bx - u) * (u - *cx) > 0.0) {
+            fu = cg_f1dim(c, u);
+            if (fu < *fc) {
+                *ax = *bx; *bx = u;
+                *fa = *fb; *fb = fu;
+                return 1;
+            } else if (fu > *fb) {
+                *cx = u;
+                *fc = fu;
+                return 1;
+            }
+            u = *cx + GOLD * (*cx - *bx);
+            fu = cg_f1dim(c, u);
+        } else if ((*cx - u) * (u - ulim) > 0.0) {
+            fu = cg_f1dim(c, u);
+            if (fu < *fc) {
+                *bx = *cx; *cx = u; u = *cx + GOLD * (*cx - *bx);
+                *fb = *fc; *fc = fu; fu = cg_f1dim(c, u);
+            }
+        } else if ((u - ulim) * (ulim - *cx) >= 0.0) {
+            u = ulim;
+            fu = cg_f1dim(c, u);
+        } else {
+            u = *cx + GOLD * (*cx - *bx);
+            fu = cg_f1dim(c, u);
+        }
+        *ax = *bx; *bx = *cx; *cx = u;
+        *fa = *fb; *fb = *fc; *fc = fu;
+    }
+    return 1;
+}
+
+static double cg_dbrent(const cg_line *c, double ax, double bx, double cx, double tol,
+                        double *xmin, int32_t *status) {
+    const int ITMAX = 100;
+    const double ZEPS = 1.0e-10;
+    double a = fmin(ax, cx), b = fmax(ax, cx);
+    double d = 0.0, e = 0.0;
+    double x = bx, w = bx, v = bx;
+    double dx, fx = cg_fdf1dim(c, x, &dx);
+    double fw = fx, fv = fx, dw = dx, dv = dx;
+    for (int iter = 0; iter < ITMAX; iter++) {
+        double xm = 0.5 * (a + b);
+        double tol1 = tol * fabs(x) + ZEPS, tol2 = 2.0 * tol1;
+        if (fabs(x - xm) <= (tol2 - 0.5 * (b - a))) {
+            *xmin = x;
+            return fx;
+        }
+        int bisect = 1;
+        if (fabs(e) > tol1) {
+            double d1 = 2.0 * (b - a), d2 = d1;
+            if (dw != dx) d1 = (w - x) * dx / (dx - dw);
+            if (dv != dx) d2 = (v - x) * dx / (dx - dv);
+            double u1 = x + d1, u2 = x + d2;
+            int ok1 = (a - u1) * (u1 - b) > 0.0 && dx * d1 <= 0.0;
+            int ok2 = (a - u2) * (u2 - b) > 0.0 && dx * d2 <= 0.0;
+            double olde = e;
+            e = d;
+            if (ok1 || ok2) {
+                if (ok1 && ok2) d = fabs(d1) < fabs(d2) ? d1 : d2;
+                else d = ok1 ? d1 : d2;
+                if (fabs(d) <= fabs(0.5 * olde)) {
+                    double u = x + d;
+                    if (u - a < tol2 || b - u < tol2) d = copysign(tol1, xm - x);
+                    bisect = 0;
+                }
+            }
+        }
+        if (bisect) {
+            e = dx >= 0.0 ? a - x : b - x;
+            d = 0.5 * e;
+        }
+        double u, fu, du;
+        if (fabs(d) >= tol1) {
+            u = x + d;
+            fu = cg_fdf1dim(c, u, &du);
+        } else {
+            u = x + copysign(tol1, d);
+            fu = cg_fdf1dim(c, u, &du);
+            if (fu > fx) {
+                *xmin = x;
+                return fx;
+            }
+        }
+        if (fu <= fx) {
+            if (u >= x) a = x;
+            else b = x;
+            v = w; fv = fw; dv = dw;
+            w = x; fw = fx; dw = dx;
+            x = u; fx = fu; dx = du;
+        } else {
+            if (u < x) a = u;
+            else b = u;
+            if (fu <= fw || w == x) {
+                v = w; fv = fw; dv = dw;
+                w = u; fw = fu; dw = du;
+            } else if (fu <= fv || v == x || v == w) {
+                v = u; fv = fu; dv = du;
+            }
+        }
+    }
+    *status |= 2;
+    *xmin = x;
+    return fx;
+}
+
+double or_cg_fit(double *a, int32_t nbath, const double *xdelta, const double *g, const double *w,
+                 int32_t L, int32_t weiss, double zcv, int32_t itmax, double ftol, double eps,
+                 int32_t istop, int32_t *iter, int32_t *status) {
+    const int na = 2 * nbath;
+    double *xi = (double *)malloc(sizeof(double) * na), *gv = (double *)malloc(sizeof(double) * na);
+    double *h = (double *)malloc(sizeof(double) * na), *q = (double *)malloc(sizeof(double) * na);
+    double *gr = (double *)malloc(sizeof(double) * na);
+    cg_line c = {a, xi, q, gr, na, nbath, L, weiss, xdelta, g, w, zcv};
+    *status = 0;
+    *iter = 0;
+    double fp = or_chi2_model(a, nbath, xdelta, g, w, L, weiss, zcv, xi);
+    for (int j = 0; j < na; j++) {
+        gv[j] = -xi[j];
+        h[j] = gv[j];
+        xi[j] = h[j];
+    }
+    double fret = fp;
+    for (int its = 1; its <= itmax; its++) {
+        *iter = its;
+        double ax = 0.0, xx = 1.0, bx, fa, fx, fb, xmin = 0.0;
+        if (!cg_mnbrak(&c, &ax, &xx, &bx, &fa, &fx, &fb)) *status |= 1;
+        fret = cg_dbrent(&c, ax, xx, bx, 1.0e-4, &xmin, status);
+        for (int j = 0; j < na; j++) {
+            xi[j] *= xmin;
+            a[j] += xi[j];
+        }
+        int done;
+        if (istop == 1) done = fabs(fret - fp) <= ftol;
+        else if (istop == 2) done = fret <= ftol;
+        else done = 2.0 * fabs(fret - fp) <= ftol * (fabs(fret) + fabs(fp) + eps);
+        if (done) break;
+        fp = fret;
+        or_chi2_model(a, nbath, xdelta, g, w, L, weiss, zcv, xi);
+        double gg = 0.0, dgg = 0.0;
+        for (int j = 0; j < na; j++) {
+            gg += gv[j] * gv[j];
+            dgg += (xi[j] + gv[j]) * xi[j];
+        }
+        if (gg == 0.0) break;
+        double gam = dgg / gg;
+        for (int j = 0; j < na; j++) {
+            gv[j] = -xi[j];
+            h[j] = gv[j] + gam * h[j];
+            xi[j] = h[j];
+        }
+    }
+    free(xi);
+    free(gv);
+    free(h);
+    free(q);
+    free(gr);
+    return fret;
+}
+
 int32_t or_host_threads(void) {
     long n = sysconf(_SC_NPROCESSORS_ONLN);
     return n > 0 ? (int32_t)n : 1;

@@ -100,6 +100,12 @@ def _declare(L):
     L.or_chi2_delta.restype = C.c_double
     L.or_chi2_delta.argtypes = [_dp, C.c_int32, _dp, _dp, _dp, C.c_int32, _dp]
     L.or_host_threads.restype = C.c_int32
+    L.or_chi2_model.restype = C.c_double
+    L.or_chi2_model.argtypes = [_dp, C.c_int32, _dp, _dp, _dp, C.c_int32, C.c_int32, C.c_double,
+                                _dp]
+    L.or_cg_fit.restype = C.c_double
+    L.or_cg_fit.argtypes = [_dp, C.c_int32, _dp, _dp, _dp, C.c_int32, C.c_int32, C.c_double,
+                            C.c_int32, C.c_double, C.c_double, C.c_int32, _ip, _ip]
 
 
 def _p(a, ct=C.c_double):
@@ -400,6 +406,65 @@ def chi2_delta(a, xdelta, g, w, grad=True):
     c2 = lib().or_chi2_delta(_p(a), a.size // 2, _p(xdelta), _p(g.view(np.float64)), _p(w),
                              xdelta.size, _p(gr) if grad else None)
     return (c2, gr) if grad else c2
+
+
+def chi2_model(a, xdelta, g, w, weiss=False, zc=0.0, grad=True):
+    """chi2 of the delta (chi2_delta_normal_normal) or weiss
+    (chi2_weiss_normal_normal with g0and_normal_normal) fit and its gradient,
+    ED_CHI2FIT/fitgf_normal_normal.f90:193-246,349-362; zc = xmu - Hloc_aa."""
+    a = np.ascontiguousarray(a, np.float64)
+    xdelta = np.ascontiguousarray(xdelta, np.float64)
+    g = np.ascontiguousarray(g, np.complex128)
+    w = np.ascontiguousarray(w, np.float64)
+    gr = np.zeros(a.size) if grad else None
+    c2 = lib().or_chi2_model(_p(a), a.size // 2, _p(xdelta), _p(g.view(np.float64)), _p(w),
+                             xdelta.size, int(weiss), float(zc), _p(gr) if grad else None)
+    return (c2, gr) if grad else c2
+
+
+def cg_fit(a, xdelta, g, w, weiss=False, zc=0.0, itmax=500, ftol=1e-5, eps=1e-6, istop=0):
+    """fmin_cg as chi2_fitgf_normal_normal calls it (fitgf_normal_normal.f90:82-119),
+    restated from the published Polak-Ribiere / Brent algorithm (oracle/ed_oracle.c
+    or_cg_fit).  Returns (parameters at the minimum, chi2, iterations, status)."""
+    a = np.ascontiguousarray(a, np.float64).copy()
+    xdelta = np.ascontiguousarray(xdelta, np.float64)
+    g = np.ascontiguousarray(g, np.complex128)
+    w = np.ascontiguousarray(w, np.float64)
+    it = C.c_int32()
+    st = C.c_int32()
+    f = lib().or_cg_fit(_p(a), a.size // 2, _p(xdelta), _p(g.view(np.float64)), _p(w),
+                        xdelta.size, int(weiss), float(zc), int(itmax), float(ftol), float(eps),
+                        int(istop), C.byref(it), C.byref(st))
+    return a, f, it.value, st.value
+
+
+def bethe_dos(le=500, wband=1.0):
+    """The Bethe-lattice density-of-states grid of drivers/ed_hm_bethe.f90:38-40:
+    He = linspace(-D, D, Le, mesh=de), Wte = dens_bethe(He, D) * de with the
+    semicircle dens_bethe(x, D) = 2 sqrt(D^2 - x^2) / (pi D^2) (SciFortran)."""
+    he = np.linspace(-wband, wband, le)
+    de = he[1] - he[0]
+    wt = 2.0 * np.sqrt(np.maximum(wband ** 2 - he ** 2, 0.0)) / (np.pi * wband ** 2) * de
+    return he, wt
+
+
+def gloc_diag(he, wt, wm, xmu, sigma):
+    """G_loc(iw_n) = sum_k wt_k / (i w_n + xmu - Sigma(iw_n) - he_k), k in order
+    (.repo/ED_GLOC.f90:54-126,257-298 for a 1x1 block; dmft_gloc_matsubara)."""
+    z = 1j * np.asarray(wm) + xmu - np.asarray(sigma)
+    g = np.zeros_like(z)
+    for k in range(len(he)):
+        g = g + (1.0 / (z - he[k])) * wt[k]
+    return g
+
+
+def weiss_diag(gloc, sigma, wm, xmu, hloc_aa, weiss=True):
+    """dmft_weiss / dmft_delta for a 1x1 block (.repo/ED_WEISS.f90:55-118):
+    1/(1/G + Sigma), or i w_n + xmu - Hloc - Sigma - 1/G."""
+    ig = 1.0 / np.asarray(gloc)
+    if weiss:
+        return 1.0 / (ig + sigma)
+    return 1j * np.asarray(wm) + xmu - hloc_aa - sigma - ig
 
 
 def cg_weights(cg_weight, xdelta):

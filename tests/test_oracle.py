@@ -237,3 +237,68 @@ def test_t0_single_sector_matches_sector_solve():
     assert a["zeta"] == 1.0
     assert abs(a["e0"] - b["e0"]) < 1e-10 * abs(b["e0"])
     assert np.abs(a["gmats"] - b["gmats"]).max() < 1e-8
+
+
+# ---- the self-consistency around the solve: fit, local G, Weiss field -------
+def _fit_problem(seed=5, nbath=9, L=1000, beta=100.0, noise=1e-4):
+    rng = np.random.default_rng(seed)
+    wm = O.matsubara(beta, L)
+    e = rng.uniform(-1.0, 1.0, nbath)
+    v = 0.5 + rng.uniform(-0.1, 0.1, nbath)
+    z = noise * (rng.normal(size=L) + 1j * rng.normal(size=L))
+    return rng, wm, e, v, z
+
+
+def test_weiss_chi2_gradient_finite_difference():
+    rng, wm, e, v, z = _fit_problem()
+    g = 1.0 / (1j * wm + 0.1 - O.delta_bath(e, v, 1j * wm)) + z
+    w = O.cg_weights(3, wm)
+    x = np.concatenate([e, v]) * (1 + 0.05 * rng.normal(size=e.size * 2))
+    c, gr = O.chi2_model(x, wm, g, w, weiss=True, zc=0.1)
+    h = 1e-6
+    fd = np.array([(O.chi2_model(x + h * d, wm, g, w, True, 0.1, False) -
+                    O.chi2_model(x - h * d, wm, g, w, True, 0.1, False)) / (2 * h)
+                   for d in np.eye(x.size)])
+    assert np.abs(fd - gr).max() <= 1e-6 * np.abs(gr).max()
+    # the delta scheme is the reference's grad_chi2_delta_normal_normal
+    c2, g2 = O.chi2_model(x, wm, g, w, weiss=False)
+    c3, g3 = O.chi2_delta(x, wm, g, w)
+    assert abs(c2 - c3) <= 1e-14 * c3 and np.abs(g2 - g3).max() <= 1e-14 * np.abs(g3).max()
+
+
+@pytest.mark.parametrize("weiss", [False, True])
+def test_cg_fit_reaches_the_minimum(weiss):
+    """The restated fmin_cg (Polak-Ribiere, Brent line searches) from a start
+    near the answer ends at the minimum an independent quasi-Newton search
+    finds (cg_weight 0, the reference default)."""
+    from scipy.optimize import minimize
+    rng, wm, e, v, z = _fit_problem()
+    d = O.delta_bath(e, v, 1j * wm)
+    g = (1.0 / (1j * wm - d) if weiss else d) + z
+    w = O.cg_weights(0, wm)
+    a0 = np.concatenate([e, v]) * (1 + 0.05 * rng.normal(size=2 * e.size))
+    a, f, it, st = O.cg_fit(a0, wm, g, w, weiss=weiss, zc=0.0)
+    assert st == 0 and it < 500
+    assert abs(f - O.chi2_model(a, wm, g, w, weiss, 0.0, False)) <= 1e-14 * f
+    r = minimize(lambda x: O.chi2_model(x, wm, g, w, weiss, 0.0)[0], a0,
+                 jac=lambda x: O.chi2_model(x, wm, g, w, weiss, 0.0)[1], method="BFGS",
+                 options=dict(gtol=1e-14, maxiter=50000))
+    # fmin_cg stops on the relative change of chi2 (cg_ftol = 1e-5): its value
+    # lies within a small factor of the true minimum, far below the start
+    assert r.fun <= f <= 2.0 * r.fun + 1e-12
+    assert f < 1e-2 * O.chi2_model(a0, wm, g, w, weiss, 0.0, False)
+
+
+def test_bethe_gloc_and_delta_self_consistency():
+    """On the semicircular grid the local G of Sigma = 0 obeys the Bethe
+    relation Delta = (D/2)^2 G_loc (to the grid's discretisation error), and
+    the Weiss and Delta routes agree: 1/G0 = i w + xmu - Delta."""
+    he, wt = O.bethe_dos(4000, 1.0)
+    wm = O.matsubara(100.0, 256)
+    sig = np.zeros(wm.size, np.complex128)
+    g = O.gloc_diag(he, wt, wm, 0.0, sig)
+    d = O.weiss_diag(g, sig, wm, 0.0, 0.0, weiss=False)
+    assert np.abs(d - 0.25 * g).max() < 2e-3
+    g0 = O.weiss_diag(g, sig, wm, 0.0, 0.0, weiss=True)
+    assert np.abs(1.0 / g0 - (1j * wm - d)).max() < 1e-12
+    assert abs(wt.sum() - 1.0) < 1e-3
