@@ -12,7 +12,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libdmfted.so")
 SOURCES = ["api.cu", "fock.cu", "hxv.cu", "lanczos.cu", "gf.cu", "observables.cu", "chi2.cu",
-           "batch.cu", "noalloc.cu", "dense.cu", "diag.cu", "fit.cu"]
+           "batch.cu", "noalloc.cu", "dense.cu", "diag.cu", "fit.cu",
+           "restart.cu"]
 HEADERS = ["internal.cuh", "reduce.cuh", "hxv.cuh", "tridiag.cuh", "sector.cuh", "jterms.cuh"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -111,6 +111,10 @@ EXPORTS = {
                                              _vp, C.c_int32, C.c_double, _vp, _vp, _vp]),
     "dmfted_gloc_matsubara_diag": (C.c_int, [_vp, C.c_int32, _dp, _dp, _dp, _dp]),
     "dmfted_get_weiss": (C.c_int, [_vp, _dp, _dp, C.c_int32, _dp]),
+    "dmfted_save_bath": (C.c_int, [C.c_void_p, C.c_char_p, _dp, C.c_int32]),
+    "dmfted_read_bath": (C.c_int, [C.c_void_p, C.c_char_p, _dp, C.c_int32]),
+    "dmfted_print_state_list": (C.c_int, [_vp, C.c_char_p]),
+    "dmfted_read_state_list": (C.c_int, [_vp, C.c_char_p]),
     "dmfted_time_hxv": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp]),
     "dmfted_hxv_timing": (C.c_int, [_vp, C.c_int32]),
     "dmfted_autotune_log": (C.c_int, [_vp, C.c_char_p, C.c_int32, C.POINTER(C.c_int32)]),
@@ -171,6 +175,21 @@ def get_bath_dimension(params):
     nb = C.c_int32()
     _ck(lib().dmfted_get_bath_dimension(C.byref(params), C.byref(nb)))
     return nb.value
+
+
+def save_bath(params, path, bath):
+    """save_dmft_bath: the bath array to a hamiltonian.restart-format file."""
+    b = np.ascontiguousarray(bath, np.float64)
+    _ck(lib().dmfted_save_bath(C.byref(params), os.fsencode(path), _p(b), b.size))
+
+
+def read_bath(params, path, bath=None):
+    """The bath read of init_dmft_bath (min(lines, Nbath) rows after the
+    header) into a copy of bath (zeros when bath is None).  Returns the array."""
+    nb = get_bath_dimension(params)
+    b = np.zeros(nb) if bath is None else np.array(bath, np.float64, copy=True)
+    _ck(lib().dmfted_read_bath(C.byref(params), os.fsencode(path), _p(b), nb))
+    return b
 
 
 def _c128(a):
@@ -423,6 +442,15 @@ class EDSolver:
                                           _p(xdelta), _p(g.view(np.float64)), _p(w), _p(chi2),
                                           _p(gr)))
         return (chi2, gr) if grad else chi2
+
+    # ---- restart files ----------------------------------------------------
+    def print_state_list(self, path):
+        """print_state_list: the last solve's eigenspace in state_list.ed format."""
+        _ck(lib().dmfted_print_state_list(self.ctx, os.fsencode(path)))
+
+    def read_state_list(self, path):
+        """state_list.restart: the per-sector state counts for the next solve."""
+        _ck(lib().dmfted_read_state_list(self.ctx, os.fsencode(path)))
 
     # ---- the self-consistency around the solve ----------------------------
     def ed_chi2_fitgf(self, fg, bath, ispin=1):

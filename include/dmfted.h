@@ -349,6 +349,32 @@ int dmfted_gloc_matsubara_diag(dmfted_ctx *ctx, int32_t le, const double *he, co
 int dmfted_get_weiss(dmfted_ctx *ctx, const double *gloc, const double *sigma, int32_t scheme,
                      double *out);
 
+/* ---- files that let a run resume across the boundary (text formats) ---------
+ * save_dmft_bath (ED_BATH/dmft_aux.f90:408-428 with write_dmft_bath :310-336,
+ * normal bath): the bath array written as hamiltonian.restart / .used are,
+ * a header of "(90(A21,1X))" labels then Nbath rows of "(90(F21.12,1X))"
+ * values ((e(s,a,k), v(s,a,k), a=1..Norb), s=1..Nspin).  No device needed. */
+int dmfted_save_bath(const dmfted_params *p, const char *path, const double *bath, int32_t nb);
+
+/* The bath read of init_dmft_bath (ED_BATH/dmft_aux.f90:158-180): the header
+ * skipped, then min(lines, Nbath) rows read list-directed into bath (the
+ * set_dmft_bath layout).  The line count includes the header, so a file with
+ * fewer than Nbath rows runs the read past its end: an error, as in the
+ * reference.  No device needed. */
+int dmfted_read_bath(const dmfted_params *p, const char *path, double *bath, int32_t nb);
+
+/* print_state_list (ED_DIAG.f90:258-264,401-445): the eigenspace of the last
+ * solve in the state_list.ed format, one "(i3,f18.12,2x,ES19.12,1x,2i3,3x,i3,
+ * i10)" row per state (i, E_i, exp(-beta(E_i-E_min)), nup, ndw, sector, dim). */
+int dmfted_print_state_list(dmfted_ctx *ctx, const char *path);
+
+/* The state_list.restart read of setup_pointers_normal (ED_SETUP.f90:403-425):
+ * lanc_nstates_total = the file's line count, neigen_sector(s) = max(1, states
+ * listed in sector s), each row's nup/ndw checked against its sector (the
+ * reference's stop message otherwise).  Call after dmfted_init, before the
+ * first solve. */
+int dmfted_read_state_list(dmfted_ctx *ctx, const char *path);
+
 /* ---- timing helpers (device time on the context's stream) ------------ */
 /* Average device milliseconds of one H*v on the current sector over reps
  * launches after warmup launches.  flags: bit 0 = float32 vectors (else

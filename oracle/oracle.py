@@ -467,6 +467,47 @@ def weiss_diag(gloc, sigma, wm, xmu, hloc_aa, weiss=True):
     return 1j * np.asarray(wm) + xmu - hloc_aa - sigma - ig
 
 
+# ------------------------------------------------------- restart files ---
+def _fortran_es(x, w, d):
+    """ESw.d output: d.ddd...E+dd, or d.ddd...+ddd for a three-digit exponent."""
+    m, e = f"{x:.{d}E}".split("E")
+    ev = int(e)
+    s = f"{m}E{'+' if ev >= 0 else '-'}{abs(ev):02d}" if abs(ev) < 100 else \
+        f"{m}{'+' if ev >= 0 else '-'}{abs(ev):03d}"
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
+def write_dmft_bath_text(bath, norb, nspin, nbath):
+    """write_dmft_bath, normal bath (ED_BATH/dmft_aux.f90:310-336): the header
+    "(90(A21,1X))" and Nbath rows "(90(F21.12,1X))" of ((e, v), orbitals), spins."""
+    half = len(bath) // 2
+    head = ""
+    for s in range(nspin):
+        for a in range(norb):
+            tag = f"l{a + 1}_s{s + 1}"
+            head += f"#Ek_{tag}".rjust(21) + " " + f"Vk_{tag}".rjust(21) + " "
+    rows = [head]
+    for k in range(nbath):
+        r = ""
+        for s in range(nspin):
+            for a in range(norb):
+                io = k + a * nbath + s * nbath * norb
+                r += f"{bath[io]:21.12f} {bath[half + io]:21.12f} "
+        rows.append(r)
+    return "\n".join(rows) + "\n"
+
+
+def print_state_list_text(energies, sectors, getnup, getndw, getdim, beta):
+    """print_state_list (ED_DIAG.f90:401-445), normal mode: header, then rows
+    "(i3,f18.12,2x,ES19.12,1x,2i3,3x,i3,i10)" with exp(-beta (E - E_min))."""
+    emin = min(energies)
+    out = ["# i       E_i           exp(-(E-E0)/T)       nup ndw  Sect     Dim"]
+    for i, (e, isec) in enumerate(zip(energies, sectors)):
+        out.append(f"{i + 1:3d}{e:18.12f}  {_fortran_es(np.exp(-beta * (e - emin)), 19, 12)} "
+                   f"{getnup[isec - 1]:3d}{getndw[isec - 1]:3d}   {isec:3d}{getdim[isec - 1]:10d}")
+    return "\n".join(out) + "\n"
+
+
 def cg_weights(cg_weight, xdelta):
     """Wdelta of chi2_fitgf_normal_normal, fitgf_normal_normal.f90:44-53."""
     L = xdelta.size
