@@ -1216,13 +1216,14 @@ int dmfted_cg_fit_batch(dmfted_ctx *c, int32_t nbatch, int32_t nbath, int32_t L,
     API_END
 }
 
-int dmfted_gloc_matsubara_diag(dmfted_ctx *c, int32_t le, const double *he, const double *wt,
-                               const double *sigma, double *gloc) {
-    API_BEGIN
+static void gloc_diag_host(dmfted_ctx *c, int32_t le, const double *he, const double *wt,
+                           const double *sigma, double *gloc, bool real_axis) {
     DM_REQUIRE(c && he && wt && sigma && gloc, DMFTED_ERR_ARG, "null argument");
     DM_REQUIRE(le >= 1, DMFTED_ERR_ARG, "gloc: empty density-of-states grid");
     DM_CUDA(cudaSetDevice(c->device));
-    const int L = c->p.lmats, no = c->norb, ns = c->nspin;
+    const int L = real_axis ? c->p.lreal : c->p.lmats, no = c->norb, ns = c->nspin;
+    DM_REQUIRE(L >= 1, DMFTED_ERR_ARG, "gloc: empty frequency grid");
+    DM_REQUIRE(!real_axis || c->p.eps > 0.0, DMFTED_ERR_ARG, "gloc: real axis needs eps > 0");
     const size_t ng = (size_t)ns * ns * no * no * L * 2;
     DBuf<double> buf;
     buf.alloc((size_t)no * le + le + 2 * ng);
@@ -1230,9 +1231,23 @@ int dmfted_gloc_matsubara_diag(dmfted_ctx *c, int32_t le, const double *he, cons
     DM_CUDA(cudaMemcpyAsync(dh, he, (size_t)no * le * 8, cudaMemcpyHostToDevice, c->stream));
     DM_CUDA(cudaMemcpyAsync(dwt, wt, (size_t)le * 8, cudaMemcpyHostToDevice, c->stream));
     DM_CUDA(cudaMemcpyAsync(ds, sigma, ng * 8, cudaMemcpyHostToDevice, c->stream));
-    gloc_diag_device(c, L, le, dh, dwt, c->d_wm.p, ds, dgl);
+    gloc_diag_device(c, L, le, dh, dwt, real_axis ? c->d_wr.p : c->d_wm.p,
+                     real_axis ? c->p.eps : 0.0, ds, dgl);
     DM_CUDA(cudaMemcpyAsync(gloc, dgl, ng * 8, cudaMemcpyDeviceToHost, c->stream));
     DM_CUDA(cudaStreamSynchronize(c->stream));
+}
+
+int dmfted_gloc_matsubara_diag(dmfted_ctx *c, int32_t le, const double *he, const double *wt,
+                               const double *sigma, double *gloc) {
+    API_BEGIN
+    gloc_diag_host(c, le, he, wt, sigma, gloc, false);
+    API_END
+}
+
+int dmfted_gloc_realaxis_diag(dmfted_ctx *c, int32_t le, const double *he, const double *wt,
+                              const double *sigma, double *gloc) {
+    API_BEGIN
+    gloc_diag_host(c, le, he, wt, sigma, gloc, true);
     API_END
 }
 

@@ -454,18 +454,22 @@ __host__ __device__ inline int64_t gf5(int nspin, int norb, int s, int a, int n)
     return (int64_t)s + nspin * ((int64_t)s + nspin * ((int64_t)a + norb * ((int64_t)a + norb * n)));
 }
 
-// G_loc(s,s,a,a,n) = sum_k wt[k] / (i w_n + xmu - Sigma(s,s,a,a,n) - he[a*le + k]),
-// k in increasing order (the reference adds the k-point terms in turn).
+// G_loc(s,s,a,a,n) = sum_k wt[k] / (z_n + xmu - Sigma(s,s,a,a,n) - he[a*le + k]),
+// z_n = i w_n (Matsubara) or w_n + i eps (real axis, eps > 0); k in increasing
+// order (the reference adds the k-point terms in turn).
 __global__ void k_gloc_diag(int nspin, int norb, int L, int le, const double *__restrict__ he,
                             const double *__restrict__ wt, const double *__restrict__ wm,
-                            double xmu, const double2 *__restrict__ sig, double2 *__restrict__ gl) {
+                            double xmu, double eps, const double2 *__restrict__ sig,
+                            double2 *__restrict__ gl) {
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= (int64_t)nspin * norb * L) return;
     const int n = (int)(t % L);
     const int sa = (int)(t / L), s = sa % nspin, a = sa / nspin;
     const int64_t o = gf5(nspin, norb, s, a, n);
     const double2 sg = sig[o];
-    const double zr = xmu - sg.x, zi = wm[n] - sg.y;
+    const bool real_axis = eps > 0.0;
+    const double zr = xmu - sg.x + (real_axis ? wm[n] : 0.0);
+    const double zi = (real_axis ? eps : wm[n]) - sg.y;
     double gr = 0.0, gi = 0.0;
     for (int k = 0; k < le; k++) {
         const double dr = zr - he[(int64_t)a * le + k];
@@ -500,12 +504,12 @@ __global__ void k_weiss_diag(int nspin, int norb, int L, int scheme, double xmu,
 }
 
 void gloc_diag_device(dmfted_ctx *c, int L, int le, const double *he, const double *wt,
-                      const double *wm, const double *sig, double *gl) {
+                      const double *wm, double eps, const double *sig, double *gl) {
     const int ns = c->nspin, no = c->norb;
     DM_CUDA(cudaMemsetAsync(gl, 0, (size_t)ns * ns * no * no * L * 16, c->stream));
     const int64_t n = (int64_t)ns * no * L;
     k_gloc_diag<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
-        ns, no, L, le, he, wt, wm, c->p.xmu, reinterpret_cast<const double2 *>(sig),
+        ns, no, L, le, he, wt, wm, c->p.xmu, eps, reinterpret_cast<const double2 *>(sig),
         reinterpret_cast<double2 *>(gl));
     DM_CHECK_LAUNCH();
     c->launches++;

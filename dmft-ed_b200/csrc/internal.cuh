@@ -479,7 +479,7 @@ void cg_fit_device(dmfted_ctx *c, int nbatch, int nbath, int L, double *a, const
                    int itmax, int istop, double ftol, double eps, int *iter, double *chi2,
                    int *status);
 void gloc_diag_device(dmfted_ctx *c, int L, int le, const double *he, const double *wt,
-                      const double *wm, const double *sig, double *gl);
+                      const double *wm, double eps, const double *sig, double *gl);
 void weiss_diag_device(dmfted_ctx *c, int L, int scheme, const double *hloc_aa, const double *wm,
                        const double *gl, const double *sig, double *out);
 

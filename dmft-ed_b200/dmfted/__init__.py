@@ -110,6 +110,7 @@ EXPORTS = {
     "dmfted_cg_fit_batch_device": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, _vp, _vp,
                                              _vp, C.c_int32, C.c_double, _vp, _vp, _vp]),
     "dmfted_gloc_matsubara_diag": (C.c_int, [_vp, C.c_int32, _dp, _dp, _dp, _dp]),
+    "dmfted_gloc_realaxis_diag": (C.c_int, [_vp, C.c_int32, _dp, _dp, _dp, _dp]),
     "dmfted_get_weiss": (C.c_int, [_vp, _dp, _dp, C.c_int32, _dp]),
     "dmfted_save_bath": (C.c_int, [C.c_void_p, C.c_char_p, _dp, C.c_int32]),
     "dmfted_read_bath": (C.c_int, [C.c_void_p, C.c_char_p, _dp, C.c_int32]),
@@ -485,18 +486,25 @@ class EDSolver:
                                       _p(it, C.c_int32), _p(c2)))
         return a, c2, it
 
-    def gloc_matsubara_diag(self, he, wt, sigma):
-        """dmft_gloc_matsubara for a lattice Hamiltonian diagonal in spin and
-        orbital: he[Norb, Le] (or [Le] for every orbital), wt[Le], sigma as
-        ed_get_sigma_matsubara returns it."""
+    def _gloc(self, fn, L, he, wt, sigma):
         p = self.params
         wt = np.ascontiguousarray(wt, np.float64)
         he = np.ascontiguousarray(np.broadcast_to(np.asarray(he, np.float64), (p.norb, wt.size)))
         sig = np.ascontiguousarray(np.asarray(sigma, np.complex128).reshape(-1, order="F"))
         out = np.zeros(sig.size, np.complex128)
-        _ck(lib().dmfted_gloc_matsubara_diag(self.ctx, wt.size, _p(he), _p(wt),
-                                             _p(sig.view(np.float64)), _p(out.view(np.float64))))
-        return out.reshape((p.nspin, p.nspin, p.norb, p.norb, p.lmats), order="F")
+        _ck(fn(self.ctx, wt.size, _p(he), _p(wt), _p(sig.view(np.float64)),
+               _p(out.view(np.float64))))
+        return out.reshape((p.nspin, p.nspin, p.norb, p.norb, L), order="F")
+
+    def gloc_matsubara_diag(self, he, wt, sigma):
+        """dmft_gloc_matsubara for a lattice Hamiltonian diagonal in spin and
+        orbital: he[Norb, Le] (or [Le] for every orbital), wt[Le], sigma as
+        ed_get_sigma_matsubara returns it."""
+        return self._gloc(lib().dmfted_gloc_matsubara_diag, self.params.lmats, he, wt, sigma)
+
+    def gloc_realaxis_diag(self, he, wt, sigma):
+        """dmft_gloc_realaxis on the same grid (w + i eps, the context's Lreal)."""
+        return self._gloc(lib().dmfted_gloc_realaxis_diag, self.params.lreal, he, wt, sigma)
 
     def get_weiss(self, gloc, sigma, scheme=None):
         """dmft_weiss (scheme CG_WEISS) or dmft_delta (CG_DELTA) on the diagonal."""

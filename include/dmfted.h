@@ -342,6 +342,12 @@ int dmfted_cg_fit_batch_device(dmfted_ctx *ctx, int32_t nbatch, int32_t nbath, i
 int dmfted_gloc_matsubara_diag(dmfted_ctx *ctx, int32_t le, const double *he, const double *wt,
                                const double *sigma, double *gloc);
 
+/* dmft_gloc_realaxis (drivers/ed_hm_bethe.f90:91) on the same grid: the sum
+ * with w + i eps in place of i w_n, over the Lreal points linspace(wini, wfin)
+ * of the context; sigma, gloc (Nspin,Nspin,Norb,Norb,Lreal) complex128. */
+int dmfted_gloc_realaxis_diag(dmfted_ctx *ctx, int32_t le, const double *he, const double *wt,
+                              const double *sigma, double *gloc);
+
 /* dmft_weiss / dmft_delta (drivers/ed_hm_bethe.f90:73-77; .repo/ED_WEISS.f90:
  * 55-118) on the diagonal: scheme DMFTED_CG_WEISS gives 1/(1/G_loc + Sigma),
  * DMFTED_CG_DELTA gives iw_n + xmu - Hloc_aa - Sigma - 1/G_loc.  Same array

@@ -376,6 +376,201 @@ void or_hxv_c128(const or_model *M, const int32_t *map, int64_t dim, const doubl
     for (int t = 0; t < nthreads; t++) pthread_join(th[t], NULL);
 }
 
+/* ------------------------------------------------------------------ */
+/* The "best CPU" variant of the baseline: the up/down-factored H*v that the
+ * device kernels use, restated on the CPU in FP64 (real: the normal-mode
+ * Hamiltonian with a real bath and Hloc is real).  It separates the gain of
+ * the factored algorithm from the gain of the hardware; it is not the
+ * reference's algorithm.  On the DimUp x DimDw matrix V (the H%map order):
+ *   (H V)[r,c] = D[r,c] V[r,c] + sum_{r'} Hup[r,r'] V[r',c] + sum_{c'} Hdw[c,c'] V[r,c'].
+ * Hup and Hdw are read off the oracle's own element emitter (row_elements):
+ * the off-diagonal elements of column 0 that keep the down word are Hup, the
+ * elements of row 0 that keep the up word are Hdw (a one-spin hop's sign
+ * depends on that spin's word only); D is the sum of the diagonal terms.
+ * Models with the Jhflag terms (which change both words) are not factored. */
+typedef struct {
+    int64_t dimup, dimdw, wu, wd; /* ELL widths */
+    int32_t *cu, *cd;             /* [dimup*wu], [dimdw*wd] target ranks, -1 = none */
+    double *vu, *vd;
+    double *diag;                 /* [dim] */
+} or_factored;
+
+typedef struct {
+    int64_t base, stride, self, count, cap;
+    int32_t *col;
+    double *val;
+    double dsum;
+    int modeup;
+    int64_t dimup;
+} fac_ctx;
+static void emit_fac(void *c, int64_t j, zc val) {
+    fac_ctx *f = (fac_ctx *)c;
+    if (j == 0) return;
+    int64_t t = j - 1;
+    if (t == f->self) {
+        f->dsum += creal(val);
+        return;
+    }
+    int64_t rank;
+    if (f->modeup) {
+        if (t >= f->dimup) return; /* changes the down word */
+        rank = t;
+    } else {
+        if (t % f->dimup != 0) return; /* changes the up word */
+        rank = t / f->dimup;
+    }
+    if (f->count < f->cap) {
+        f->col[f->count] = (int32_t)rank;
+        f->val[f->count] = creal(val);
+        f->count++;
+    }
+}
+
+/* Diagonal of every element: only the diagonal terms, emitted to a sum. */
+typedef struct {
+    const or_model *M;
+    const int32_t *map;
+    int64_t dim, r0, r1;
+    double *diag;
+} fac_diag_job;
+static void *fac_diag_worker(void *arg) {
+    fac_diag_job *J = (fac_diag_job *)arg;
+    or_model M1 = *J->M;
+    /* the diagonal alone: no hops can reach the row itself, so an emitter that
+       keeps only the self terms, with the hoppings switched off, is exact */
+    double zero_v[8 * 64] = {0};
+    M1.v = zero_v;
+    double hl[2 * 2 * 2 * 3 * 3];
+    int nh = 2 * M1.nspin * M1.nspin * M1.norb * M1.norb;
+    for (int q = 0; q < nh; q++) hl[q] = J->M->hloc[q];
+    for (int is = 0; is < M1.nspin; is++)
+        for (int js = 0; js < M1.nspin; js++)
+            for (int a = 0; a < M1.norb; a++)
+                for (int b = 0; b < M1.norb; b++)
+                    if (a != b || is != js) {
+                        long idx = is + M1.nspin * (js + M1.nspin * (a + (long)M1.norb * b));
+                        hl[2 * idx] = hl[2 * idx + 1] = 0.0;
+                    }
+    M1.hloc = hl;
+    M1.jhflag = 0;
+    for (int64_t i = J->r0; i < J->r1; i++) {
+        fac_ctx f = {0};
+        f.self = i;
+        f.dimup = 1;
+        row_elements(&M1, J->map, J->dim, i, emit_fac, &f);
+        J->diag[i] = f.dsum;
+    }
+    return NULL;
+}
+
+or_factored *or_factored_setup(const or_model *M, const int32_t *map, int64_t dimup,
+                               int64_t dimdw, int32_t nthreads) {
+    if (M->jhflag && M->norb > 1) return NULL;
+    if (M->norb * M->nbath > 64) return NULL;
+    const int64_t dim = dimup * dimdw;
+    or_factored *F = (or_factored *)calloc(1, sizeof(or_factored));
+    F->dimup = dimup;
+    F->dimdw = dimdw;
+    F->wu = F->wd = M->norb * (M->nbath + M->norb) + 1;
+    F->cu = (int32_t *)malloc(sizeof(int32_t) * dimup * F->wu);
+    F->vu = (double *)calloc((size_t)(dimup * F->wu), sizeof(double));
+    F->cd = (int32_t *)malloc(sizeof(int32_t) * dimdw * F->wd);
+    F->vd = (double *)calloc((size_t)(dimdw * F->wd), sizeof(double));
+    for (int64_t q = 0; q < dimup * F->wu; q++) F->cu[q] = -1;
+    for (int64_t q = 0; q < dimdw * F->wd; q++) F->cd[q] = -1;
+    for (int64_t r = 0; r < dimup; r++) {
+        fac_ctx f = {0};
+        f.self = r;
+        f.cap = F->wu;
+        f.col = F->cu + r * F->wu;
+        f.val = F->vu + r * F->wu;
+        f.modeup = 1;
+        f.dimup = dimup;
+        row_elements(M, map, dim, r, emit_fac, &f);
+    }
+    for (int64_t c = 0; c < dimdw; c++) {
+        fac_ctx f = {0};
+        f.self = c * dimup;
+        f.cap = F->wd;
+        f.col = F->cd + c * F->wd;
+        f.val = F->vd + c * F->wd;
+        f.modeup = 0;
+        f.dimup = dimup;
+        row_elements(M, map, dim, c * dimup, emit_fac, &f);
+    }
+    F->diag = (double *)malloc(sizeof(double) * dim);
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    fac_diag_job jobs[256];
+    int64_t chunk = (dim + nthreads - 1) / nthreads;
+    for (int t = 0; t < nthreads; t++) {
+        int64_t r0 = t * chunk < dim ? t * chunk : dim;
+        int64_t r1 = r0 + chunk < dim ? r0 + chunk : dim;
+        jobs[t] = (fac_diag_job){M, map, dim, r0, r1, F->diag};
+        pthread_create(&th[t], NULL, fac_diag_worker, &jobs[t]);
+    }
+    for (int t = 0; t < nthreads; t++) pthread_join(th[t], NULL);
+    return F;
+}
+
+void or_factored_free(or_factored *F) {
+    if (!F) return;
+    free(F->cu);
+    free(F->vu);
+    free(F->cd);
+    free(F->vd);
+    free(F->diag);
+    free(F);
+}
+
+typedef struct {
+    const or_factored *F;
+    const double *x;
+    double *y;
+    int64_t c0, c1;
+} fac_job;
+static void *fac_worker(void *arg) {
+    fac_job *J = (fac_job *)arg;
+    const or_factored *F = J->F;
+    const int64_t du = F->dimup;
+    for (int64_t c = J->c0; c < J->c1; c++) {
+        const double *xc = J->x + c * du;
+        double *yc = J->y + c * du;
+        for (int64_t r = 0; r < du; r++) yc[r] = F->diag[c * du + r] * xc[r];
+        for (int64_t r = 0; r < du; r++) {
+            double acc = 0.0;
+            const int32_t *cl = F->cu + r * F->wu;
+            const double *vl = F->vu + r * F->wu;
+            for (int64_t e = 0; e < F->wu && cl[e] >= 0; e++) acc += vl[e] * xc[cl[e]];
+            yc[r] += acc;
+        }
+        const int32_t *cl = F->cd + c * F->wd;
+        const double *vl = F->vd + c * F->wd;
+        for (int64_t e = 0; e < F->wd && cl[e] >= 0; e++) {
+            const double v = vl[e];
+            const double *xn = J->x + (int64_t)cl[e] * du;
+            for (int64_t r = 0; r < du; r++) yc[r] += v * xn[r];
+        }
+    }
+    return NULL;
+}
+
+void or_factored_hxv(const or_factored *F, const double *x, double *y, int32_t nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    fac_job jobs[256];
+    int64_t chunk = (F->dimdw + nthreads - 1) / nthreads;
+    for (int t = 0; t < nthreads; t++) {
+        int64_t c0 = t * chunk < F->dimdw ? t * chunk : F->dimdw;
+        int64_t c1 = c0 + chunk < F->dimdw ? c0 + chunk : F->dimdw;
+        jobs[t] = (fac_job){F, x, y, c0, c1};
+        pthread_create(&th[t], NULL, fac_worker, &jobs[t]);
+    }
+    for (int t = 0; t < nthreads; t++) pthread_join(th[t], NULL);
+}
+
 typedef struct {
     int64_t row;
     int64_t n, cap;
@@ -725,6 +920,7 @@ double or_gf_vvinit(int32_t particle, int32_t isite, const int32_t *map_i, int64
     const zc *psi = (const zc *)psi_;
     zc *vv = (zc *)vv_;
     for (int64_t j = 0; j < jdim; j++) vv[j] = 0.0;
+    if (isite < 1 || isite > 31) return -1.0; /* sites are 1-based levels of the word */
     for (int64_t m = 0; m < idim; m++) {
         int32_t i = map_i[m], r;
         double sgn;
@@ -736,6 +932,7 @@ double or_gf_vvinit(int32_t particle, int32_t isite, const int32_t *map_i, int64
             op_c(isite, i, &r, &sgn);
         }
         int64_t j = or_binary_search(map_j, jdim, r);
+        if (j < 1) return -1.0; /* target state outside sector j: wrong sector pair */
         vv[j - 1] = sgn * psi[m];
     }
     return creal(zdot(vv, vv, jdim));

@@ -100,6 +100,10 @@ def _declare(L):
     L.or_chi2_delta.restype = C.c_double
     L.or_chi2_delta.argtypes = [_dp, C.c_int32, _dp, _dp, _dp, C.c_int32, _dp]
     L.or_host_threads.restype = C.c_int32
+    L.or_factored_setup.restype = C.c_void_p
+    L.or_factored_setup.argtypes = [C.POINTER(_Model), _ip, C.c_int64, C.c_int64, C.c_int32]
+    L.or_factored_free.argtypes = [C.c_void_p]
+    L.or_factored_hxv.argtypes = [C.c_void_p, _dp, _dp, C.c_int32]
     L.or_chi2_model.restype = C.c_double
     L.or_chi2_model.argtypes = [_dp, C.c_int32, _dp, _dp, _dp, C.c_int32, C.c_int32, C.c_double,
                                 _dp]
@@ -225,6 +229,35 @@ def hxv(model, hmap, v, nthreads=1):
     lib().or_hxv_c128(C.byref(ms), _p(hmap, C.c_int32), hmap.size, _p(v.view(np.float64)),
                       _p(out.view(np.float64)), nthreads)
     return out
+
+
+class FactoredHxv:
+    """The up/down-factored FP64 H*v on the CPU (oracle/ed_oracle.c,
+    or_factored_*): the device's algorithm restated as the "best CPU" variant
+    of the baseline.  Not the reference's algorithm; real models without the
+    Jhflag terms only."""
+
+    def __init__(self, model, nup, ndw, nthreads=1):
+        self.hmap = build_sector(model.ns, nup, ndw)
+        self.dimup = binomial(model.ns, nup)
+        self.dimdw = binomial(model.ns, ndw)
+        self._ms = model._struct()
+        self.nthreads = nthreads
+        self.h = lib().or_factored_setup(C.byref(self._ms), _p(self.hmap, C.c_int32), self.dimup,
+                                         self.dimdw, nthreads)
+        if not self.h:
+            raise ValueError("model not factored (Jhflag terms or too many bath levels)")
+
+    def __call__(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(x)
+        lib().or_factored_hxv(self.h, _p(x), _p(y), self.nthreads)
+        return y
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_factored_free(self.h)
+            self.h = None
 
 
 def sparse_h(model, hmap):

@@ -94,6 +94,23 @@ def test_gloc_and_weiss_match_oracle():
         assert np.abs(gl[0, 0, 0, 1]).max() == 0.0 and np.abs(gl[0, 1, 0, 0]).max() == 0.0
 
 
+def test_gloc_real_axis_matches_oracle():
+    p = dmfted.default_params(norb=1, nbath=3, nspin=1, beta=50.0, lmats=64, lreal=400, xmu=0.1,
+                              wini=-3.0, wfin=3.0, eps=0.05)
+    with dmfted.EDSolver(p) as s:
+        rng = np.random.default_rng(4)
+        sig = np.zeros((1, 1, 1, 1, 400), np.complex128, order="F")
+        sig[0, 0, 0, 0] = 0.2 * rng.normal(size=400) - 0.1j * np.abs(rng.normal(size=400))
+        he, wt = bethe.bethe_dos(500, 1.0)
+        gr = s.gloc_realaxis_diag(he, wt, sig)
+        w = np.linspace(-3.0, 3.0, 400)
+        z = w + 0.05j + 0.1 - sig[0, 0, 0, 0]
+        ref = np.zeros(400, np.complex128)
+        for k in range(he.size):
+            ref = ref + (1.0 / (z - he[k])) * wt[k]
+        assert np.abs(gr[0, 0, 0, 0] - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
 def test_chi2_fitgf_per_orbital_matches_oracle():
     """ed_chi2_fitgf on a two-orbital bath: each orbital's fit of spin 1 equals
     the oracle's fit of that orbital; the spin-2 parameters stay as they were."""

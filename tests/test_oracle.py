@@ -302,3 +302,14 @@ def test_bethe_gloc_and_delta_self_consistency():
     g0 = O.weiss_diag(g, sig, wm, 0.0, 0.0, weiss=True)
     assert np.abs(1.0 / g0 - (1j * wm - d)).max() < 1e-12
     assert abs(wt.sum() - 1.0) < 1e-3
+
+
+@pytest.mark.parametrize("norb,nbath,nup,ndw", [(1, 7, 4, 4), (1, 5, 3, 2), (2, 3, 4, 3)])
+def test_factored_cpu_hxv_equals_map_hxv(norb, nbath, nup, ndw):
+    """The "best CPU" baseline (the up/down-factored FP64 product on the host)
+    is the same operator as the reference-faithful map H*v."""
+    m = O.seeded_model(3, norb=norb, nbath=nbath, u=2.0, beta=100.0)
+    F = O.FactoredHxv(m, nup, ndw, nthreads=2)
+    x = np.random.default_rng(1).normal(size=F.hmap.size)
+    ref = O.hxv(m, F.hmap, x.astype(np.complex128), nthreads=2).real
+    assert np.abs(F(x) - ref).max() <= 1e-13 * np.abs(ref).max()
