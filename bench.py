@@ -309,6 +309,34 @@ def dmft_workload(dmfted, device, steps, warmup):
                 fit_host=(a[:8].copy(), wm, delta, w, am[:8].copy(), c2[:8].copy()))
 
 
+def small_configs_workload(dmfted, device, steps, warmup):
+    """The two smaller single-orbital configurations through the same solve:
+    Ns=8 (Nbath=7, U=2, sector 4/4, dim 4,900) and Ns=12 (Nbath=11, U=3, bath
+    seed 2, sector 6/6, dim 853,776), beta=100, Lmats=4096, 200-step chains;
+    median device milliseconds per solve in both precisions."""
+    out = {}
+    for name, nbath, u, seed, nn in (("ns8_4_4", 7, 2.0, SEED, 4), ("ns12_6_6", 11, 3.0, 2, 6)):
+        rng = np.random.default_rng(seed)
+        bath = np.concatenate([rng.uniform(-1.0, 1.0, nbath), 0.5 + rng.uniform(-0.1, 0.1, nbath)])
+        row = {}
+        for prec, tag in ((dmfted.MIXED, "mixed"), (dmfted.FP64, "fp64")):
+            p = dmfted.default_params(norb=1, nbath=nbath, uloc=[u], beta=BETA, lmats=LMATS,
+                                      lreal=0, lanc_nstates_sector=1, precision=prec,
+                                      device=device)
+            with dmfted.EDSolver(p) as s:
+                isec = s.sector_index(nn, nn)
+                for _ in range(warmup):
+                    s.ed_solve(bath, sectors=[isec])
+                ms = []
+                for _ in range(steps):
+                    s.ed_solve(bath, sectors=[isec])
+                    ms.append(s.timings()["total_ms"])
+                row[tag + "_ms"] = statistics.median(ms)
+                row[tag + "_e0"] = s.egs()
+        out[name] = row
+    return out
+
+
 def fit_cpu(host):
     """The oracle's conjugate-gradient fit (one thread) on the first start
     points of the batch: fits per second and the largest chi^2 difference."""
@@ -425,6 +453,8 @@ def run_ours(args, rank, world, local_rank):
         extra["differentiation"] = differentiation_workload(
             dmfted, local_rank, args.steps, args.warmup, solvers[dmfted.FP64], isec, bath)
         extra["self_consistency"] = dmft_workload(dmfted, local_rank, args.steps, args.warmup)
+        extra["smaller_configs"] = small_configs_workload(dmfted, local_rank, args.steps,
+                                                          args.warmup)
     for sv in solvers.values():
         sv.close()
     return res, dim, hv32, hv64, extra
@@ -525,25 +555,24 @@ def reference_hv_per_step():
     return 2 * nl - 1 + 2 * NGF, nl
 
 
-def small_solve_check(nthreads):
+def small_solve_check(nthreads, nbath=7, nn=4, u=2.0, seed=SEED, threads=None, reps=50):
     """The model behind the extrapolation (3 map builds + per-product time x
-    products) against a complete oracle solve, measured end to end, on the
-    small configuration (Ns=8, sector 4/4, dim 4900, U=2, Lmats=4096): plain
+    products) against a complete oracle solve, measured end to end: plain
     Lanczos ground state with its second pass, observables, two 200-step
-    chains, G and Sigma."""
+    chains, G and Sigma on Lmats=4096.  Default: the small configuration (Ns=8,
+    sector 4/4, dim 4900, U=2), single-thread and on every core."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    m = O.seeded_model(SEED, nbath=7, u=2.0, beta=BETA)
+    m = O.seeded_model(seed, nbath=nbath, u=u, beta=BETA)
     out = {}
-    for nt in (1, nthreads):
+    for nt in (threads or (1, nthreads)):
         t0 = time.perf_counter()
-        r = O.solve_t0(m, sectors=[(4, 4)], nstates_sector=1, lmats=LMATS, nthreads=nt)
+        r = O.solve_t0(m, sectors=[(nn, nn)], nstates_sector=1, lmats=LMATS, nthreads=nt)
         t_full = time.perf_counter() - t0
         t0 = time.perf_counter()
-        hm = O.build_sector(m.ns, 4, 4)
+        hm = O.build_sector(m.ns, nn, nn)
         t_map = time.perf_counter() - t0
         v = O.start_vector(hm.size)
-        reps = 50
         t0 = time.perf_counter()
         for _ in range(reps):
             v = O.hxv(m, hm, v, nthreads=nt)
@@ -578,6 +607,11 @@ def reference_arm(args, nthreads):
     t_map1, t_hv1 = cpu_sample(1, 1)
     single = 1.0 / cpu_step_seconds(t_map1, t_hv1, hv_per_step)
     check = small_solve_check(nthreads)
+    # the same check at Ns=12 (sector 6/6, dim 853,776, U=3, bath seed 2), where
+    # the products dominate as at Ns=14: every core only (one thread would
+    # take about ten minutes)
+    check12 = small_solve_check(nthreads, nbath=11, nn=6, u=3.0, seed=2, threads=(nthreads,),
+                                reps=2)
     return dict(
         metric=METRIC, value=val, unit=UNIT, n_gpus=args.gpus, steps=args.steps,
         warmup=args.warmup, ms_per_step=sec * 1e3, higher_is_better=True, scaling="weak",
@@ -596,6 +630,7 @@ def reference_arm(args, nthreads):
                                sample="the map build and 1 product on one thread, same scaling"),
             best_cpu_factored=best_cpu_line(nthreads, hv_per_step),
             model_check_small_config=check,
+            model_check_ns12=check12,
             sampled_wall_s=t_sampled),
         e2e=dict(value=val, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
 

@@ -1143,7 +1143,7 @@ int dmfted_chi2_fitgf(dmfted_ctx *c, const double *fg, int32_t ispin, double *ba
     DM_CUDA(cudaMemcpyAsync(dx, xd.data(), (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
     DM_CUDA(cudaMemcpyAsync(dw, w.data(), (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
     DM_CUDA(cudaMemcpyAsync(dz, zc.data(), (size_t)no * 8, cudaMemcpyHostToDevice, c->stream));
-    cg_fit_device(c, no, nbth, L, da, dx, dg, no, dw, dz, c->p.cg_scheme == DMFTED_CG_WEISS,
+    cg_fit_device(c, no, nbth, L, da, dx, dg, no, dw, dz, 0.0, c->p.cg_scheme == DMFTED_CG_WEISS,
                   c->p.cg_niter, c->p.cg_stop, c->p.cg_ftol, c->p.cg_eps, ibuf.p, dc, ibuf.p + no);
     std::vector<double> c2(no);
     std::vector<int> it(2 * (size_t)no);
@@ -1173,10 +1173,7 @@ int dmfted_cg_fit_batch_device(dmfted_ctx *c, int32_t nbatch, int32_t nbath, int
                "null argument");
     check_cg_params(c, scheme);
     DM_CUDA(cudaSetDevice(c->device));
-    DBuf<double> z;
-    z.alloc(1);
-    DM_CUDA(cudaMemcpyAsync(z.p, &zc, 8, cudaMemcpyHostToDevice, c->stream));
-    cg_fit_device(c, nbatch, nbath, L, d_a, d_xdelta, d_g, 1, d_w, z.p,
+    cg_fit_device(c, nbatch, nbath, L, d_a, d_xdelta, d_g, 1, d_w, nullptr, zc,
                   scheme == DMFTED_CG_WEISS, c->p.cg_niter, c->p.cg_stop, c->p.cg_ftol,
                   c->p.cg_eps, d_iter, d_chi2, d_status);
     DM_CUDA(cudaStreamSynchronize(c->stream));
@@ -1193,17 +1190,15 @@ int dmfted_cg_fit_batch(dmfted_ctx *c, int32_t nbatch, int32_t nbath, int32_t L,
     DM_CUDA(cudaSetDevice(c->device));
     const size_t na = (size_t)nbatch * 2 * nbath;
     DBuf<double> buf;
-    buf.alloc(na + 4 * (size_t)L + 1 + nbatch);
-    double *da = buf.p, *dx = da + na, *dg = dx + L, *dw = dg + 2 * (size_t)L, *dz = dw + L,
-           *dc = dz + 1;
+    buf.alloc(na + 4 * (size_t)L + nbatch);
+    double *da = buf.p, *dx = da + na, *dg = dx + L, *dw = dg + 2 * (size_t)L, *dc = dw + L;
     DBuf<int> ibuf;
     ibuf.alloc(2 * (size_t)nbatch);
     DM_CUDA(cudaMemcpyAsync(da, a, na * 8, cudaMemcpyHostToDevice, c->stream));
     DM_CUDA(cudaMemcpyAsync(dx, xdelta, (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
     DM_CUDA(cudaMemcpyAsync(dg, g, 2 * (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
     DM_CUDA(cudaMemcpyAsync(dw, w, (size_t)L * 8, cudaMemcpyHostToDevice, c->stream));
-    DM_CUDA(cudaMemcpyAsync(dz, &zc, 8, cudaMemcpyHostToDevice, c->stream));
-    cg_fit_device(c, nbatch, nbath, L, da, dx, dg, 1, dw, dz, scheme == DMFTED_CG_WEISS,
+    cg_fit_device(c, nbatch, nbath, L, da, dx, dg, 1, dw, nullptr, zc, scheme == DMFTED_CG_WEISS,
                   c->p.cg_niter, c->p.cg_stop, c->p.cg_ftol, c->p.cg_eps, ibuf.p, dc,
                   ibuf.p + nbatch);
     std::vector<int> it(2 * (size_t)nbatch);

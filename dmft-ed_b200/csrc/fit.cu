@@ -55,7 +55,8 @@ struct FitArgs {
     const double2 *g;     // [ng][L] targets; job b fits target b % ng
     int ng;
     const double *w;      // [L] weights W_n
-    const double *zc;     // [ng] xmu - Hloc_aa of the target (weiss scheme)
+    const double *zc;     // [ng] xmu - Hloc_aa of the target (weiss scheme), or null:
+    double zc0;           //      then zc0 for every target
     int weiss;
     int itmax, istop;
     double ftol, eps;
@@ -336,7 +337,7 @@ __global__ void __launch_bounds__(kFitThreads) k_cg_fit(const FitArgs A) {
     S.acc = S.red + 2 * (nt >> 5);
     const int tg = b % A.ng;
     const double2 *g = A.g + (int64_t)tg * A.L;
-    const double zc = A.zc ? A.zc[tg] : 0.0;
+    const double zc = A.zc ? A.zc[tg] : A.zc0;
     double *a = A.a + (int64_t)b * na;
     for (int j = tid; j < na; j += nt) S.p[j] = a[j];
     __syncthreads();
@@ -407,9 +408,9 @@ static size_t fit_smem(int nbath, int nt) {
 }
 
 void cg_fit_device(dmfted_ctx *c, int nbatch, int nbath, int L, double *a, const double *x,
-                   const double *g, int ng, const double *w, const double *zc, int weiss,
-                   int itmax, int istop, double ftol, double eps, int *iter, double *chi2,
-                   int *status) {
+                   const double *g, int ng, const double *w, const double *zc, double zc0,
+                   int weiss, int itmax, int istop, double ftol, double eps, int *iter,
+                   double *chi2, int *status) {
     DM_REQUIRE(nbatch > 0 && nbath > 0 && L > 0 && ng > 0, DMFTED_ERR_ARG,
                "cg fit: empty batch, bath or grid");
     DM_REQUIRE(itmax >= 1, DMFTED_ERR_ARG, "cg fit: cg_niter < 1");
@@ -432,6 +433,7 @@ void cg_fit_device(dmfted_ctx *c, int nbatch, int nbath, int L, double *a, const
     A.ng = ng;
     A.w = w;
     A.zc = zc;
+    A.zc0 = zc0;
     A.weiss = weiss;
     A.itmax = itmax;
     A.istop = istop;

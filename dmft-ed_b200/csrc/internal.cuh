@@ -475,9 +475,9 @@ void chi2_batch_device(dmfted_ctx *c, int nbatch, int nbath, int L, const double
 
 // ---- fit.cu ----------------------------------------------------------------
 void cg_fit_device(dmfted_ctx *c, int nbatch, int nbath, int L, double *a, const double *x,
-                   const double *g, int ng, const double *w, const double *zc, int weiss,
-                   int itmax, int istop, double ftol, double eps, int *iter, double *chi2,
-                   int *status);
+                   const double *g, int ng, const double *w, const double *zc, double zc0,
+                   int weiss, int itmax, int istop, double ftol, double eps, int *iter,
+                   double *chi2, int *status);
 void gloc_diag_device(dmfted_ctx *c, int L, int le, const double *he, const double *wt,
                       const double *wm, double eps, const double *sig, double *gl);
 void weiss_diag_device(dmfted_ctx *c, int L, int scheme, const double *hloc_aa, const double *wm,
