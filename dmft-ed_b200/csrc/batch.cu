@@ -907,27 +907,31 @@ static void launch_persistent(dmfted_ctx *c, void (*kern)(KArgs...), int CL, int
 }
 
 // CTAs per eigensolve job: from the largest sector (at least
-// batch_cluster_min states per CTA, to amortise the cluster barriers), or
-// DMFTED_BATCH_CLUSTER_EIGS.  Only sectors that give every CTA that many
-// states are shared; smaller ones run one per CTA.
+// batch_cluster_min states per CTA, to amortise the cluster barriers; 16, the
+// non-portable cluster size, from 32 per CTA: on the Ns=10 workload, whose
+// largest sector holds 63,504 states, 16 took 35.9 ms of eigensolves against
+// 38.6 ms for 8), or DMFTED_BATCH_CLUSTER_EIGS.  Only sectors that give every
+// CTA that many states are shared; smaller ones run one per CTA.
 static int eigs_cluster(const dmfted_ctx *c, int64_t dmax) {
     const int64_t per = c->batch_cluster_min;
     if (const char *e = getenv("DMFTED_BATCH_CLUSTER_EIGS")) {
         const int v = atoi(e);
         if (v == 1 || v == 2 || v == 4 || v == 8 || v == 16) return v;
     }
-    return dmax >= 8 * per ? 8 : dmax >= 4 * per ? 4 : dmax >= 2 * per ? 2 : 1;
+    return dmax >= 32 * per ? 16 : dmax >= 8 * per ? 8 : dmax >= 4 * per ? 4 : dmax >= 2 * per ? 2 : 1;
 }
 
-// CTAs per chain: more than one only while the chains leave SMs idle, or
-// DMFTED_BATCH_CLUSTER_GF.
+// CTAs per chain: two once the largest chain holds 16 x batch_cluster_min
+// states (the long chains set the phase's time: 200 chains of the Ns=10
+// workload took 35.0 ms with pairs against 38.9 ms one per CTA), more only
+// while the chains leave SMs idle; or DMFTED_BATCH_CLUSTER_GF.
 static int chain_cluster(dmfted_ctx *c, int njobs, int64_t dmax) {
     const int64_t per = c->batch_cluster_min;
     if (const char *e = getenv("DMFTED_BATCH_CLUSTER_GF")) {
         const int v = atoi(e);
         if (v == 1 || v == 2 || v == 4 || v == 8 || v == 16) return v;
     }
-    int cl = 1;
+    int cl = dmax >= 16 * per ? 2 : 1;
     while (cl < 8 && (int64_t)njobs * cl * 2 <= 2 * (int64_t)num_sms(c) &&
            dmax / (cl * 2) >= 2 * per)
         cl *= 2;
