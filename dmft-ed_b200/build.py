@@ -13,8 +13,9 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libdmfted.so")
 SOURCES = ["api.cu", "fock.cu", "hxv.cu", "lanczos.cu", "gf.cu", "observables.cu", "chi2.cu",
            "batch.cu", "noalloc.cu", "dense.cu", "diag.cu", "fit.cu",
-           "restart.cu"]
-HEADERS = ["internal.cuh", "reduce.cuh", "hxv.cuh", "tridiag.cuh", "sector.cuh", "jterms.cuh"]
+           "restart.cu", "edio.cu"]
+HEADERS = ["internal.cuh", "reduce.cuh", "hxv.cuh", "tridiag.cuh", "sector.cuh", "jterms.cuh",
+           "fortfmt.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

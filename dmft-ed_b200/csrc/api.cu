@@ -341,6 +341,34 @@ static void local_energies(dmfted_ctx *c, const std::vector<double> &acc) {
     c->eloc = {epot, 0.0, ehart, eknot, dust, dund, dse, dph};
 }
 
+// sz2, n2 and s2tot of observables_impurity (ED_OBSERVABLES.f90:131-160)
+// from the weighted impurity-configuration histogram: sz_a = (n_a,up -
+// n_a,dw)/2, n_a = n_a,up + n_a,dw, s2tot = <(sum_a sz_a)^2>.
+static void spin_charge_moments(dmfted_ctx *c, const std::vector<double> &acc) {
+    const int no = c->norb, ni = 1 << no;
+    const double *P = acc.data() + obs_count(c) - ni * ni;
+    c->sz2.assign((size_t)no * no, 0.0);
+    c->n2.assign((size_t)no * no, 0.0);
+    c->s2tot = 0.0;
+    for (int iu = 0; iu < ni; iu++)
+        for (int id = 0; id < ni; id++) {
+            const double w = P[iu * ni + id];
+            double sz[kMaxNorb], nt[kMaxNorb], stot = 0.0;
+            for (int a = 0; a < no; a++) {
+                const double u = (iu >> a) & 1, d = (id >> a) & 1;
+                sz[a] = (u - d) / 2.0;
+                nt[a] = u + d;
+                stot += sz[a];
+            }
+            for (int a = 0; a < no; a++)
+                for (int b = 0; b < no; b++) {
+                    c->sz2[a * no + b] += sz[a] * sz[b] * w;
+                    c->n2[a * no + b] += nt[a] * nt[b] * w;
+                }
+            c->s2tot += stot * stot * w;
+        }
+}
+
 static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list) {
     DM_REQUIRE(c->bath_set, DMFTED_ERR_STATE, "ed_solve: bath not set");
     const dmfted_params &p = c->p;
@@ -385,6 +413,8 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     c->hf_terms.assign(acc.begin() + 3 * no, acc.begin() + 3 * no + 4 * no * c->nbath);
     c->hf_hops = false;  // the hop terms are computed when the gradient is asked for
     local_energies(c, acc);
+    spin_charge_moments(c, acc);
+    c->szr_sigma = c->sigma_now;
     DM_CUDA(cudaEventRecord(ev[2], c->stream));
     // ---- Green's functions ---------------------------------------------------
     const size_t gsz = (size_t)c->nspin * no;
@@ -393,6 +423,7 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     c->sm.alloc(std::max<size_t>(2 * gsz * p.lmats, 2));
     c->sr.alloc(std::max<size_t>(2 * gsz * p.lreal, 2));
     c->g0m.alloc(std::max<size_t>(2 * gsz * p.lmats, 2));
+    c->g0r.alloc(std::max<size_t>(2 * gsz * p.lreal, 2));
     DM_CUDA(cudaMemsetAsync(c->gm.p, 0, c->gm.n * sizeof(double), c->stream));
     DM_CUDA(cudaMemsetAsync(c->gr.p, 0, c->gr.n * sizeof(double), c->stream));
     int64_t hv_gf = 0;
@@ -431,6 +462,16 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
     gf_sigma(c);
     DM_CUDA(cudaEventRecord(ev[3], c->stream));
     DM_CUDA(cudaStreamSynchronize(c->stream));
+    // Im Sigma(iw_1), Im Sigma(iw_2) per (spin, orbital): get_szr of the
+    // next solve reads them
+    c->sigma_now.assign(2 * gsz, 0.0);
+    for (size_t so = 0; so < gsz && p.lmats >= 2; so++) {
+        double v[4];
+        DM_CUDA(cudaMemcpy(v, c->sm.p + 2 * so * p.lmats, sizeof v, cudaMemcpyDeviceToHost));
+        c->sigma_now[2 * so] = v[1];
+        c->sigma_now[2 * so + 1] = v[3];
+    }
+    c->sigma_read = false;
     float ms;
     DM_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
     c->stats.ms[0] = ms;
@@ -450,7 +491,8 @@ static void ed_solve_impl(dmfted_ctx *c, const int32_t *sectors, int nsect_list)
 // (Nspin,Nspin,Norb,Norb,L) Fortran layout from the device [nspin][norb][L]
 // complex blocks (normal bath: diagonal in spin and orbital).
 static void get_gf(dmfted_ctx *c, const dmfted::DBuf<double> &d, int L, double *out) {
-    DM_REQUIRE(c->solved, DMFTED_ERR_STATE, "no solve has run on this context");
+    DM_REQUIRE(c->solved || (c->sigma_read && (&d == &c->sm || &d == &c->sr)), DMFTED_ERR_STATE,
+               "no solve has run on this context");
     const int ns = c->nspin, no = c->norb;
     std::vector<double> h(2 * (size_t)ns * no * std::max(L, 1));
     if (L > 0)
@@ -930,6 +972,12 @@ int dmfted_get_g0imp_matsubara(dmfted_ctx *c, double *g) {
     API_BEGIN
     DM_REQUIRE(c && g, DMFTED_ERR_ARG, "null argument");
     get_gf(c, c->g0m, c->p.lmats, g);
+    API_END
+}
+int dmfted_get_g0imp_real(dmfted_ctx *c, double *g) {
+    API_BEGIN
+    DM_REQUIRE(c && g, DMFTED_ERR_ARG, "null argument");
+    get_gf(c, c->g0r, c->p.lreal, g);
     API_END
 }
 

@@ -76,11 +76,13 @@ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
 // Sigma = G0^-1 - G^-1 with G0^-1 = z + xmu - Hloc_aa - Delta(z),
 // Delta(z) = sum_k V_k^2/(z - e_k) (get_sigma_normal.f90:17-39,
 // ED_BATH_FUNCTIONS.f90:247-257,1800-1806), and G0and = 1/G0^-1
-// (g0and_bath_mats, :1026-1056).  One thread per (spin, orbital, frequency).
+// (g0and_bath_mats / g0and_bath_real, :1026-1056).  One thread per (spin,
+// orbital, frequency).
 __global__ void k_sigma(int nspin, int norb, int nbath, const double *e, const double *v,
                         const double *hloc_aa, double xmu, const double *wm, int lmats,
                         const double *wr, int lreal, double eps, const double2 *gm,
-                        const double2 *gr, double2 *sm, double2 *sr, double2 *g0m) {
+                        const double2 *gr, double2 *sm, double2 *sr, double2 *g0m,
+                        double2 *g0r) {
     const int L = lmats + lreal;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (t >= (int64_t)nspin * norb * L) return;
@@ -103,6 +105,7 @@ __global__ void k_sigma(int nspin, int norb, int nbath, const double *e, const d
         g0m[(int64_t)so * lmats + f] = cdiv(make_double2(1.0, 0.0), ig0);
     } else {
         sr[(int64_t)so * lreal + f - lmats] = sg;
+        g0r[(int64_t)so * lreal + f - lmats] = cdiv(make_double2(1.0, 0.0), ig0);
     }
 }
 
@@ -126,7 +129,8 @@ void gf_sigma(dmfted_ctx *c) {
     k_sigma<<<div_up(n, 256), 256, 0, c->stream>>>(
         c->nspin, c->norb, c->nbath, c->d_bath_e.p, c->d_bath_v.p, c->d_hloc_aa.p, c->p.xmu,
         c->d_wm.p, c->p.lmats, c->d_wr.p, c->p.lreal, c->p.eps, (const double2 *)c->gm.p,
-        (const double2 *)c->gr.p, (double2 *)c->sm.p, (double2 *)c->sr.p, (double2 *)c->g0m.p);
+        (const double2 *)c->gr.p, (double2 *)c->sm.p, (double2 *)c->sr.p, (double2 *)c->g0m.p,
+        (double2 *)c->g0r.p);
     DM_CHECK_LAUNCH();
     c->launches++;
 }

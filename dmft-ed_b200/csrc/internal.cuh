@@ -302,10 +302,20 @@ struct dmfted_ctx {
     double zeta = 1.0, egs = 0.0;
     bool finite_t = false;
     int nstates_total = 1;  // lanc_nstates_total, adapted by ed_analysis between solves
-    dmfted::DBuf<double> gm, gr, g0m, sm, sr;  // complex (nspin,norb,L) blocks
+    dmfted::DBuf<double> gm, gr, g0m, g0r, sm, sr;  // complex (nspin,norb,L) blocks
     std::vector<double> obs;                   // dens, up, dw, docc, magz (norb each)
     std::vector<double> hf_terms;              // nk[2][norb][nbath], hop[2][norb][nbath]
     std::vector<double> eloc = std::vector<double>(8, 0.0);  // Epot Eint Ehartree Eknot Dust Dund Dse Dph
+    // observables_impurity's other averages of the last solve: sz2(a,b),
+    // n2(a,b) (norb x norb, b fastest), s2tot; and Im Sigma(iw_1), Im
+    // Sigma(iw_2) per (spin, orbital) as they stood when its observables were
+    // taken (get_szr runs before the Green's functions of the same solve:
+    // the previous solve's self-energy, 0 before the first)
+    std::vector<double> sz2, n2;
+    double s2tot = 0.0;
+    std::vector<double> szr_sigma;              // [nspin*norb][2]
+    std::vector<double> sigma_now;              // the same two values after the last solve
+    bool sigma_read = false;                    // Sigma loaded by dmfted_read_impsigma
     dmfted::SolveStats stats;
     bool solved = false;
 };

@@ -26,6 +26,7 @@
 #include <string>
 #include <vector>
 
+#include "fortfmt.h"
 #include "internal.cuh"
 
 using namespace dmfted;
@@ -34,53 +35,10 @@ namespace {
 
 int ok() { return set_error(DMFTED_OK, ""); }
 
-// Fortran Aw output: right-justified in w characters (longer strings keep
-// their first w characters).
-std::string fa(const std::string &s, int w) {
-    if ((int)s.size() >= w) return s.substr(0, w);
-    return std::string(w - s.size(), ' ') + s;
-}
-
-// Fortran Fw.d output of a finite value; a field too narrow is all '*'.
-std::string ff(double x, int w, int d) {
-    char buf[64];
-    std::snprintf(buf, sizeof buf, "%*.*f", w, d, x);
-    std::string s(buf);
-    if ((int)s.size() > w) return std::string(w, '*');
-    return s;
-}
-
-// Fortran ESw.d output: one digit before the point, d after, exponent
-// "E+dd"; a three-digit exponent drops the letter ("+ddd"), as the Fortran
-// standard's exponent form for |exp| > 99 with no Ee given.
-std::string fes(double x, int w, int d) {
-    char buf[64];
-    std::snprintf(buf, sizeof buf, "%.*E", d, x);
-    std::string s(buf);
-    const size_t e = s.find('E');
-    if (e != std::string::npos) {
-        const std::string mant = s.substr(0, e);
-        const char sign = s[e + 1];
-        std::string digs = s.substr(e + 2);
-        while (digs.size() > 2 && digs[0] == '0') digs.erase(0, 1);
-        if (digs.size() <= 2) {
-            if (digs.size() < 2) digs = "0" + digs;
-            s = mant + "E" + sign + digs;
-        } else {
-            s = mant + sign + digs;
-        }
-    }
-    if ((int)s.size() > w) return std::string(w, '*');
-    return std::string(w - s.size(), ' ') + s;
-}
-
-std::string fi(long long v, int w) {
-    char buf[64];
-    std::snprintf(buf, sizeof buf, "%*lld", w, v);
-    std::string s(buf);
-    if ((int)s.size() > w) return std::string(w, '*');
-    return s;
-}
+using fort::A;
+using fort::ES;
+using fort::F;
+using fort::I;
 
 void check_bath_dims(const dmfted_params *p, int32_t nb) {
     DM_REQUIRE(p->norb >= 1 && p->nspin >= 1 && p->nbath >= 0, DMFTED_ERR_ARG, "bad dimensions");
@@ -103,20 +61,21 @@ int dmfted_save_bath(const dmfted_params *p, const char *path, const double *bat
         DM_REQUIRE(p && path && bath, DMFTED_ERR_ARG, "null argument");
         check_bath_dims(p, nb);
         const int64_t half = (int64_t)nb / 2;
-        std::string out;
+        fort::Record head;
         for (int s = 0; s < p->nspin; s++)
             for (int a = 0; a < p->norb; a++) {
                 const std::string tag = "l" + std::to_string(a + 1) + "_s" + std::to_string(s + 1);
-                out += fa("#Ek_" + tag, 21) + " " + fa("Vk_" + tag, 21) + " ";
+                head.add(A("#Ek_" + tag, 21)).add(A("Vk_" + tag, 21));
             }
-        out += "\n";
+        std::string out = head.s + "\n";
         for (int k = 0; k < p->nbath; k++) {
+            fort::Record row;
             for (int s = 0; s < p->nspin; s++)
                 for (int a = 0; a < p->norb; a++) {
                     const int64_t io = bath_io(p, s, a, k);
-                    out += ff(bath[io], 21, 12) + " " + ff(bath[half + io], 21, 12) + " ";
+                    row.add(F(bath[io], 21, 12)).add(F(bath[half + io], 21, 12));
                 }
-            out += "\n";
+            out += row.s + "\n";
         }
         std::FILE *f = std::fopen(path, "w");
         DM_REQUIRE(f, DMFTED_ERR_ARG, std::string("save_dmft_bath: cannot open ") + path);
@@ -172,10 +131,10 @@ int dmfted_print_state_list(dmfted_ctx *c, const char *path) {
         for (size_t i = 0; i < c->states.size(); i++) {
             const auto &st = c->states[i];
             const int is = st.isector;
-            out += fi((long long)i + 1, 3) + ff(st.e, 18, 12) + "  " +
-                   fes(std::exp(-c->p.beta * (st.e - emin)), 19, 12) + " " +
-                   fi(c->getnup[is - 1], 3) + fi(c->getndw[is - 1], 3) + "   " + fi(is, 3) +
-                   fi(c->getdim[is - 1], 10) + "\n";
+            out += I((long long)i + 1, 3) + F(st.e, 18, 12) + "  " +
+                   ES(std::exp(-c->p.beta * (st.e - emin)), 19, 12) + " " +
+                   I(c->getnup[is - 1], 3) + I(c->getndw[is - 1], 3) + "   " + I(is, 3) +
+                   I(c->getdim[is - 1], 10) + "\n";
         }
         std::FILE *f = std::fopen(path, "w");
         DM_REQUIRE(f, DMFTED_ERR_ARG, std::string("print_state_list: cannot open ") + path);

@@ -94,6 +94,7 @@ EXPORTS = {
     "dmfted_get_sigma_matsubara": (C.c_int, [_vp, _dp]),
     "dmfted_get_sigma_real": (C.c_int, [_vp, _dp]),
     "dmfted_get_g0imp_matsubara": (C.c_int, [_vp, _dp]),
+    "dmfted_get_g0imp_real": (C.c_int, [_vp, _dp]),
     "dmfted_get_observables": (C.c_int, [_vp, _dp, _dp, _dp, _dp, _dp]),
     "dmfted_get_eigenspace": (C.c_int, [_vp, C.c_int32, _dp, _ip, _ip, _dp]),
     "dmfted_get_egs": (C.c_int, [_vp, _dp]),
@@ -116,6 +117,12 @@ EXPORTS = {
     "dmfted_read_bath": (C.c_int, [C.c_void_p, C.c_char_p, _dp, C.c_int32]),
     "dmfted_print_state_list": (C.c_int, [_vp, C.c_char_p]),
     "dmfted_read_state_list": (C.c_int, [_vp, C.c_char_p]),
+    "dmfted_print_impg": (C.c_int, [_vp, C.c_char_p, C.c_char_p]),
+    "dmfted_print_impsigma": (C.c_int, [_vp, C.c_char_p, C.c_char_p]),
+    "dmfted_print_impg0": (C.c_int, [_vp, C.c_char_p, C.c_char_p]),
+    "dmfted_read_impsigma": (C.c_int, [_vp, C.c_char_p, C.c_char_p]),
+    "dmfted_write_observables": (C.c_int, [_vp, C.c_char_p, C.c_char_p, C.c_int32]),
+    "dmfted_write_energy": (C.c_int, [_vp, C.c_char_p, C.c_char_p]),
     "dmfted_time_hxv": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, _dp]),
     "dmfted_hxv_timing": (C.c_int, [_vp, C.c_int32]),
     "dmfted_autotune_log": (C.c_int, [_vp, C.c_char_p, C.c_int32, C.POINTER(C.c_int32)]),
@@ -372,6 +379,9 @@ class EDSolver:
     def ed_get_g0imp_matsubara(self):
         return self._gf(lib().dmfted_get_g0imp_matsubara, self.params.lmats)
 
+    def ed_get_g0imp_real(self):
+        return self._gf(lib().dmfted_get_g0imp_real, self.params.lreal)
+
     def observables(self):
         no = self.params.norb
         arrs = [np.zeros(no) for _ in range(5)]
@@ -452,6 +462,33 @@ class EDSolver:
     def read_state_list(self, path):
         """state_list.restart: the per-sector state counts for the next solve."""
         _ck(lib().dmfted_read_state_list(self.ctx, os.fsencode(path)))
+
+    # ---- printed outputs (ED_IO, ED_OBSERVABLES) ---------------------------
+    def print_impG(self, dir="", suffix=""):
+        """print_impG_normal: impG_l<a><a>_s<s>_iw/_realw<suffix>.ed in dir."""
+        _ck(lib().dmfted_print_impg(self.ctx, os.fsencode(dir), suffix.encode()))
+
+    def print_impSigma(self, dir="", suffix=""):
+        """print_impSigma_normal: impSigma_l<a><a>_s<s>_iw/_realw<suffix>.ed."""
+        _ck(lib().dmfted_print_impsigma(self.ctx, os.fsencode(dir), suffix.encode()))
+
+    def print_impG0(self, dir="", suffix=""):
+        """print_impG0_normal: the Weiss field under the impG_... names."""
+        _ck(lib().dmfted_print_impg0(self.ctx, os.fsencode(dir), suffix.encode()))
+
+    def read_impSigma(self, dir="", suffix=""):
+        """read_impSigma_normal: the impSigma files back into the context."""
+        _ck(lib().dmfted_read_impsigma(self.ctx, os.fsencode(dir), suffix.encode()))
+
+    def write_observables(self, dir="", suffix="", legend=False):
+        """write_observables (and write_legend when legend): observables_all
+        (appended), observables_last, parameters_last<suffix>.ed."""
+        _ck(lib().dmfted_write_observables(self.ctx, os.fsencode(dir), suffix.encode(),
+                                           1 if legend else 0))
+
+    def write_energy(self, dir="", suffix=""):
+        """write_energy_info and write_energy: energy_info.ed, energy_last<suffix>.ed."""
+        _ck(lib().dmfted_write_energy(self.ctx, os.fsencode(dir), suffix.encode()))
 
     # ---- the self-consistency around the solve ----------------------------
     def ed_chi2_fitgf(self, fg, bath, ispin=1):

@@ -242,6 +242,9 @@ int dmfted_get_gimp_real(dmfted_ctx *ctx, double *g);
 int dmfted_get_sigma_matsubara(dmfted_ctx *ctx, double *s);
 int dmfted_get_sigma_real(dmfted_ctx *ctx, double *s);
 int dmfted_get_g0imp_matsubara(dmfted_ctx *ctx, double *g);
+/* ed_get_g0imp_real: G0and(w + i eps) = 1/G0^-1 on the real axis
+ * (get_sigma_normal.f90:68 with g0and_bath_real), the same layout (Lreal). */
+int dmfted_get_g0imp_real(dmfted_ctx *ctx, double *g);
 /* ed_dens, ed_dens_up, ed_dens_dw, ed_docc (Norb each), ed_magz (Norb). */
 int dmfted_get_observables(dmfted_ctx *ctx, double *dens, double *dens_up, double *dens_dw,
                            double *docc, double *magz);
@@ -380,6 +383,54 @@ int dmfted_print_state_list(dmfted_ctx *ctx, const char *path);
  * reference's stop message otherwise).  Call after dmfted_init, before the
  * first solve. */
 int dmfted_read_state_list(dmfted_ctx *ctx, const char *path);
+
+/* ---- printed outputs (ED_IO, ED_OBSERVABLES) --------------------------------
+ * dir: the directory the files are written to or read from (NULL or "": the
+ * working directory, as the reference); suffix: ed_file_suffix (ED_MAIN.f90:
+ * 185,193,214), "" or NULL for one impurity.  All need a solve on ctx except
+ * dmfted_read_impsigma.  The reference calls print_impSigma and print_impG at
+ * the end of buildgf_impurity when ed_print_Sigma / ed_print_G are set
+ * (ED_GREENS_FUNCTIONS.f90:161-165), write_observables at the end of
+ * observables_impurity (ED_OBSERVABLES.f90:418-420) and write_energy at the
+ * end of local_energy_impurity (:681-684). */
+
+/* print_impG_normal (ED_IO/print_impG.f90:38-46): per spin s and orbital a,
+ * impG_l<a><a>_s<s>_iw<suffix>.ed (Lmats lines) and impG_l<a><a>_s<s>_realw
+ * <suffix>.ed (Lreal lines), each line the abscissa, Im G, Re G: the columns
+ * of SciFortran's splot (not in the tree, version unpinned), written here in
+ * ES24.16 so that a read gives back the same doubles. */
+int dmfted_print_impg(dmfted_ctx *ctx, const char *dir, const char *suffix);
+/* print_impSigma_normal (ED_IO/print_impSigma.f90:37-45): the same for the
+ * self-energy, impSigma_l<a><a>_s<s>_iw / _realw<suffix>.ed. */
+int dmfted_print_impsigma(dmfted_ctx *ctx, const char *dir, const char *suffix);
+/* print_impG0_normal (ED_IO/print_impG0.f90:37-45): the Weiss field G0and,
+ * written under the impG_... names as the reference does (so it replaces the
+ * files of dmfted_print_impg). */
+int dmfted_print_impg0(dmfted_ctx *ctx, const char *dir, const char *suffix);
+/* read_impSigma_normal (ED_IO/read_impSigma.f90:38-46): the impSigma files
+ * read back (three numbers per line, list-directed; Lmats and Lreal lines)
+ * into the context's self-energies, which dmfted_get_sigma_* then return and
+ * the next solve's scattering rate and Z in observables_all.ed use.  Every
+ * file is read before anything changes; a missing or short file is
+ * DMFTED_ERR_ARG. */
+int dmfted_read_impsigma(dmfted_ctx *ctx, const char *dir, const char *suffix);
+/* write_observables (ED_OBSERVABLES.f90:780-849), normal mode: one
+ * "(90(F15.9,1X))" record dens(a), docc(a), dens_up(a), dens_dw(a), magz(a),
+ * s2tot, egs, sz2(a,b), n2(a,b), zimp(a,s), simp(a,s) appended to
+ * observables_all<suffix>.ed and written to observables_last<suffix>.ed, and
+ * parameters_last<suffix>.ed ("(90F15.9)": xmu, beta, Uloc(a), Ust, Jh, Jx,
+ * Jp).  zimp and simp are get_szr (:695-708) of the self-energy the solve's
+ * observables saw: the reference takes them before the same solve's Green's
+ * functions, i.e. from the previous solve (or a read self-energy), 0 before
+ * the first.  legend != 0 also writes observables_info.ed and
+ * parameters_info.ed (write_legend, :715-758), which the reference does on
+ * its first call. */
+int dmfted_write_observables(dmfted_ctx *ctx, const char *dir, const char *suffix,
+                             int32_t legend);
+/* write_energy_info and write_energy (ED_OBSERVABLES.f90:760-774,851-857):
+ * energy_info.ed and energy_last<suffix>.ed ("(90F15.9)": Epot,
+ * Epot-Ehartree, Eknot, Ehartree, Dust, Dund, Dse, Dph). */
+int dmfted_write_energy(dmfted_ctx *ctx, const char *dir, const char *suffix);
 
 /* ---- timing helpers (device time on the context's stream) ------------ */
 /* Average device milliseconds of one H*v on the current sector over reps

@@ -514,19 +514,20 @@ def write_dmft_bath_text(bath, norb, nspin, nbath):
     """write_dmft_bath, normal bath (ED_BATH/dmft_aux.f90:310-336): the header
     "(90(A21,1X))" and Nbath rows "(90(F21.12,1X))" of ((e, v), orbitals), spins."""
     half = len(bath) // 2
-    head = ""
+    head = []
     for s in range(nspin):
         for a in range(norb):
             tag = f"l{a + 1}_s{s + 1}"
-            head += f"#Ek_{tag}".rjust(21) + " " + f"Vk_{tag}".rjust(21) + " "
-    rows = [head]
+            head += [f"#Ek_{tag}".rjust(21), f"Vk_{tag}".rjust(21)]
+    # the 1X after a record's last item transmits nothing
+    rows = [" ".join(head)]
     for k in range(nbath):
-        r = ""
+        r = []
         for s in range(nspin):
             for a in range(norb):
                 io = k + a * nbath + s * nbath * norb
-                r += f"{bath[io]:21.12f} {bath[half + io]:21.12f} "
-        rows.append(r)
+                r += [f"{bath[io]:21.12f}", f"{bath[half + io]:21.12f}"]
+        rows.append(" ".join(r))
     return "\n".join(rows) + "\n"
 
 
@@ -539,6 +540,78 @@ def print_state_list_text(energies, sectors, getnup, getndw, getdim, beta):
         out.append(f"{i + 1:3d}{e:18.12f}  {_fortran_es(np.exp(-beta * (e - emin)), 19, 12)} "
                    f"{getnup[isec - 1]:3d}{getndw[isec - 1]:3d}   {isec:3d}{getdim[isec - 1]:10d}")
     return "\n".join(out) + "\n"
+
+
+def moments_state(model, hmap, psi, peso):
+    """sz2(a,b), n2(a,b) and s2tot of observables_impurity for one state,
+    ED_OBSERVABLES.f90:131-160 (impurity orbital a: up bit a, down bit a+Ns)."""
+    no, ns = model.norb, model.ns
+    m = np.asarray(hmap, np.int64)
+    w = peso * np.abs(np.asarray(psi)) ** 2
+    nup = np.stack([((m >> a) & 1).astype(np.float64) for a in range(no)])
+    ndw = np.stack([((m >> (a + ns)) & 1).astype(np.float64) for a in range(no)])
+    sz = (nup - ndw) / 2.0
+    nt = nup + ndw
+    sz2 = np.array([[np.sum(sz[a] * sz[b] * w) for b in range(no)] for a in range(no)])
+    n2 = np.array([[np.sum(nt[a] * nt[b] * w) for b in range(no)] for a in range(no)])
+    s2tot = float(np.sum(sz.sum(axis=0) ** 2 * w))
+    return sz2, n2, s2tot
+
+
+def szr(sigma_iw, beta):
+    """get_szr (ED_OBSERVABLES.f90:695-708) from Sigma(iw_1), Sigma(iw_2):
+    (zimp, simp)."""
+    wm1, wm2 = np.pi / beta, 3.0 * np.pi / beta
+    s1, s2 = sigma_iw[0].imag, sigma_iw[1].imag
+    return 1.0 / (1.0 + abs(s1 / wm1)), s1 - wm1 * (s2 - s1) / (wm2 - wm1)
+
+
+def observables_legend_text(norb, nspin):
+    """write_legend, normal mode (ED_OBSERVABLES.f90:720-731): "(A1,90(A10,6X))"
+    labels, the 6X after the last one not transmitted."""
+    no, ns = norb, nspin
+    lab = []
+    lab += [f"{a}dens_{a}" for a in range(1, no + 1)]
+    lab += [f"{no + a}docc_{a}" for a in range(1, no + 1)]
+    lab += [f"{2 * no + a}nup_{a}" for a in range(1, no + 1)]
+    lab += [f"{3 * no + a}ndw_{a}" for a in range(1, no + 1)]
+    lab += [f"{4 * no + a}mag_{a}" for a in range(1, no + 1)]
+    lab += [f"{5 * no + 1}s2", f"{5 * no + 2}egs"]
+    lab += [f"{5 * no + 2 + (a - 1) * no + b}sz2_{a}{b}" for a in range(1, no + 1)
+            for b in range(1, no + 1)]
+    lab += [f"{(5 + no) * no + 2 + (a - 1) * no + b}n2_{a}{b}" for a in range(1, no + 1)
+            for b in range(1, no + 1)]
+    lab += [f"{(5 + 2 * no) * no + 2 + (s - 1) * ns + a}z_{a}s{s}" for s in range(1, ns + 1)
+            for a in range(1, no + 1)]
+    lab += [f"{(6 + 2 * no) * no + 2 + ns + (s - 1) * ns + a}sig_{a}s{s}"
+            for s in range(1, ns + 1) for a in range(1, no + 1)]
+    return "#" + (" " * 6).join(x.rjust(10)[:10] for x in lab) + "\n"
+
+
+def f15_9(x):
+    """F15.9 (a field too narrow is all '*')."""
+    t = f"{x:15.9f}"
+    return t if len(t) <= 15 else "*" * 15
+
+
+def observables_record_text(dens, docc, dens_up, dens_dw, magz, s2tot, egs, sz2, n2, zimp, simp):
+    """write_observables, normal mode (ED_OBSERVABLES.f90:786-797): one
+    "(90(F15.9,1X))" record; zimp/simp are [spin][orbital]."""
+    vals = list(dens) + list(docc) + list(dens_up) + list(dens_dw) + list(magz) + [s2tot, egs]
+    vals += list(np.asarray(sz2).reshape(-1)) + list(np.asarray(n2).reshape(-1))
+    vals += list(np.asarray(zimp).reshape(-1)) + list(np.asarray(simp).reshape(-1))
+    return " ".join(f15_9(v) for v in vals) + "\n"
+
+
+def energy_texts(eimp, doubles):
+    """write_energy_info and write_energy (ED_OBSERVABLES.f90:760-774,851-857)
+    from ed_get_eimp = [Epot, Eint, Ehartree, Eknot] and ed_get_doubles =
+    [Dust, Dund, Dse, Dph]."""
+    names = ["<Hi>", "<V>=<Hi-Ehf>", "<Eloc>", "<Ehf>", "<Dst>", "<Dnd>", "<Dse>", "<Dph>"]
+    info = "#" + " ".join(f"{k + 1}{n}".rjust(14)[:14] for k, n in enumerate(names)) + "\n"
+    epot, _, ehart, eknot = eimp
+    vals = [epot, epot - ehart, eknot, ehart] + list(doubles)
+    return info, "".join(f15_9(v) for v in vals) + "\n"
 
 
 def cg_weights(cg_weight, xdelta):
@@ -633,6 +706,7 @@ def _gf_and_obs(model, states, egs, zeta, finite_t, lmats, lreal, wini, wfin, ep
     (:442-488), followed by get_sigma_normal.  states: [(e, nup, ndw, psi)]."""
     ns, no = model.ns, model.norb
     obs = {k: np.zeros(no) for k in ["dens", "dens_up", "dens_dw", "docc", "magz"]}
+    obs["sz2"], obs["n2"], obs["s2tot"] = np.zeros((no, no)), np.zeros((no, no)), 0.0
     eacc = np.zeros(8)
     wm = matsubara(model.beta, lmats)
     wr = realaxis(wini, wfin, lreal)
@@ -644,8 +718,12 @@ def _gf_and_obs(model, states, egs, zeta, finite_t, lmats, lreal, wini, wfin, ep
         peso = (np.exp(-model.beta * (e - egs)) if finite_t else 1.0) / zeta
         psi = np.asarray(psi).astype(np.complex128)
         o = observables_state(model, hm, psi, peso)
-        for k in obs:
+        for k in ["dens", "dens_up", "dens_dw", "docc", "magz"]:
             obs[k] += o[k]
+        sz2, n2, s2 = moments_state(model, hm, psi, peso)
+        obs["sz2"] += sz2
+        obs["n2"] += n2
+        obs["s2tot"] += s2
         local_energy_state(model, hm, psi, peso, eacc)
         for ispin in range(model.nspin):
             for iorb in range(no):

@@ -62,3 +62,31 @@ def test_fortran_es_format():
     assert O._fortran_es(1.0, 19, 12) == " 1.000000000000E+00"
     assert O._fortran_es(3.5e-218, 19, 12) == " 3.500000000000-218"
     assert O._fortran_es(2.0e-5, 19, 12) == " 2.000000000000E-05"
+
+
+def test_observable_file_formats():
+    """The oracle's restatement of write_legend / write_energy_info /
+    write_energy (ED_OBSERVABLES.f90:715-774,851-857): "#" then A10 labels
+    16 characters apart (A10,6X), the 6X after the last label not transmitted;
+    the column numbers of z and sig step by Nspin per spin, as the reference
+    writes them."""
+    t = O.observables_legend_text(1, 1)
+    assert t.startswith("#   1dens_1      ") and t.endswith("  12sig_1s1\n")
+    fields = [t[1 + 16 * k:11 + 16 * k].strip() for k in range((len(t) - 1 + 6) // 16)]
+    assert fields == ["1dens_1", "2docc_1", "3nup_1", "4ndw_1", "5mag_1", "6s2", "7egs",
+                      "8sz2_11", "9n2_11", "10z_1s1", "12sig_1s1"]
+    t2 = O.observables_legend_text(2, 2)
+    labels = t2[1:].split()
+    assert labels[20:24] == ["21z_1s1", "22z_2s1", "23z_1s2", "24z_2s2"]
+    assert labels[-1] == "28sig_2s2" and len(labels) == 5 * 2 + 2 + 2 * 4 + 2 * 4
+    info, last = O.energy_texts([-1.25, 0.0, 0.5, -0.75], [0.1, 0.2, 0.0, 0.0])
+    assert info == ("#" + " ".join(lab.rjust(14) for lab in [
+        "1<Hi>", "2<V>=<Hi-Ehf>", "3<Eloc>", "4<Ehf>", "5<Dst>", "6<Dnd>", "7<Dse>",
+        "8<Dph>"]) + "\n")
+    assert last == ("   -1.250000000   -1.750000000   -0.750000000    0.500000000"
+                    "    0.100000000    0.200000000    0.000000000    0.000000000\n")
+    rec = O.observables_record_text([1.0], [0.25], [0.5], [0.5], [0.0], 0.375, -3.5,
+                                    [[0.375]], [[1.5]], [[1.0]], [[0.0]])
+    assert rec == " ".join(f"{x:15.9f}" for x in
+                           [1.0, 0.25, 0.5, 0.5, 0.0, 0.375, -3.5, 0.375, 1.5, 1.0, 0.0]) + "\n"
+    assert O.f15_9(1e7) == "*" * 15
