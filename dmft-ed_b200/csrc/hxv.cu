@@ -791,8 +791,10 @@ __global__ void __launch_bounds__(256, MB) k_hxv_lean(const HxvArgs<T> a,
             const uint2 wu2 = *reinterpret_cast<const uint2 *>(a.wu + r);
             const T2 du2 = *reinterpret_cast<const T2 *>(a.du + r);
 
-            // 2. diagonal from the staged tile
+            // 2. diagonal from the staged tile; the rows' own values stay in
+            // registers for the alpha partial of step 5
             T acc[NC][2];
+            T x0[NC], x1[NC];
             {
                 T xa[NC], xb[NC];
                 vld<T, NC>(xs + (r + sw) * NC, xa);
@@ -800,8 +802,10 @@ __global__ void __launch_bounds__(256, MB) k_hxv_lean(const HxvArgs<T> a,
                 const unsigned iu0 = wu2.x & imask, iu1 = wu2.y & imask;
 #pragma unroll
                 for (int j = 0; j < NC; j++) {
-                    acc[j][0] = (du2.x + cdg[j][iu0]) * (sw ? xb[j] : xa[j]);
-                    acc[j][1] = (du2.y + cdg[j][iu1]) * (sw ? xa[j] : xb[j]);
+                    x0[j] = sw ? xb[j] : xa[j];
+                    x1[j] = sw ? xa[j] : xb[j];
+                    acc[j][0] = (du2.x + cdg[j][iu0]) * x0[j];
+                    acc[j][1] = (du2.y + cdg[j][iu1]) * x1[j];
                 }
             }
             // 3. row hops: NC-wide gathers from the tile, fixed count
@@ -856,20 +860,8 @@ __global__ void __launch_bounds__(256, MB) k_hxv_lean(const HxvArgs<T> a,
                     acc[j][1] += vv[e] * nb[j][e].y;
                 }
             }
-            // 5. Lanczos combination, store, alpha partial (the rows' own
-            // values re-read from the tile)
+            // 5. Lanczos combination, store, alpha partial
             double part = 0.0;
-            T x0[NC], x1[NC];
-            if (LZ) {
-                T xa[NC], xb[NC];
-                vld<T, NC>(xs + (r + sw) * NC, xa);
-                vld<T, NC>(xs + (r + 1 - sw) * NC, xb);
-#pragma unroll
-                for (int j = 0; j < NC; j++) {
-                    x0[j] = sw ? xb[j] : xa[j];
-                    x1[j] = sw ? xa[j] : xb[j];
-                }
-            }
 #pragma unroll
             for (int j = 0; j < NC; j++) {
                 if (j >= nc) continue;
