@@ -174,3 +174,42 @@ def test_bethe_dmft_iteration_matches_oracle():
     assert abs(c2[0][0] - O.chi2_model(new, xd, tg, w, True, 0.0, False)) <= 1e-12 * fr
     assert abs(c2[0][0] - fr) <= 2e-2 * fr, (c2[0][0], fr)
     assert c2[0][0] < 1e-2 * O.chi2_model(bath, xd, tg, w, True, 0.0, False)
+
+
+def test_bethe_dmft_loop_converges_to_a_self_consistent_solution():
+    """The whole loop of drivers/ed_hm_bethe.f90:53-88 (dmft_loop) at the small
+    configuration (Ns=8, U=2, half filling, the ground state of sector 4/4):
+    it reaches the reference's convergence test (relative change of the Weiss
+    field below 1e-5) within the iteration budget, and its fixed point is
+    self-consistent: the impurity G equals the local G built from the same
+    Sigma to the bath-fit accuracy (Nbath=7).  At the converged bath the
+    solve's Sigma and the Weiss field agree with the oracle's chain of steps,
+    as in the one-iteration test above."""
+    m = O.seeded_model(1, norb=1, nbath=7, u=2.0, beta=100.0)
+    p = dmfted.default_params(norb=1, nbath=7, uloc=[2.0], beta=100.0, lmats=1024, lreal=0,
+                              lanc_nstates_sector=1)
+    he, wt = bethe.bethe_dos(500, 1.0)
+    wm = O.matsubara(100.0, 1024)
+    with dmfted.EDSolver(p) as s:
+        sec = [s.sector_index(4, 4)]
+        bath, nit = bethe.dmft_loop(s, m.bath_array(), nloop=80, wmixing=0.5, dmft_error=1e-5,
+                                    sectors=sec)
+        assert nit < 80, "the loop did not converge"
+        s.ed_solve(bath, sectors=sec)
+        gimp = s.ed_get_gimp_matsubara()[0, 0, 0, 0]
+        smats = s.ed_get_sigma_matsubara()[0, 0, 0, 0]
+        gloc = s.gloc_matsubara_diag(he, wt, s.ed_get_sigma_matsubara())[0, 0, 0, 0]
+        weiss = s.get_weiss(s.gloc_matsubara_diag(he, wt, s.ed_get_sigma_matsubara()),
+                            s.ed_get_sigma_matsubara(), None)[0, 0, 0, 0]
+    # self-consistency G_imp = G_loc on the fitted frequencies
+    rel = np.abs(gimp[:1000] - gloc[:1000]).max() / np.abs(gloc[:1000]).max()
+    assert rel < 5e-3, rel
+    # the converged bath through the oracle's steps
+    mc = O.seeded_model(1, norb=1, nbath=7, u=2.0, beta=100.0)
+    mc.e[0, 0], mc.v[0, 0] = bath[:7], bath[7:]
+    ref = O.solve_t0(mc, sectors=[(4, 4)], nstates_sector=1, lmats=1024, nthreads=4)
+    assert np.all(np.abs(smats - ref["smats"][0, 0]) <= 1e-8 * np.maximum(1.0, wm ** 2))
+    gl = O.gloc_diag(he, wt, wm, 0.0, ref["smats"][0, 0])
+    assert np.abs(gloc - gl).max() <= 1e-8
+    wr = O.weiss_diag(gl, ref["smats"][0, 0], wm, 0.0, 0.0, weiss=True)
+    assert np.abs(weiss - wr).max() <= 1e-7
