@@ -31,14 +31,6 @@ namespace dmfted {
 
 constexpr int kDenseThreads = 1024;
 
-struct DenseJob {
-    int nup, ndw;
-    int n;            // sector dimension
-    int m;            // eigenpairs wanted (lowest m)
-    int slot;         // output slot: evals[slot * kDenseMaxEigen + j]
-    int64_t a_off;    // work: A (n x n, row-major)
-    int64_t out_off;  // eigenvectors: m x n FP64, vector j at out_off + j*n
-};
 
 // Sum over the block of one double per thread (plain FP64), returned in every
 // thread.  red: 32 doubles of shared memory.
@@ -199,12 +191,15 @@ static int dense_ritz_doubles(int n, int m) {
 }
 
 // Host side: the lowest want[i] eigenpairs of every sector list[i] whose
-// want[i] > 0, in one persistent launch.
-void dense_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<int> &want,
-                std::vector<DenseEig> &res) {
-    res.assign(list.size(), DenseEig());
-    std::vector<DenseJob> jobs;
-    std::vector<int> where;
+// want[i] > 0, in one persistent launch.  dense_eigs_launch queues the work on
+// the context's stream and returns without waiting; dense_eigs_collect waits
+// for it and fills the results.
+void dense_eigs_launch(dmfted_ctx *c, const std::vector<int> &list, const std::vector<int> &want,
+                       DensePending &pd) {
+    pd = DensePending();
+    pd.nlist = list.size();
+    std::vector<DenseJob> &jobs = pd.jobs;
+    std::vector<int> &where = pd.where;
     int64_t work = 0, vec = 0;
     for (size_t i = 0; i < list.size(); i++) {
         if (want[i] <= 0) continue;
@@ -256,10 +251,19 @@ void dense_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<i
         c->dense_eval.p, (int64_t)c->dense_work.n, (int64_t)c->dense_vec.n, rcap);
     DM_CHECK_LAUNCH();
     c->launches++;
+    pd.stream = c->stream;
+}
+
+void dense_eigs_collect(dmfted_ctx *c, DensePending &pd, std::vector<DenseEig> &res) {
+    res.assign(pd.nlist, DenseEig());
+    const std::vector<DenseJob> &jobs = pd.jobs;
+    const std::vector<int> &where = pd.where;
+    const int nj = (int)jobs.size();
+    if (nj == 0) return;
     std::vector<double> ev((size_t)nj * kDenseMaxEigen);
     DM_CUDA(cudaMemcpyAsync(ev.data(), c->dense_eval.p, ev.size() * sizeof(double),
-                            cudaMemcpyDeviceToHost, c->stream));
-    DM_CUDA(cudaStreamSynchronize(c->stream));
+                            cudaMemcpyDeviceToHost, pd.stream));
+    DM_CUDA(cudaStreamSynchronize(pd.stream));
     for (int j = 0; j < nj; j++) {
         const DenseJob &J = jobs[j];
         DenseEig &r = res[where[j]];
@@ -268,6 +272,13 @@ void dense_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<i
                        ev.begin() + (size_t)J.slot * kDenseMaxEigen + J.m);
         r.vecs = c->dense_vec.p + J.out_off;
     }
+}
+
+void dense_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<int> &want,
+                std::vector<DenseEig> &res) {
+    DensePending pd;
+    dense_eigs_launch(c, list, want, pd);
+    dense_eigs_collect(c, pd, res);
 }
 
 }  // namespace dmfted

@@ -292,25 +292,55 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
     }
     if (pool > 0) c->lockpool.alloc((size_t)pool);
     // ---- dense sectors --------------------------------------------------
-    {
-        std::vector<int> dl, dw;
-        std::vector<size_t> at;
-        for (size_t i = 0; i < jobs.size(); i++)
-            if (jobs[i].br == kDense) {
-                dl.push_back(jobs[i].isector);
-                dw.push_back(jobs[i].neigen);
-                at.push_back(i);
+    // One CTA per sector (a few dozen at most): on the second stream when
+    // batched Lanczos sectors follow, so that the batched kernel's CTAs start
+    // on the SMs the dense ones leave free instead of after them (both take
+    // their jobs from atomic queues, so neither waits for the other).
+    std::vector<int> dense_l, dense_w;
+    std::vector<size_t> dense_at;
+    for (size_t i = 0; i < jobs.size(); i++)
+        if (jobs[i].br == kDense) {
+            dense_l.push_back(jobs[i].isector);
+            dense_w.push_back(jobs[i].neigen);
+            dense_at.push_back(i);
+        }
+    bool any_batch = false;
+    for (auto &j : jobs) any_batch = any_batch || j.br == kBatch;
+    const bool dense_aside = !dense_l.empty() && any_batch && c->stream2 && !dbg;
+    DensePending dense_pd;
+    if (!dense_l.empty()) {
+        if (dense_aside) {
+            DM_CUDA(cudaEventRecord(c->ev_fork, c->stream));
+            DM_CUDA(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0));
+            std::swap(c->stream, c->stream2);
+            try {
+                dense_eigs_launch(c, dense_l, dense_w, dense_pd);
+            } catch (...) {
+                std::swap(c->stream, c->stream2);
+                throw;
             }
-        if (!dl.empty()) {
-            std::vector<DenseEig> dr;
-            dense_eigs(c, dl, dw, dr);
-            for (size_t k = 0; k < dl.size(); k++) {
-                SectorJob &j = jobs[at[k]];
-                j.e = dr[k].evals;
-                j.dense_vecs = dr[k].vecs;
-            }
+            std::swap(c->stream, c->stream2);
+        } else {
+            dense_eigs_launch(c, dense_l, dense_w, dense_pd);
         }
     }
+    auto dense_finish = [&]() {
+        if (dense_l.empty()) return;
+        std::vector<DenseEig> dr;
+        dense_eigs_collect(c, dense_pd, dr);
+        if (dense_aside) {
+            // the vectors are read on the main stream from here on
+            DM_CUDA(cudaEventRecord(c->ev_join, c->stream2));
+            DM_CUDA(cudaStreamWaitEvent(c->stream, c->ev_join, 0));
+        }
+        for (size_t k = 0; k < dense_l.size(); k++) {
+            SectorJob &j = jobs[dense_at[k]];
+            j.e = dr[k].evals;
+            j.dense_vecs = dr[k].vecs;
+        }
+        dense_l.clear();
+    };
+    if (!dense_aside) dense_finish();
     stamp("dense branch");
     // ---- first Lanczos run ---------------------------------------------------
     {
@@ -339,6 +369,7 @@ static int64_t sector_spectra(dmfted_ctx *c, std::vector<SectorJob> &jobs, bool 
             }
         }
     }
+    dense_finish();
     stamp("batched first runs");
     std::vector<double> ev(kLzMax + 8);
     for (auto &j : jobs) {

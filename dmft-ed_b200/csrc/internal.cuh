@@ -397,6 +397,25 @@ struct DenseEig {
 };
 void dense_eigs(dmfted_ctx *c, const std::vector<int> &list, const std::vector<int> &want,
                 std::vector<DenseEig> &res);
+// The same in two halves: the launch queues the work on the context's stream
+// (the one current at the call) and returns; the collect waits for it.
+struct DenseJob {
+    int nup, ndw;
+    int n;            // sector dimension
+    int m;            // eigenpairs wanted (lowest m)
+    int slot;         // output slot: evals[slot * kDenseMaxEigen + j]
+    int64_t a_off;    // work: A (n x n, row-major)
+    int64_t out_off;  // eigenvectors: m x n FP64, vector j at out_off + j*n
+};
+struct DensePending {
+    std::vector<DenseJob> jobs;
+    std::vector<int> where;
+    size_t nlist = 0;
+    cudaStream_t stream = nullptr;
+};
+void dense_eigs_launch(dmfted_ctx *c, const std::vector<int> &list, const std::vector<int> &want,
+                       DensePending &pd);
+void dense_eigs_collect(dmfted_ctx *c, DensePending &pd, std::vector<DenseEig> &res);
 
 // ---- diag.cu ---------------------------------------------------------------
 // ed_diag_c (ED_DIAG.f90:93-228): every sector of `list` diagonalised with the
