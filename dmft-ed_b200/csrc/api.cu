@@ -611,6 +611,7 @@ int dmfted_init(const dmfted_params *p, const double *hloc, dmfted_ctx **out) {
         if (const char *e = getenv("DMFTED_HXV_OCC")) c->tune_occ = atoi(e);
         if (const char *e = getenv("DMFTED_ELL_GROUP")) c->tune_ell_group = std::max(1, std::min(32, atoi(e)));
         if (const char *e = getenv("DMFTED_MIXED_TOL32")) c->mixed_tol32 = atof(e);
+        if (const char *e = getenv("DMFTED_GS_BASIS_MB")) c->gs_basis_budget = atoll(e) << 20;
         if (const char *e = getenv("DMFTED_AUTOTUNE")) c->autotune = atoi(e) != 0;
         if (const char *e = getenv("DMFTED_CHAIN_LANES")) c->chain_lanes = atoi(e);
         if (const char *e = getenv("DMFTED_GF_HEAD64")) c->gf_head64 = std::max(0, atoi(e));

@@ -897,6 +897,85 @@ __global__ void __launch_bounds__(256, MB) k_hxv_lean(const HxvArgs<T> a,
     }
 }
 
+// ---------------------------------------------------------------------------
+// k_hxv_global: the same product for sectors whose columns do not fit in
+// shared memory (DimUp x 16 bytes above the 200 KB a tile may take: Ns >= 16
+// near half filling).  One thread per element, in index order (a warp holds
+// consecutive rows of one column): the up hops gather from the element's own
+// column in global memory (a column is at most a few hundred KB, served from
+// L1/L2), the down hops read whole neighbour columns (coalesced), the tables
+// are the ELL ones of the other kernels.
+template <typename T, bool LZ>
+__global__ void __launch_bounds__(256) k_hxv_global(const HxvArgs<T> a) {
+    if (LZ) {
+        if (a.status[0]) return;  // chain finished: every later step is a no-op
+    }
+    __shared__ T spu[kMaxParams];
+    __shared__ T sdint[64];
+    const int tid = threadIdx.x;
+    for (int i = tid; i < a.P && i < kMaxParams; i += blockDim.x) spu[i] = a.pu[i];
+    const int ni = 1 << a.norb;
+    for (int i = tid; i < ni * ni; i += blockDim.x)
+        sdint[i] = a.dint[a.dswap ? (i % ni) * ni + i / ni : i];
+    __syncthreads();
+    const unsigned imask = (unsigned)ni - 1u;
+    const int64_t dimup = a.dimup, dimdw = a.dimdw, ncols = dimdw * a.nstack;
+    const int64_t total = ncols * dimup;
+    double sc = 1.0, cprev = 0.0;
+    if (LZ) {
+        sc = a.scale[a.k];
+        cprev = a.k > 0 ? a.beta[a.k] * a.scale[a.k - 1] : 0.0;
+    }
+    const T sch = (T)sc, scl = (T)(sc - (double)sch);
+    const T cph = (T)cprev, cpl = (T)(cprev - (double)cph);
+    const T *x = a.x + (int64_t)blockIdx.y * a.vstride;
+    T *y = a.y + (int64_t)blockIdx.y * a.vstride;
+    const T *xprev = LZ ? a.xprev + (int64_t)blockIdx.y * a.vstride : nullptr;
+    CSum dot;
+    dot.zero();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + tid; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t cg = i / dimup, r = i - cg * dimup;
+        const int64_t q = cg / dimdw, cc = cg - q * dimdw;
+        const T xi = x[i];
+        T acc = (a.du[r] + a.dd[cc] + sdint[(a.wu[r] & imask) * ni + (a.wd[cc] & imask)]) * xi;
+        const int nu = a.cu[r], nd = a.cd[cc];
+        const T *col = x + cg * dimup;
+        for (int e = 0; e < nu && e < a.W; e++) {
+            const uint32_t en = a.eu[(int64_t)e * dimup + r];
+            if (!DM_IN(ell_col(en), dimup) || !DM_IN(ell_par(en), a.P)) continue;
+            const T v = ell_neg(en) ? -spu[ell_par(en)] : spu[ell_par(en)];
+            acc += v * col[ell_col(en)];
+        }
+        for (int e = 0; e < nd && e < a.W; e++) {
+            const uint32_t en = a.ed[(int64_t)e * dimdw + cc];
+            if (!DM_IN(ell_col(en), dimdw) || !DM_IN(ell_par(en), a.P)) continue;
+            const T v = ell_neg(en) ? -a.pd[ell_par(en)] : a.pd[ell_par(en)];
+            acc += v * x[(q * dimdw + (int64_t)ell_col(en)) * dimup + r];
+        }
+        if (LZ) {
+            const T xp = xprev[i];
+            if constexpr (sizeof(T) == 8) {
+                acc = sc * acc - cprev * xp;
+            } else {
+                T t = -cpl * xp;
+                t = fmaf(-cph, xp, t);
+                t = fmaf(scl, acc, t);
+                acc = fmaf(sch, acc, t);
+            }
+            dot.add((double)xi * (double)acc);
+        }
+        y[i] = acc;
+    }
+    if (LZ) {
+        CSum arr[1] = {dot};
+        double tot[1];
+        if (grid_reduce<1>(arr, a.partials, a.counter, tot)) {
+            if (tid == 0) a.alpha[a.k] = sc * tot[0];
+        }
+    }
+}
+
 template <typename T>
 HxvArgs<T> make_hxv_args(const dmfted_ctx *c, const SectorView &s) {
     HxvArgs<T> a{};
@@ -952,6 +1031,7 @@ struct HxvCfg {
     int nc, vw, threads;
     size_t smem;
     int grid;
+    bool global;  // the columns do not fit in shared memory: k_hxv_global
 };
 
 
@@ -971,8 +1051,15 @@ static HxvCfg hxv_config(dmfted_ctx *c, const SectorView &s, const HxvArgs<T> &a
     const int64_t ncols = a.dimdw * nstack;
     g.nc = 16 / (int)sizeof(T);  // one 16-byte gather serves the whole tile
     const size_t tile = (size_t)a.dimup * sizeof(T) * g.nc;
-    DM_REQUIRE(tile <= 200 * 1024, DMFTED_ERR_UNSUPPORTED,
-               "sector column too long for the shared-memory H*v (DimUp too large)");
+    g.global = tile > (size_t)200 * 1024 || c->tune_hxv == 3;
+    if (g.global) {
+        // one thread per element
+        g.threads = 256;
+        g.smem = 0;
+        g.grid = (int)std::min<int64_t>(std::max<int64_t>(div_up(ncols * a.dimup, 256), 1),
+                                        std::min<int64_t>(kMaxRedBlocks, 8 * num_sms(c)));
+        return g;
+    }
     g.threads = (a.dimup <= (int64_t)128 * g.vw * 2) ? 128 : 256;
     g.smem = tile;
     g.grid = (int)std::min<int64_t>((ncols + g.nc - 1) / g.nc, kMaxRedBlocks);
@@ -1062,9 +1149,13 @@ static void launch_hxv(dmfted_ctx *c, const HxvArgs<T> &a, const HxvCfg &g, int 
     // offsets within the stacked vector
     const bool rv = g.vw == 2 && c->tune_hxv != 1 &&
                     (double)a.dimup * a.dimdw * a.nstack < 4.0e9;
-    const bool lean = lean_ok<T>(c, a, g);
+    const bool lean = !g.global && lean_ok<T>(c, a, g);
     hv_timer_begin(c);
-    if (lean) launch_lean<T, LZ ? 1 : 0>(c, a, g, nvec);
+    if (g.global) {
+        k_hxv_global<T, LZ><<<dim3(g.grid, nvec), g.threads, 0, c->stream>>>(a);
+        DM_CHECK_LAUNCH();
+        c->launches++;
+    } else if (lean) launch_lean<T, LZ ? 1 : 0>(c, a, g, nvec);
     else if (rv) launch_rv<T, LZ>(c, a, g, nvec);
     else if (g.vw == 2) launch_nc<T, NCT, 2, LZ>(c, a, g, nvec);
     else launch_nc<T, NCT, 1, LZ>(c, a, g, nvec);

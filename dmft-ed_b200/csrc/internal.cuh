@@ -232,9 +232,10 @@ struct dmfted_ctx {
     dmfted::DBuf<uint8_t> chainbuf;       // rotating vectors of a GF chain
     dmfted::DBuf<double> s64a, s64b, s64c;  // sector-sized FP64 scratch
     double mixed_tol32 = 1e-6;            // FP32-phase stopping tolerance of the mixed form
+    int64_t gs_basis_budget = 0;          // bytes the ground-state basis may take (0: 85 % of free memory)
     int gf_head64 = 20;                   // leading FP64 steps of a mixed-form GF chain
     int tune_nc = 0;                      // H*v columns per CTA override (0 = automatic)
-    int tune_hxv = 0;                     // H*v kernel: 0 automatic, 1 k_hxv, 2 k_hxv_rv
+    int tune_hxv = 0;                     // H*v kernel: 0 automatic, 1 k_hxv, 2 k_hxv_rv, 3 k_hxv_global
     int tune_occ = 3;                     // k_hxv_lean CTAs per SM (3: 80 registers; 2: 128)
     int tune_ell_group = 0;               // lanes per hop-table balance group (0: 8)
     dmfted::DBuf<double> d_wm, d_wr;      // Matsubara / real-axis grids
@@ -454,6 +455,7 @@ struct LanczosResult {
     double e0;
     int steps;
     bool converged;
+    bool capped = false;  // the stored basis was cut below the iteration limit by device memory
 };
 // Ground state of sector s.  psi (device, length dim, float64) receives the
 // normalised Ritz vector.  start: optional device float64 start vector.

@@ -354,8 +354,26 @@ template <typename T>
 static LanczosResult gs_run(dmfted_ctx *c, const SectorView &s, double *psi, const double *start,
                             double tol, int nitermax, int ncheck, bool refine) {
     const int64_t dim = s.dim;
-    const int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
+    int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
     const size_t ld = (size_t)((dim + 31) / 32 * 32);
+    // The stored basis takes at most 85 % of the device memory left (the
+    // buffer already held counts as free), or the context's budget.  A run
+    // cut below its iteration limit this way restarts from its Ritz vector
+    // (lanczos_gs).
+    bool capped = false;
+    {
+        size_t free_b = 0, total_b = 0;
+        DM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        double avail = 0.85 * ((double)free_b + (double)c->work.n);
+        if (c->gs_basis_budget > 0) avail = std::min(avail, (double)c->gs_basis_budget);
+        const int64_t fit = (int64_t)(avail / (double)(ld * sizeof(T))) - 1;
+        DM_REQUIRE(fit >= 8 || fit >= kmax, DMFTED_ERR_NOMEM,
+                   "ground-state Lanczos: the device holds fewer than 9 basis vectors");
+        if (fit < kmax) {
+            kmax = (int)fit;
+            capped = true;
+        }
+    }
     c->work.alloc(ld * sizeof(T) * (size_t)(kmax + 1));
     T *basis = reinterpret_cast<T *>(c->work.p);
     LanczosScalars lz = lz_slot(c, 0, kmax);
@@ -444,7 +462,9 @@ static LanczosResult gs_run(dmfted_ctx *c, const SectorView &s, double *psi, con
     DM_CHECK_LAUNCH();
     c->launches += 3;
     DM_CUDA(cudaStreamSynchronize(c->stream));
-    return LanczosResult{e0, n, hst[ST_CONV] != 0};
+    LanczosResult res{e0, n, hst[ST_CONV] != 0};
+    res.capped = capped;
+    return res;
 }
 
 // ||H psi - <psi|H|psi> psi|| of a unit FP64 vector: Lanczos step 0 from
@@ -478,7 +498,10 @@ LanczosResult lanczos_gs(dmfted_ctx *c, const SectorView &s, double *psi, const 
         // short run from a near eigenvector, before any copy can form.
         LanczosResult r = gs_run<double>(c, s, psi, start, tol, nitermax, ncheck, false);
         int steps = r.steps;
-        for (int round = 0; round < 3; round++) {
+        // a basis cut by device memory restarts until its steps add up to
+        // about twice the iteration limit
+        const int rounds = r.capped ? 3 + 2 * (nitermax + std::max(r.steps, 1) - 1) / std::max(r.steps, 1) : 3;
+        for (int round = 0; round < rounds; round++) {
             const double bound = 10.0 * tol * std::max(3.666852862501036e-11, std::fabs(r.e0));
             if (!(gs_residual(c, s, psi) > bound)) break;
             c->s64b.alloc(s.dim);
@@ -497,8 +520,9 @@ LanczosResult lanczos_gs(dmfted_ctx *c, const SectorView &s, double *psi, const 
     const double tol32 = std::max(tol, c->mixed_tol32);
     LanczosResult r = gs_run<float>(c, s, psi, start, tol32, nitermax, ncheck, false);
     int steps = r.steps;
+    const int rounds = r.capped ? 4 + 2 * (nitermax + std::max(r.steps, 1) - 1) / std::max(r.steps, 1) : 4;
     c->s64b.alloc(s.dim);
-    for (int round = 0; round < 4; round++) {
+    for (int round = 0; round < rounds; round++) {
         DM_CUDA(cudaMemcpyAsync(c->s64b.p, psi, s.dim * sizeof(double), cudaMemcpyDeviceToDevice,
                                 c->stream));
         r = gs_run<float>(c, s, psi, c->s64b.p, tol, nitermax, std::max(2, ncheck / 2), true);
@@ -831,8 +855,26 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
                     int ncheck, double *evals_h, double *vecs, const double *locked, int nlock,
                     double top) {
     const int64_t dim = s.dim;
-    const int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
+    int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
     const size_t ld = (size_t)((dim + 31) / 32 * 32);
+    // The stored basis takes at most 85 % of the device memory left (the
+    // buffer already held counts as free), or the context's budget.  A run
+    // cut below its iteration limit this way restarts from its Ritz vector
+    // (lanczos_gs).
+    bool capped = false;
+    {
+        size_t free_b = 0, total_b = 0;
+        DM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        double avail = 0.85 * ((double)free_b + (double)c->work.n);
+        if (c->gs_basis_budget > 0) avail = std::min(avail, (double)c->gs_basis_budget);
+        const int64_t fit = (int64_t)(avail / (double)(ld * sizeof(T))) - 1;
+        DM_REQUIRE(fit >= 8 || fit >= kmax, DMFTED_ERR_NOMEM,
+                   "ground-state Lanczos: the device holds fewer than 9 basis vectors");
+        if (fit < kmax) {
+            kmax = (int)fit;
+            capped = true;
+        }
+    }
     c->work.alloc(ld * sizeof(T) * (size_t)(kmax + 1));
     T *basis = reinterpret_cast<T *>(c->work.p);
     LanczosScalars lz = lz_slot(c, 0, kmax);
