@@ -360,13 +360,19 @@ static LanczosResult gs_run(dmfted_ctx *c, const SectorView &s, double *psi, con
     // buffer already held counts as free), or the context's budget.  A run
     // cut below its iteration limit this way restarts from its Ritz vector
     // (lanczos_gs).
+    // The memory query runs only when the basis has to grow, so that a solve
+    // whose buffer is already in place makes no driver call here.
     bool capped = false;
-    {
-        size_t free_b = 0, total_b = 0;
-        DM_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        double avail = 0.85 * ((double)free_b + (double)c->work.n);
+    const size_t need = ld * sizeof(T) * (size_t)(kmax + 1);
+    if (need > c->work.n || c->gs_basis_budget > 0) {
+        double avail = 1e300;
+        if (need > c->work.n) {
+            size_t free_b = 0, total_b = 0;
+            DM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            avail = 0.85 * ((double)free_b + (double)c->work.n);
+        }
         if (c->gs_basis_budget > 0) avail = std::min(avail, (double)c->gs_basis_budget);
-        const int64_t fit = (int64_t)(avail / (double)(ld * sizeof(T))) - 1;
+        const int64_t fit = (int64_t)std::min(avail / (double)(ld * sizeof(T)), 1e9) - 1;
         DM_REQUIRE(fit >= 8 || fit >= kmax, DMFTED_ERR_NOMEM,
                    "ground-state Lanczos: the device holds fewer than 9 basis vectors");
         if (fit < kmax) {
@@ -855,26 +861,8 @@ static int eigs_run(dmfted_ctx *c, const SectorView &s, int neigen, double tol, 
                     int ncheck, double *evals_h, double *vecs, const double *locked, int nlock,
                     double top) {
     const int64_t dim = s.dim;
-    int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
+    const int kmax = (int)std::min<int64_t>(std::min(nitermax, kLzMax - 2), dim);
     const size_t ld = (size_t)((dim + 31) / 32 * 32);
-    // The stored basis takes at most 85 % of the device memory left (the
-    // buffer already held counts as free), or the context's budget.  A run
-    // cut below its iteration limit this way restarts from its Ritz vector
-    // (lanczos_gs).
-    bool capped = false;
-    {
-        size_t free_b = 0, total_b = 0;
-        DM_CUDA(cudaMemGetInfo(&free_b, &total_b));
-        double avail = 0.85 * ((double)free_b + (double)c->work.n);
-        if (c->gs_basis_budget > 0) avail = std::min(avail, (double)c->gs_basis_budget);
-        const int64_t fit = (int64_t)(avail / (double)(ld * sizeof(T))) - 1;
-        DM_REQUIRE(fit >= 8 || fit >= kmax, DMFTED_ERR_NOMEM,
-                   "ground-state Lanczos: the device holds fewer than 9 basis vectors");
-        if (fit < kmax) {
-            kmax = (int)fit;
-            capped = true;
-        }
-    }
     c->work.alloc(ld * sizeof(T) * (size_t)(kmax + 1));
     T *basis = reinterpret_cast<T *>(c->work.p);
     LanczosScalars lz = lz_slot(c, 0, kmax);
