@@ -101,7 +101,10 @@ __device__ inline void tridiag_evec(const double *a, const double *b, int n, dou
     double *D = ws, *U1 = ws + n, *U2 = ws + 2 * n, *M = ws + 3 * n;
     double nrm = 0.0;
     for (int i = 0; i < n; i++) nrm = fmax(nrm, fabs(a[i] - lam) + (i > 0 ? fabs(b[i]) : 0.0));
-    const double tiny = fmax(nrm, 1e-300) * 1e-15;
+    // the replacement of a zero pivot; T - lam = 0 (a 1 x 1 sector, or lam I)
+    // has no scale of its own, and 1e-15 keeps 1/tiny and the squares of the
+    // solve finite
+    const double tiny = (nrm > 1e-290 ? nrm : 1.0) * 1e-15;
     double d = a[0] - lam, u1 = n > 1 ? b[1] : 0.0, u2 = 0.0;
     for (int i = 0; i < n - 1; i++) {
         const double l = b[i + 1], dn = a[i + 1] - lam, un = (i + 2 < n) ? b[i + 2] : 0.0;
