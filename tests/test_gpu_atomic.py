@@ -65,3 +65,30 @@ def test_two_orbital_atom_matches_oracle():
     for a in range(2):
         assert np.abs(g[0, 0, a, a] - ref["gmats"][0, a]).max() <= 1e-8
     s.close()
+
+
+@pytest.mark.parametrize("nspin", [1, 2])
+def test_single_orbital_atom_finite_temperature(nspin):
+    """beta = 2, all four states kept (lanc_nstates_total = 4): Z over the
+    kept states, relative to the ground doublet's weight, is
+    2 + 2 e^{-beta U/2}; <n> = 1 and docc = e^{-beta U/2}/Z; at half filling
+    G(iwn) is the same atomic limit at any temperature; the chains have
+    length one (jdim = 1)."""
+    u, beta = 2.0, 2.0
+    m = O.Model(norb=1, nbath=0, nspin=nspin, uloc=(u, 0.0, 0.0), beta=beta,
+                e=np.zeros((nspin, 1, 0)), v=np.zeros((nspin, 1, 0)))
+    s = solver(m, lanc_nstates_total=4)
+    s.ed_solve(np.zeros(0))
+    e, _, z = s.eigenspace()
+    assert len(e) == 4
+    # weights relative to the ground state (E = -U/4): two states at +U/4
+    assert abs(z - (2.0 + 2.0 * np.exp(-beta * u / 2))) <= 1e-12 * z
+    ob = s.observables()
+    assert abs(ob["dens"][0] - 1.0) <= 1e-13
+    assert abs(ob["docc"][0] - np.exp(-beta * u / 2) / z) <= 1e-13
+    wm = O.matsubara(beta, LM)
+    g = s.ed_get_gimp_matsubara()
+    ref = 0.5 * (1.0 / (1j * wm - u / 2) + 1.0 / (1j * wm + u / 2))
+    for i in range(nspin):
+        assert np.abs(g[i, i, 0, 0] - ref).max() <= 1e-12
+    s.close()
