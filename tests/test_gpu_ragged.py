@@ -52,3 +52,32 @@ def test_single_matsubara_point(tmp_path):
     assert np.isclose(a[0, 2] + 1j * a[0, 1], s.ed_get_sigma_matsubara()[0, 0, 0, 0, 0],
                       rtol=0, atol=0)
     s.close()
+
+
+@pytest.mark.parametrize("precision", [dmfted.FP64, dmfted.MIXED])
+def test_doped_polarised_scan_t0(precision):
+    """xmu = 0.7, HFMODE off, a spin-split bath (Nspin = 2), T = 0 over all
+    sectors: the ground state lies away from half filling and is magnetised;
+    E0, Z, n_up, n_dw, magz and G(iwn) of both spins against the oracle's
+    solve (1e-10, 1e-9, 1e-8)."""
+    rng = np.random.default_rng(21)
+    e = rng.uniform(-1.0, 1.0, (1, 1, 4))
+    v = 0.5 + rng.uniform(-0.1, 0.1, (1, 1, 4))
+    e = np.concatenate([e - 0.15, e + 0.15])
+    v = np.concatenate([v, v * 1.05])
+    m = O.Model(norb=1, nbath=4, nspin=2, uloc=(2.5, 0.0, 0.0), xmu=0.7, hfmode=False,
+                beta=100.0, e=e, v=v)
+    s = solver(m, lmats=128, lreal=0, precision=precision)
+    s.ed_solve(m.bath_array())
+    ref = O.solve_t0(m, lmats=128, nthreads=4)
+    assert abs(s.egs() - ref["egs"]) <= 1e-10 * abs(ref["egs"])
+    _, _, z = s.eigenspace()
+    assert abs(z - ref["zeta"]) <= 1e-12
+    ob = s.observables()
+    for k in ("dens_up", "dens_dw", "magz"):
+        assert np.allclose(ob[k], ref["obs"][k], rtol=0, atol=1e-9), k
+    assert abs(ob["magz"][0]) > 1e-3 and abs(ob["dens"][0] - 1.0) > 1e-3
+    g = s.ed_get_gimp_matsubara()
+    for i in range(2):
+        assert np.abs(g[i, i, 0, 0] - ref["gmats"][i, 0]).max() <= 1e-8
+    s.close()
