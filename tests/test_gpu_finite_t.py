@@ -67,3 +67,33 @@ def test_finite_t_second_solve_adapts_state_count():
     assert len(e2) >= n1
     assert np.all(np.diff(e2) >= -1e-12)
     s.close()
+
+
+def test_finite_t_three_orbitals_with_spin_exchange():
+    """Norb = 3 (the largest orbital count) with the Jhflag spin-exchange and
+    pair-hopping terms (Jx = Jp = 0.4) at finite temperature on a spin-split
+    bath: the kept eigenspace, Z, the observables and G(iwn) of every spin and
+    orbital against the oracle (1e-10, 1e-9, 1e-8)."""
+    import dataclasses
+    m = split_model(41, 3, 1, beta=30.0, ust=2.0, jh=0.4)
+    m = dataclasses.replace(m, jx=0.4, jp=0.4, jhflag=True)
+    p = dmfted.default_params(norb=3, nbath=1, nspin=2, uloc=list(m.uloc), ust=m.ust, jh=m.jh,
+                              jx=m.jx, jp=m.jp, jhflag=1, beta=m.beta, lmats=256, lreal=0,
+                              lanc_nstates_total=12)
+    s = dmfted.EDSolver(p)
+    s.ed_solve(m.bath_array())
+    ref = O.solve_finite_t(m, lmats=256, nstates_total=12, nthreads=4)
+    e, secs, z = s.eigenspace()
+    re = np.array([x[0] for x in ref["states"]])
+    assert len(e) == len(re)
+    assert np.array_equal(secs, np.array([x[1] for x in ref["states"]]))
+    assert np.allclose(e, re, rtol=0, atol=1e-10 * max(1.0, np.abs(re).max()))
+    assert abs(z - ref["zeta"]) <= 1e-10 * ref["zeta"]
+    ob = s.observables()
+    for k in ("dens", "docc", "magz"):
+        assert np.allclose(ob[k], ref["obs"][k], rtol=0, atol=1e-9), k
+    gm = s.ed_get_gimp_matsubara()
+    for ispin in range(2):
+        for a in range(3):
+            assert np.abs(gm[ispin, ispin, a, a] - ref["gmats"][ispin, a]).max() <= 1e-8
+    s.close()
